@@ -1,0 +1,46 @@
+"""cdft_b200: the cdft hot path (cusp-factorised apply, CheFSI + Rayleigh--Ritz, Coulomb-cutoff
+Poisson, LDA/PBE XC with the cusp-aware quadrature, and the SCF driver around them) as sm_100a CUDA
+kernels behind a C ABI (``include/cdftb.h``), with a host layer that mirrors the reference's Python
+interfaces (``src/cdft/operators``, ``src/cdft/eigen``, ``src/cdft/xc``, ``src/cdft/scf``).
+
+The package directory's name is not a Python identifier; ``__graft_entry__.package()`` imports it
+and registers it as ``cdft_b200``.
+"""
+
+from __future__ import annotations
+
+from . import _lib
+from .eigen import (
+    ChebyshevFilteredSubspace,
+    EigenConfig,
+    EigenResult,
+    SpectralBoundsHint,
+    chebyshev_coefficients,
+    chebyshev_filter,
+    rayleigh_ritz,
+    residual_norms,
+)
+from .grid import UniformGrid
+from .operators import CuspFactoredHamiltonian, Measure, lanczos_bounds, measure_cross, seeded_randn, weighted_divergence
+
+__all__ = [
+    "ChebyshevFilteredSubspace",
+    "CuspFactoredHamiltonian",
+    "EigenConfig",
+    "EigenResult",
+    "Measure",
+    "SpectralBoundsHint",
+    "UniformGrid",
+    "chebyshev_coefficients",
+    "chebyshev_filter",
+    "lanczos_bounds",
+    "measure_cross",
+    "rayleigh_ritz",
+    "residual_norms",
+    "seeded_randn",
+    "weighted_divergence",
+]
+
+
+def library_path() -> str:
+    return str(_lib.LIBRARY_PATH)

@@ -1,0 +1,67 @@
+// Shared helpers of the cdftb library: status plumbing, launch checks and small device utilities.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cdftb.h"
+
+namespace cdftb {
+
+// The last failed CUDA call's error, per host thread (cdftb_last_cuda_error).
+extern thread_local int g_last_cuda_error;
+
+inline int check_launch() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        g_last_cuda_error = static_cast<int>(e);
+        return CDFTB_ERR_LAUNCH;
+    }
+    return CDFTB_OK;
+}
+
+inline int check(cudaError_t e) {
+    if (e != cudaSuccess) {
+        g_last_cuda_error = static_cast<int>(e);
+        return CDFTB_ERR_LAUNCH;
+    }
+    return CDFTB_OK;
+}
+
+inline cudaStream_t as_stream(cdftb_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+template <typename T>
+__device__ __forceinline__ T load_as(const void* p, int dtype, int64_t i);
+
+template <>
+__device__ __forceinline__ double load_as<double>(const void* p, int dtype, int64_t i) {
+    return dtype == CDFTB_F64 ? static_cast<const double*>(p)[i]
+                              : static_cast<double>(static_cast<const float*>(p)[i]);
+}
+
+template <>
+__device__ __forceinline__ float load_as<float>(const void* p, int dtype, int64_t i) {
+    return dtype == CDFTB_F64 ? static_cast<float>(static_cast<const double*>(p)[i])
+                              : static_cast<const float*>(p)[i];
+}
+
+template <typename T>
+__device__ __forceinline__ void store_as(void* p, int dtype, int64_t i, T v) {
+    if (dtype == CDFTB_F64)
+        static_cast<double*>(p)[i] = static_cast<double>(v);
+    else
+        static_cast<float*>(p)[i] = static_cast<float>(v);
+}
+
+// Staggered first-derivative weights onto a face from `accuracy` nodes (k = -p .. p-1), the exact
+// rationals of src/cdft/operators/divergence.py:31-74 rounded to double. Filled on the host.
+struct StaggeredTaps {
+    double c[8];
+    int half;
+};
+
+StaggeredTaps staggered_taps(int accuracy);
+
+}  // namespace cdftb

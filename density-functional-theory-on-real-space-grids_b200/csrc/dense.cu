@@ -1,0 +1,251 @@
+// (e2-e5) The small dense steps of Rayleigh--Ritz kept on the device, so an eigensolver iteration
+// needs no host round trip: Cholesky of the m x m Gram matrix, the triangular solve L^{-1} B
+// applied column by column (what torch.linalg.solve_triangular does for each grid point,
+// src/cdft/eigen/rayleigh_ritz.py:51-72), the symmetric eigenproblem of the subspace matrix by
+// cyclic Jacobi (rayleigh_ritz.py:97-99), the block rotation U^T Q (rayleigh_ritz.py:100), the
+// residual H psi - eps psi (rayleigh_ritz.py:105-115) and the Lanczos vector updates
+// (src/cdft/operators/hamiltonian.py:252-262). m is at most 32.
+
+#include <math.h>
+
+#include "common.cuh"
+
+namespace cdftb {
+
+namespace {
+
+constexpr int MMAX = 32;
+
+__global__ void cholesky_kernel(const double* __restrict__ gram, double* __restrict__ lower, int* __restrict__ info,
+                                int m, int groups) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= groups) return;
+    const double* s = gram + static_cast<int64_t>(g) * m * m;
+    double* l = lower + static_cast<int64_t>(g) * m * m;
+    int bad = 0;
+    for (int i = 0; i < m * m; ++i) l[i] = 0.0;
+    for (int j = 0; j < m && !bad; ++j) {
+        double d = s[j * m + j];
+        for (int k = 0; k < j; ++k) d -= l[j * m + k] * l[j * m + k];
+        if (!(d > 0.0)) {
+            bad = j + 1;
+            break;
+        }
+        const double ljj = sqrt(d);
+        l[j * m + j] = ljj;
+        for (int i = j + 1; i < m; ++i) {
+            double v = s[i * m + j];
+            for (int k = 0; k < j; ++k) v -= l[i * m + k] * l[j * m + k];
+            l[i * m + j] = v / ljj;
+        }
+    }
+    info[g] = bad;
+}
+
+// Forward substitution x = L^{-1} b for every column p of a block (rows are orbitals).
+__global__ void trsm_lower_kernel(const double* __restrict__ lower, const double* __restrict__ in, int64_t in_stride,
+                                  void* out, int out_dtype, int64_t out_stride, int m, int64_t n, int groups) {
+    __shared__ double l[MMAX * MMAX];
+    const int g = blockIdx.y;
+    for (int i = threadIdx.x; i < m * m; i += blockDim.x) l[i] = lower[static_cast<int64_t>(g) * m * m + i];
+    __syncthreads();
+    const double* src = in + g * in_stride;
+    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double x[MMAX];
+#pragma unroll
+        for (int i = 0; i < MMAX; ++i) {
+            if (i >= m) break;
+            double v = src[i * n + p];
+            for (int k = 0; k < i; ++k) v -= l[i * m + k] * x[k];
+            x[i] = v / l[i * m + i];
+            store_as<double>(out, out_dtype, g * out_stride + i * n + p, x[i]);
+        }
+    }
+}
+
+__global__ void eigh_kernel(const double* __restrict__ matrix, double* __restrict__ evals, double* __restrict__ vectors,
+                            int m, int groups) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= groups) return;
+    double a[MMAX * MMAX];
+    double v[MMAX * MMAX];
+    const double* src = matrix + static_cast<int64_t>(g) * m * m;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+            a[i * m + j] = 0.5 * (src[i * m + j] + src[j * m + i]);
+            v[i * m + j] = (i == j) ? 1.0 : 0.0;
+        }
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < m; ++i) {
+            diag += a[i * m + i] * a[i * m + i];
+            for (int j = i + 1; j < m; ++j) off += a[i * m + j] * a[i * m + j];
+        }
+        if (off <= 1e-36 * diag || off == 0.0) break;
+        for (int p = 0; p < m - 1; ++p) {
+            for (int q = p + 1; q < m; ++q) {
+                const double apq = a[p * m + q];
+                if (apq == 0.0) continue;
+                const double app = a[p * m + p];
+                const double aqq = a[q * m + q];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0);
+                const double s = t * c;
+                for (int k = 0; k < m; ++k) {
+                    const double akp = a[k * m + p];
+                    const double akq = a[k * m + q];
+                    a[k * m + p] = c * akp - s * akq;
+                    a[k * m + q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < m; ++k) {
+                    const double apk = a[p * m + k];
+                    const double aqk = a[q * m + k];
+                    a[p * m + k] = c * apk - s * aqk;
+                    a[q * m + k] = s * apk + c * aqk;
+                }
+                a[p * m + q] = 0.0;
+                a[q * m + p] = 0.0;
+                for (int k = 0; k < m; ++k) {
+                    const double vkp = v[k * m + p];
+                    const double vkq = v[k * m + q];
+                    v[k * m + p] = c * vkp - s * vkq;
+                    v[k * m + q] = s * vkp + c * vkq;
+                }
+            }
+        }
+    }
+    // Sort ascending (selection sort: m is small) and write eigenvectors as rows.
+    int order[MMAX];
+    for (int i = 0; i < m; ++i) order[i] = i;
+    for (int i = 0; i < m; ++i) {
+        int best = i;
+        for (int j = i + 1; j < m; ++j)
+            if (a[order[j] * m + order[j]] < a[order[best] * m + order[best]]) best = j;
+        const int tmp = order[i];
+        order[i] = order[best];
+        order[best] = tmp;
+    }
+    double* ev = evals + static_cast<int64_t>(g) * m;
+    double* vec = vectors + static_cast<int64_t>(g) * m * m;
+    for (int k = 0; k < m; ++k) {
+        const int col = order[k];
+        ev[k] = a[col * m + col];
+        for (int j = 0; j < m; ++j) vec[k * m + j] = v[j * m + col];
+    }
+}
+
+__global__ void rotate_kernel(const double* __restrict__ r, const double* __restrict__ in, int64_t in_stride, void* out,
+                              int out_dtype, int64_t out_stride, int m_out, int m_in, int64_t n) {
+    __shared__ double rs[MMAX * MMAX];
+    const int g = blockIdx.y;
+    for (int i = threadIdx.x; i < m_out * m_in; i += blockDim.x) rs[i] = r[static_cast<int64_t>(g) * m_out * m_in + i];
+    __syncthreads();
+    const double* src = in + g * in_stride;
+    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double x[MMAX];
+        for (int j = 0; j < m_in; ++j) x[j] = src[j * n + p];
+        for (int i = 0; i < m_out; ++i) {
+            double v = 0.0;
+            for (int j = 0; j < m_in; ++j) v = fma(rs[i * m_in + j], x[j], v);
+            store_as<double>(out, out_dtype, g * out_stride + i * n + p, v);
+        }
+    }
+}
+
+__global__ void residual_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                const double* __restrict__ evals, double* __restrict__ out, int m, int64_t n,
+                                int64_t group_stride) {
+    const int g = blockIdx.y;
+    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        for (int i = 0; i < m; ++i) {
+            const int64_t k = g * group_stride + i * n + p;
+            out[k] = a[k] - evals[g * m + i] * b[k];
+        }
+}
+
+__global__ void lanczos_kernel(int mode, double* __restrict__ w, const double* __restrict__ v,
+                               const double* __restrict__ v_prev, const double* __restrict__ s1,
+                               const double* __restrict__ s2, int64_t n) {
+    const int g = blockIdx.y;
+    const double a1 = s1 ? s1[g] : 0.0;
+    const double a2 = s2 ? s2[g] : 0.0;
+    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t k = g * n + p;
+        if (mode == 0 || mode == 1) {
+            // w - a1 v - a2 v_prev, as (w - a1 v) - a2 v_prev (hamiltonian.py:255, 258)
+            w[k] = (w[k] - a1 * v[k]) - a2 * v_prev[k];
+        } else {
+            // v_next = w / sqrt(a1) with a1 = <w, w> (hamiltonian.py:259-262)
+            w[k] = w[k] / sqrt(a1 > 0.0 ? a1 : 0.0);
+        }
+    }
+}
+
+inline unsigned point_blocks(int64_t n) {
+    const int64_t b = ceil_div(n, 256);
+    return static_cast<unsigned>(b < 148 * 8 ? b : 148 * 8);
+}
+
+}  // namespace
+
+}  // namespace cdftb
+
+using namespace cdftb;
+
+extern "C" int cdftb_small_cholesky_f64(const double* gram, double* lower, int* info, int m, int groups,
+                                        cdftb_stream_t stream) {
+    if (!gram || !lower || !info || m <= 0 || m > MMAX || groups <= 0) return CDFTB_ERR_ARGUMENT;
+    cholesky_kernel<<<static_cast<unsigned>(ceil_div(groups, 32)), 32, 0, as_stream(stream)>>>(gram, lower, info, m, groups);
+    return check_launch();
+}
+
+extern "C" int cdftb_block_trsm_lower_f64(const double* lower, const double* in, int64_t in_group_stride, void* out,
+                                          int out_dtype, int64_t out_group_stride, int m, int64_t n, int groups,
+                                          cdftb_stream_t stream) {
+    if (!lower || !in || !out || m <= 0 || m > MMAX || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
+    dim3 grid(point_blocks(n), groups);
+    trsm_lower_kernel<<<grid, 256, 0, as_stream(stream)>>>(lower, in, in_group_stride, out, out_dtype, out_group_stride, m, n,
+                                                           groups);
+    return check_launch();
+}
+
+extern "C" int cdftb_small_eigh_f64(const double* matrix, double* evals, double* vectors, int m, int groups,
+                                    cdftb_stream_t stream) {
+    if (!matrix || !evals || !vectors || m <= 0 || m > MMAX || groups <= 0) return CDFTB_ERR_ARGUMENT;
+    eigh_kernel<<<static_cast<unsigned>(ceil_div(groups, 32)), 32, 0, as_stream(stream)>>>(matrix, evals, vectors, m, groups);
+    return check_launch();
+}
+
+extern "C" int cdftb_block_rotate_f64(const double* r, const double* in, int64_t in_group_stride, void* out,
+                                      int out_dtype, int64_t out_group_stride, int m_out, int m_in, int64_t n,
+                                      int groups, cdftb_stream_t stream) {
+    if (!r || !in || !out || m_out <= 0 || m_in <= 0 || m_out > MMAX || m_in > MMAX || n <= 0 || groups <= 0 ||
+        groups > 65535)
+        return CDFTB_ERR_ARGUMENT;
+    dim3 grid(point_blocks(n), groups);
+    rotate_kernel<<<grid, 256, 0, as_stream(stream)>>>(r, in, in_group_stride, out, out_dtype, out_group_stride, m_out, m_in, n);
+    return check_launch();
+}
+
+extern "C" int cdftb_block_residual_f64(const double* a, const double* b, const double* evals, double* out, int m,
+                                        int64_t n, int groups, int64_t group_stride, cdftb_stream_t stream) {
+    if (!a || !b || !evals || !out || m <= 0 || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
+    dim3 grid(point_blocks(n), groups);
+    residual_kernel<<<grid, 256, 0, as_stream(stream)>>>(a, b, evals, out, m, n, group_stride);
+    return check_launch();
+}
+
+extern "C" int cdftb_lanczos_update_f64(int mode, double* w, const double* v, const double* v_prev, const double* s1,
+                                        const double* s2, int64_t n, int groups, cdftb_stream_t stream) {
+    if (!w || mode < 0 || mode > 2 || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
+    if (mode < 2 && (!v || !v_prev || !s1 || !s2)) return CDFTB_ERR_ARGUMENT;
+    if (mode == 2 && !s1) return CDFTB_ERR_ARGUMENT;
+    dim3 grid(point_blocks(n), groups);
+    lanczos_kernel<<<grid, 256, 0, as_stream(stream)>>>(mode, w, v, v_prev, s1, s2, n);
+    return check_launch();
+}

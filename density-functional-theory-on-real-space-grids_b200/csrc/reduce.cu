@@ -1,0 +1,142 @@
+// (e1) Tall-skinny weighted products M_ij = sum_p q_p a_ip b_jp for blocks of a few rows and
+// O(10^5-10^6) columns: the Gram, cross and inner products of the measure
+// (src/cdft/eigen/measure.py:72-96). Two deterministic passes: every CTA reduces a fixed chunk of
+// columns for a tile of (i, j) pairs into a partial, and a second kernel sums the partials of each
+// pair in chunk order, so the result does not depend on scheduling.
+
+#include "common.cuh"
+
+namespace cdftb {
+
+namespace {
+
+constexpr int RT = 256;
+
+struct CrossShape {
+    int ti, tj, tiles_i, tiles_j, chunks;
+    int64_t chunk;
+};
+
+CrossShape cross_shape(int ma, int mb, int64_t n, int groups) {
+    CrossShape s{};
+    if (ma <= 6 && mb <= 6) {
+        s.ti = s.tj = 6;
+    } else {
+        s.ti = s.tj = 4;
+    }
+    s.tiles_i = static_cast<int>(ceil_div(ma, s.ti));
+    s.tiles_j = static_cast<int>(ceil_div(mb, s.tj));
+    const int64_t blocks_per_chunkset = static_cast<int64_t>(s.tiles_i) * s.tiles_j * groups;
+    int64_t chunks = ceil_div(2 * 148, blocks_per_chunkset);
+    const int64_t max_chunks = ceil_div(n, 2048);
+    if (chunks > max_chunks) chunks = max_chunks;
+    if (chunks < 1) chunks = 1;
+    s.chunk = ceil_div(n, chunks);
+    s.chunks = static_cast<int>(ceil_div(n, s.chunk));
+    return s;
+}
+
+template <int TI, int TJ>
+__global__ void __launch_bounds__(RT) cross_partial_kernel(const double* __restrict__ a, int ma, int64_t sa,
+                                                            const double* __restrict__ b, int mb, int64_t sb,
+                                                            const double* __restrict__ q, int64_t n, int tiles_j,
+                                                            int64_t chunk, int chunks, double* __restrict__ partial) {
+    const int c = blockIdx.x;
+    const int tile = blockIdx.y;
+    const int g = blockIdx.z;
+    const int i0 = (tile / tiles_j) * TI;
+    const int j0 = (tile % tiles_j) * TJ;
+    const int64_t p0 = c * chunk;
+    const int64_t p1 = (p0 + chunk < n) ? p0 + chunk : n;
+    const double* ag = a + g * sa;
+    const double* bg = b + g * sb;
+    double acc[TI][TJ];
+#pragma unroll
+    for (int i = 0; i < TI; ++i)
+#pragma unroll
+        for (int j = 0; j < TJ; ++j) acc[i][j] = 0.0;
+    for (int64_t p = p0 + threadIdx.x; p < p1; p += RT) {
+        const double w = q ? q[p] : 1.0;
+        double av[TI], bv[TJ];
+#pragma unroll
+        for (int i = 0; i < TI; ++i) av[i] = (i0 + i < ma) ? ag[(i0 + i) * n + p] * w : 0.0;
+#pragma unroll
+        for (int j = 0; j < TJ; ++j) bv[j] = (j0 + j < mb) ? bg[(j0 + j) * n + p] : 0.0;
+#pragma unroll
+        for (int i = 0; i < TI; ++i)
+#pragma unroll
+            for (int j = 0; j < TJ; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+    __shared__ double red[RT / 32][TI * TJ];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < TI; ++i)
+#pragma unroll
+        for (int j = 0; j < TJ; ++j) {
+            double v = acc[i][j];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0) red[warp][i * TJ + j] = v;
+        }
+    __syncthreads();
+    if (threadIdx.x < TI * TJ) {
+        double v = 0.0;
+        for (int w = 0; w < RT / 32; ++w) v += red[w][threadIdx.x];
+        partial[((static_cast<int64_t>(g) * gridDim.y + tile) * chunks + c) * (TI * TJ) + threadIdx.x] = v;
+    }
+}
+
+__global__ void cross_final_kernel(const double* __restrict__ partial, int ma, int mb, int ti, int tj, int tiles_j,
+                                   int tiles, int chunks, int groups, double* __restrict__ out) {
+    const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t total = static_cast<int64_t>(groups) * ma * mb;
+    if (idx >= total) return;
+    const int g = static_cast<int>(idx / (static_cast<int64_t>(ma) * mb));
+    const int rem = static_cast<int>(idx % (static_cast<int64_t>(ma) * mb));
+    const int i = rem / mb;
+    const int j = rem % mb;
+    const int tile = (i / ti) * tiles_j + (j / tj);
+    const int slot = (i % ti) * tj + (j % tj);
+    const double* src = partial + (static_cast<int64_t>(g) * tiles + tile) * chunks * (ti * tj) + slot;
+    double v = 0.0;
+    for (int c = 0; c < chunks; ++c) v += src[static_cast<int64_t>(c) * ti * tj];
+    out[idx] = v;
+}
+
+}  // namespace
+
+}  // namespace cdftb
+
+using namespace cdftb;
+
+extern "C" int64_t cdftb_measure_cross_scratch_bytes(int ma, int mb, int64_t n, int groups) {
+    if (ma <= 0 || mb <= 0 || n <= 0 || groups <= 0) return 0;
+    CrossShape s = cross_shape(ma, mb, n, groups);
+    return static_cast<int64_t>(groups) * s.tiles_i * s.tiles_j * s.chunks * s.ti * s.tj * 8;
+}
+
+extern "C" int cdftb_measure_cross_f64(const double* a, int ma, int64_t group_stride_a, const double* b, int mb,
+                                       int64_t group_stride_b, const double* q, int64_t n, int groups, double* out,
+                                       void* scratch, int64_t scratch_bytes, cdftb_stream_t stream) {
+    if (!a || !b || !out || ma <= 0 || mb <= 0 || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
+    CrossShape s = cross_shape(ma, mb, n, groups);
+    const int64_t need = cdftb_measure_cross_scratch_bytes(ma, mb, n, groups);
+    if (!scratch || scratch_bytes < need) return CDFTB_ERR_ARGUMENT;
+    cudaStream_t st = as_stream(stream);
+    double* partial = static_cast<double*>(scratch);
+    const int tiles = s.tiles_i * s.tiles_j;
+    dim3 grid(s.chunks, tiles, groups);
+    if (s.ti == 6)
+        cross_partial_kernel<6, 6><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, n, s.tiles_j,
+                                                        s.chunk, s.chunks, partial);
+    else
+        cross_partial_kernel<4, 4><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, n, s.tiles_j,
+                                                        s.chunk, s.chunks, partial);
+    int rc = check_launch();
+    if (rc != CDFTB_OK) return rc;
+    const int64_t total = static_cast<int64_t>(groups) * ma * mb;
+    cross_final_kernel<<<static_cast<unsigned>(ceil_div(total, 128)), 128, 0, st>>>(partial, ma, mb, s.ti, s.tj, s.tiles_j,
+                                                                                   tiles, s.chunks, groups, out);
+    return check_launch();
+}

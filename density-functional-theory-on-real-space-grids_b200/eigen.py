@@ -1,0 +1,323 @@
+"""Chebyshev-filtered subspace iteration and Rayleigh--Ritz on the device.
+
+Host mirror of ``src/cdft/eigen/chefsi.py`` (chebyshev_filter, chebyshev_coefficients,
+SpectralBoundsHint, ChebyshevFilteredSubspace) and ``src/cdft/eigen/rayleigh_ritz.py``
+(orthonormalise, rayleigh_ritz, residual_norms). The filter is one library call
+(``cdftb_chebyshev_filter``: every step of the recurrence fused into the apply); the Rayleigh--Ritz
+step is the Gram reduction, a device Cholesky, the column-wise triangular solve, one apply, the
+subspace reduction, a device Jacobi eigensolver and a rotation -- no host round trip inside it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import F32, F64, call, ptr, stream_handle
+from .operators import Measure, measure_cross, rowwise_inner, seeded_randn
+
+BOUND_REUSE_RITZ_FRACTION = 0.9
+
+
+def chebyshev_coefficients(degree: int, lower: float, upper: float, spectrum_min: float):
+    """Rows ``(c, a_k, b_k)`` of the scaled recurrence (``src/cdft/eigen/chefsi.py:116-136``)."""
+    if upper <= lower:
+        raise ValueError(f"filter interval is empty: lower={lower}, upper={upper}")
+    e = 0.5 * (upper - lower)
+    c = 0.5 * (upper + lower)
+    sigma = e / (spectrum_min - c)
+    sigma1 = sigma
+    rows = [(c, sigma1 / e, 0.0)]
+    for _ in range(2, degree + 1):
+        sigma2 = 1.0 / (2.0 / sigma1 - sigma)
+        rows.append((c, 2.0 * sigma2 / e, sigma * sigma2))
+        sigma = sigma2
+    return rows
+
+
+def chebyshev_filter(hamiltonian, block: torch.Tensor, degree: int, lower: float, upper: float,
+                     spectrum_min: float, *, precision: torch.dtype | None = None) -> torch.Tensor:
+    """The scaled Chebyshev filter of [F2] (``src/cdft/eigen/chefsi.py:81-113``), one library call.
+
+    ``precision=torch.float32`` runs the recurrence in float (the mixed-precision form): the
+    float64 block is read once, every intermediate is float, and the result is written back as
+    float64 for the float64 Rayleigh--Ritz step.
+    """
+    if upper <= lower:
+        raise ValueError(f"filter interval is empty: lower={lower}, upper={upper}")
+    rows = chebyshev_coefficients(degree, lower, upper, spectrum_min)
+    table = torch.tensor(rows, dtype=torch.float64).to(block.device, non_blocking=False)
+    return filter_with_table(hamiltonian, block, table, degree, orbitals_per_group=block.numel() // block.shape[-1],
+                             precision=precision)
+
+
+def filter_with_table(hamiltonian, block: torch.Tensor, table: torch.Tensor, degree: int, *, orbitals_per_group: int,
+                      potential: torch.Tensor | None = None, precision: torch.dtype | None = None) -> torch.Tensor:
+    """Run the fused filter with a device coefficient table ``(groups, degree, 3)``."""
+    _lib.require_cuda(block, "block")
+    x = block.contiguous()
+    n = hamiltonian.grid.n_points
+    batch = x.numel() // n
+    work_dtype = precision or hamiltonian.dtype
+    if work_dtype != hamiltonian.dtype:
+        raise ValueError("the filter runs in the Hamiltonian's dtype; build it with dtype=float32 for the mixed form")
+    out = torch.empty_like(x)
+    work = torch.empty((2, batch, n), dtype=work_dtype, device=x.device)
+    op = hamiltonian.operator(potential, orbitals_per_group=orbitals_per_group)
+    hamiltonian.note_applications(degree)
+    call("cdftb_chebyshev_filter", ctypes.byref(op), ptr(x), _lib.dtype_code(x), ptr(out), _lib.dtype_code(out),
+         ptr(work), batch, ptr(table.contiguous()), degree, stream_handle(x.device))
+    return out
+
+
+class RitzWorkspace:
+    """Device buffers of one Rayleigh--Ritz step, reused across calls of the same shape."""
+
+    def __init__(self):
+        self._key = None
+
+    def get(self, m: int, groups: int, device):
+        key = (m, groups, str(device))
+        if key != self._key:
+            f = dict(dtype=torch.float64, device=device)
+            self.lower = torch.empty((groups, m, m), **f)
+            self.info = torch.empty(groups, dtype=torch.int32, device=device)
+            self.evals = torch.empty((groups, m), **f)
+            self.rot = torch.empty((groups, m, m), **f)
+            self._key = key
+        return self
+
+
+_WS = RitzWorkspace()
+
+
+def orthonormalise(block: torch.Tensor, measure: Measure, groups: int = 1) -> torch.Tensor:
+    """Cholesky orthonormalisation in the measure (``src/cdft/eigen/rayleigh_ritz.py:51-72``).
+
+    On a Cholesky failure the reference falls back to an eigendecomposition that drops rank; that
+    rare branch reads the Gram matrix to the host and builds the reduced basis there.
+    """
+    n = measure.grid.n_points
+    flat = block.to(torch.float64).reshape(groups, -1, n).contiguous()
+    m = flat.shape[1]
+    gram = measure_cross(flat, flat, measure.quadrature, groups)
+    ws = _WS.get(m, groups, block.device)
+    stream = stream_handle(block.device)
+    call("cdftb_small_cholesky_f64", ptr(gram), ptr(ws.lower), ptr(ws.info), m, groups, stream)
+    basis = torch.empty_like(flat)
+    call("cdftb_block_trsm_lower_f64", ptr(ws.lower), ptr(flat), flat.stride(0), ptr(basis), F64, basis.stride(0), m, n,
+         groups, stream)
+    ws.last_info = ws.info
+    return basis, gram
+
+
+def _rank_revealing_basis(flat: torch.Tensor, gram: torch.Tensor) -> torch.Tensor:
+    """The eigh fallback of rayleigh_ritz.py:64-70 for one group (host-side small matrix)."""
+    g = gram.cpu().numpy()
+    evals, evecs = np.linalg.eigh(0.5 * (g + g.T))
+    keep = evals > evals[-1] * 1e-14
+    if not keep.any():
+        raise ValueError("the orbital block collapsed to rank zero")
+    scaled = evecs[:, keep] / np.sqrt(evals[keep])
+    r = torch.from_numpy(np.ascontiguousarray(scaled.T)).to(flat.device)
+    out = torch.empty((1, r.shape[0], flat.shape[-1]), dtype=torch.float64, device=flat.device)
+    call("cdftb_block_rotate_f64", ptr(r), ptr(flat.contiguous()), 0, ptr(out), F64, 0, r.shape[0], r.shape[1],
+         flat.shape[-1], 1, stream_handle(flat.device))
+    return out[0]
+
+
+def rayleigh_ritz(hamiltonian, block: torch.Tensor, measure: Measure, *, host: bool = True):
+    """Diagonalise within span(block) (``src/cdft/eigen/rayleigh_ritz.py:75-102``).
+
+    Returns ``(eigenvalues, eigenvectors, orthonormality_error)``; with ``host=False`` the error is
+    a 0-d device tensor. Also leaves ``applied = A @ eigenvectors`` on the result for the residual
+    (it equals ``U^T (A Q)`` with ``U`` orthogonal), so :func:`residual_norms` needs no extra apply.
+    """
+    n = measure.grid.n_points
+    flat = block.to(torch.float64).reshape(-1, n)
+    basis, gram = orthonormalise(flat, measure)
+    ws = _WS.get(flat.shape[0], 1, block.device)
+    if int(ws.info[0].item()) != 0:
+        basis = _rank_revealing_basis(flat, gram[0]).reshape(1, -1, n)
+    m = basis.shape[1]
+    stream = stream_handle(block.device)
+    applied = hamiltonian.apply(basis[0]).reshape(1, m, n)
+    sub = measure_cross(basis, applied, measure.quadrature)
+    ws = _WS.get(m, 1, block.device)
+    call("cdftb_small_eigh_f64", ptr(sub), ptr(ws.evals), ptr(ws.rot), m, 1, stream)
+    vectors = torch.empty((1, m, n), dtype=torch.float64, device=block.device)
+    call("cdftb_block_rotate_f64", ptr(ws.rot), ptr(basis), basis.stride(0), ptr(vectors), F64, vectors.stride(0), m, m,
+         n, 1, stream)
+    rotated_applied = torch.empty_like(vectors)
+    call("cdftb_block_rotate_f64", ptr(ws.rot), ptr(applied), applied.stride(0), ptr(rotated_applied), F64,
+         rotated_applied.stride(0), m, m, n, 1, stream)
+    g2 = measure_cross(vectors, vectors, measure.quadrature)[0]
+    error = (g2 - torch.eye(m, dtype=torch.float64, device=block.device)).abs().max()
+    evals = ws.evals[0].clone()
+    vec = vectors[0]
+    _APPLIED[id(vec)] = (vec, rotated_applied[0])
+    return evals, vec, (float(error) if host else error)
+
+
+_APPLIED: dict[int, tuple] = {}
+
+
+def residual_norms(hamiltonian, eigenvalues: torch.Tensor, vectors: torch.Tensor, measure: Measure) -> torch.Tensor:
+    """``||H psi_i - eps_i psi_i||`` in the measure (``src/cdft/eigen/rayleigh_ritz.py:105-115``).
+
+    When ``vectors`` came from :func:`rayleigh_ritz`, ``H psi`` is the rotated ``A Q`` it already
+    formed (one apply fewer); otherwise the operator is applied.
+    """
+    n = measure.grid.n_points
+    cached = _APPLIED.pop(id(vectors), None)
+    if cached is not None and cached[0] is vectors:
+        applied = cached[1]
+    else:
+        applied = hamiltonian.apply(vectors)
+    m = vectors.shape[0]
+    res = torch.empty((m, n), dtype=torch.float64, device=vectors.device)
+    call("cdftb_block_residual_f64", ptr(applied.contiguous()), ptr(vectors.contiguous()),
+         ptr(eigenvalues.contiguous()), ptr(res), m, n, 1, m * n, stream_handle(vectors.device))
+    return rowwise_inner(res, res, measure.quadrature).clamp_min(0.0).sqrt()
+
+
+@dataclass(frozen=True)
+class SpectralBoundsHint:
+    """Bounds carried over from the previous SCF iteration (``src/cdft/eigen/chefsi.py:169-182``)."""
+
+    lower: float
+    upper: float
+    shift: torch.Tensor | float = 0.0
+
+
+@dataclass
+class EigenConfig:
+    """The eigensolver settings of ``contract.EigenConfig`` (contract.py:431-449) the path reads."""
+
+    n_extra_states: int = 4
+    extra_states_fraction: float = 0.20
+    chebyshev_degree: int = 20
+    lanczos_steps: int = 12
+    bound_safety: float = 1.02
+    max_iterations: int = 300
+    residual_tol: float = 1.0e-8
+    cross_check_tol: float = 1.0e-8
+
+
+@dataclass
+class EigenResult:
+    eigenvalues: torch.Tensor
+    eigenvectors: torch.Tensor
+    residuals: torch.Tensor
+    n_iterations: int
+    converged: bool
+
+
+def _interval_fraction(value: float, low: float, high: float) -> float:
+    width = high - low
+    return (value - low) / width if width > 0.0 else float("inf")
+
+
+class ChebyshevFilteredSubspace:
+    """CheFSI (``src/cdft/eigen/chefsi.py:408-585``) with the native filter and Rayleigh--Ritz.
+
+    ``filter_precision=torch.float32`` filters in float (the Hamiltonian passed in must then be
+    built with ``dtype=torch.float32`` for the filter via ``filter_hamiltonian``); every
+    Rayleigh--Ritz, residual and Lanczos step stays float64.
+    """
+
+    def __init__(self, grid, config: EigenConfig, ritz_stop: bool = True, filter_hamiltonian=None) -> None:
+        self.grid = grid
+        self.config = config
+        self.ritz_stop = ritz_stop
+        self.filter_hamiltonian = filter_hamiltonian
+        self.history: list[dict] = []
+        self.spectral_bounds = None
+        self.bounds_source = "unset"
+        self.bounds_shift = 0.0
+        self.top_ritz_fraction = float("nan")
+
+    def solve(self, hamiltonian, n_states: int, initial: torch.Tensor | None = None,
+              generator: torch.Generator | None = None, bounds: SpectralBoundsHint | None = None) -> EigenResult:
+        grid = self.grid
+        cfg = self.config
+        measure = hamiltonian.measure
+        extra = max(cfg.n_extra_states, int(cfg.extra_states_fraction * n_states))
+        size = min(n_states + extra, grid.n_points)
+        if initial is None:
+            block = seeded_randn((size, grid.n_points), generator, device=grid.device)
+        else:
+            block = initial.to(torch.float64).reshape(-1, grid.n_points)
+            if block.shape[0] < size:
+                pad = seeded_randn((size - block.shape[0], grid.n_points), generator, device=grid.device)
+                block = torch.cat([block, pad], dim=0)
+
+        def lanczos():
+            return hamiltonian.spectral_bounds(steps=cfg.lanczos_steps, safety=cfg.bound_safety, generator=generator)
+
+        if bounds is None:
+            spectrum_min, spectrum_max = lanczos()
+            self.bounds_source = "lanczos"
+            self.bounds_shift = 0.0
+        evals, vectors, orth = rayleigh_ritz(hamiltonian, block, measure, host=False)
+        converged = False
+        iteration = 0
+        residual = residual_norms(hamiltonian, evals, vectors, measure)
+        previous = evals.clone()
+        stable = 0
+        self.eigenvalue_drift = float("inf")
+        self.stop_reason = "iteration limit"
+        weak_form = self.ritz_stop and bool(getattr(hamiltonian, "uses_divergence_form", False))
+        eigenvalue_tol = 0.1 * cfg.cross_check_tol
+        top = min(size, evals.shape[0]) - 1
+        if bounds is None:
+            next_lower = float(evals[top])
+        else:
+            shift = bounds.shift if isinstance(bounds.shift, float) else bounds.shift
+            vals = torch.stack([evals[top], torch.as_tensor(shift, dtype=torch.float64, device=evals.device)]).tolist()
+            next_lower, shift = vals
+            spectrum_min, spectrum_max = bounds.lower - shift, bounds.upper + shift
+            self.bounds_source = "reused"
+            self.bounds_shift = shift
+        top_fraction = float("-inf")
+        filt = self.filter_hamiltonian or hamiltonian
+        for iteration in range(1, cfg.max_iterations + 1):
+            lower = next_lower
+            fraction = _interval_fraction(lower, spectrum_min, spectrum_max)
+            if self.bounds_source == "reused" and not fraction < BOUND_REUSE_RITZ_FRACTION:
+                spectrum_min, spectrum_max = lanczos()
+                self.bounds_source = (f"lanczos (reuse rejected: top Ritz fraction {fraction:.3f} >= "
+                                      f"{BOUND_REUSE_RITZ_FRACTION:g} at iteration {iteration})")
+                fraction = _interval_fraction(lower, spectrum_min, spectrum_max)
+            top_fraction = max(top_fraction, fraction)
+            lower = min(max(lower, spectrum_min + 1e-8), spectrum_max - 1e-8)
+            filtered = chebyshev_filter(filt, vectors, cfg.chebyshev_degree, lower, spectrum_max, spectrum_min)
+            if filt is not hamiltonian:
+                hamiltonian.note_applications(cfg.chebyshev_degree)
+            evals, vectors, orth_error = rayleigh_ritz(hamiltonian, filtered, measure, host=False)
+            residual = residual_norms(hamiltonian, evals, vectors, measure)
+            top = min(size, evals.shape[0]) - 1
+            worst, drift, orth, next_lower = torch.stack([
+                residual[:n_states].max(), (evals[:n_states] - previous[:n_states]).abs().max(), orth_error,
+                evals[top]]).tolist()
+            previous = evals.clone()
+            self.eigenvalue_drift = drift
+            self.history.append({"iteration": float(iteration), "residual": worst, "orthonormality": orth,
+                                 "eigenvalue_drift": drift})
+            if worst < cfg.residual_tol:
+                converged = True
+                self.stop_reason = "residual below residual_tol"
+                break
+            stable = stable + 1 if (weak_form and drift < eigenvalue_tol) else 0
+            if stable >= 2:
+                converged = True
+                self.stop_reason = ("Ritz values stable on the weak-form path; the collocation residual is "
+                                    f"{worst:.3e}, above residual_tol {cfg.residual_tol:.1e}")
+                break
+        self.spectral_bounds = (spectrum_min, spectrum_max)
+        self.top_ritz_fraction = top_fraction
+        return EigenResult(evals[:n_states], vectors[:n_states], residual[:n_states], iteration, converged)

@@ -1,0 +1,380 @@
+"""Benchmark: He-LDA 65^3 SCF solves per second on one B200 (or N replicas, one per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|fp64] [--impl native|reference]
+
+A step is one complete self-consistent solve of He at VWN-LDA on the 16-bohr, h = 0.25 (65^3) grid
+with linear density mixing alpha = 0.3 -- from the hydrogenic initial density to the converged
+energy (|dE| < 1e-8 Ha, ||dn||_1 < 1e-6), then the final full diagonalisation -- with the geometry
+(cusp factor, quadrature, Poisson plan) built before the timed region, as the reference caches it.
+``--form mixed`` (default) filters in float32 and refines in float64; ``fp64`` is the plain float64
+drop-in. The device-timed ``value`` starts from the initial density resident in HBM; ``e2e`` copies
+the initial density from pinned host memory and reads the converged density and energies back every
+step, through the package's public ``solve_self_consistent``. The L2 cache is flushed (a 256 MiB
+write) before every step, outside the timed events.
+
+``--impl reference`` times the CPU restatement of the reference (``oracle/``) on this host on a
+bounded sample of the same solve (one Chebyshev filter and two potential evaluations, scaled by a
+full solve's counts of both) and prints the same metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "He-LDA 65^3 SCF solves/s at <=1e-8 Ha vs FP64"
+UNIT = "solves/s"
+REFERENCE_ENERGY_KEY = "he65_lda_linear"
+
+
+def _args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("native", "reference"), default="native")
+    p.add_argument("--form", choices=("mixed", "fp64"), default="mixed")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--kernel-only", action="store_true",
+                   help="time only the fused Chebyshev step on a He grid of --edge points (for profiling)")
+    p.add_argument("--edge", type=int, default=65)
+    p.add_argument("--orbitals", type=int, default=5)
+    return p.parse_args()
+
+
+def _golden():
+    return json.loads((ROOT / "tests" / "golden" / "reference_values.json").read_text())[REFERENCE_ENERGY_KEY]
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows: list[list[str]] = []
+        self._proc = None
+        self._thread = None
+
+    def start(self):
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                          stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self._proc = None
+            return
+        self._thread = threading.Thread(target=self._read, daemon=True)
+        self._thread.start()
+
+    def _read(self):
+        for line in self._proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self) -> dict:
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+        if self._thread is not None:
+            self._thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) > 8:
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _profile_traffic(kernel_tag: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if present."""
+    path = ROOT / "profiles" / "stencil_filter_he65.txt"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith(f"traffic_bytes_per_launch[{kernel_tag}]"):
+            try:
+                return float(line.split("=", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def filter_step_roofline(pkg, dev, grid, hamiltonian, m: int, precision, reps: int = 5, degree: int = 20):
+    """Average device time of one fused Chebyshev step (stencil apply + recurrence) on m orbitals."""
+    import torch
+
+    block = torch.randn((m, grid.n_points), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
+    for _ in range(2):
+        pkg.chebyshev_filter(hamiltonian, block, degree, 1.0, 100.0, -3.0)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    total = 0.0
+    for _ in range(reps):
+        flush.fill_(1.0)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        pkg.chebyshev_filter(hamiltonian, block, degree, 1.0, 100.0, -3.0)
+        end.record(stream)
+        end.synchronize()
+        total += start.elapsed_time(end) / 1e3
+    per_launch_s = total / (reps * degree)
+    s_bytes = 4 if precision == torch.float32 else 8
+    algorithmic = grid.n_points * s_bytes * (3 * m + 5)
+    return per_launch_s, algorithmic
+
+
+def run_kernel_only(args) -> None:
+    """The fused Chebyshev step alone on a He grid (profiling entry: small, bounded)."""
+    import torch
+
+    import __graft_entry__
+
+    pkg = __graft_entry__.package()
+    dev = torch.device("cuda:0")
+    spacing = 16.0 / (args.edge - 1)
+    grid = pkg.UniformGrid.box((16.0, 16.0, 16.0), spacing, (0.0, 0.0, 0.0), device=dev)
+    geometry = pkg.build_cusp_geometry(grid, (2.0,), ((0.0, 0.0, 0.0),))
+    precision = torch.float32 if args.form == "mixed" else torch.float64
+    ham = pkg.CuspFactoredHamiltonian(grid, geometry.factor, quadrature=geometry.quadrature, dtype=precision)
+    per_launch_s, algorithmic = filter_step_roofline(pkg, dev, grid, ham, args.orbitals, precision, reps=args.steps)
+    peak, kind = _peaks()
+    achieved = algorithmic / per_launch_s / 1e9
+    print(json.dumps({"kernel": "stencil_kernel (one Chebyshev step)", "grid": grid.shape, "orbitals": args.orbitals,
+                      "form": args.form, "us_per_launch": per_launch_s * 1e6, "algorithmic_bytes": algorithmic,
+                      "achieved_gbs": achieved, "peak_gbs": peak, "peak_kind": kind, "frac": achieved / peak}),
+          flush=True)
+
+
+def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str]:
+    """Seconds for one full solve of the CPU restatement, from a bounded, measured sample.
+
+    The sample is one degree-20 Chebyshev filter of the 5-orbital block (20 operator applications)
+    and two Kohn--Sham potential evaluations; a full solve makes ``golden['applications']`` (3146)
+    block applications and 72 potential evaluations (two per SCF iteration, 35 iterations plus the
+    final one), so the estimate is the sum of those counts times the measured unit costs.
+    """
+    import numpy as np
+
+    from oracle import eigen as oeigen
+    from oracle import scf as oscf
+    from oracle.operators import CuspHamiltonian
+
+    grid, factor, quad = geometry
+    step = oscf.KohnShamStep(system, grid, factor, quad)
+    n0 = oscf.initial_density(step)
+    t = time.perf_counter()
+    p = step.potentials(n0)
+    p = step.potentials(n0)
+    t_pot = (time.perf_counter() - t) / 2
+    ham = CuspHamiltonian(grid, factor, quad, extra_potential=p["effective"], bare=step.bare)
+    block = np.random.default_rng(0).standard_normal((5, grid.n_points))
+    t = time.perf_counter()
+    oeigen.chebyshev_filter(ham, block, 20, 1.0, 100.0, -3.0)
+    t_apply = (time.perf_counter() - t) / 20
+    n_pot = 2 * (golden["iterations"] + 1)
+    full = golden["applications"] * t_apply + n_pot * t_pot
+    text = (f"numpy restatement, one thread: one degree-20 filter of 5 orbitals ({t_apply * 1e3:.0f} ms per block "
+            f"application) and two potential evaluations ({t_pot * 1e3:.0f} ms each), scaled to a full solve's "
+            f"{golden['applications']:.0f} applications and {n_pot} evaluations; geometry build excluded")
+    return full, text
+
+
+def run_reference(args) -> None:
+    """CPU restatement of the reference on this host, bounded sample of the solve per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import scf as oscf
+
+    system = oscf.he_lda()
+    geometry = oscf.build_geometry(system)
+    golden = _golden()
+    samples = []
+    steps = max(1, args.steps)
+    text = ""
+    for i in range(max(0, args.warmup) + steps):
+        full, text = oracle_solve_estimate(system, geometry, golden)
+        if i >= args.warmup:
+            samples.append(full)
+    full_s = statistics.median(samples)
+    value = 1.0 / full_s
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": full_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (the He atom system itself; no dataset)",
+        "config": {"workload": "He-LDA 65^3 SCF solve (box 16 bohr, h 0.25, linear mixing 0.3)", "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": text},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    if args.kernel_only:
+        run_kernel_only(args)
+        return
+    import torch
+
+    import __graft_entry__
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and world > 1:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE {world}")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+
+    pkg = __graft_entry__.package()
+    lib = pkg._lib.library()
+    from oracle import scf as oscf  # the system definition only (charges, box, spacing)
+
+    system = oscf.he_lda()
+    grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev)
+    geometry = pkg.build_cusp_geometry(grid, system.charges, system.positions)
+    precision = torch.float32 if args.form == "mixed" else torch.float64
+    step = pkg.KohnShamStep(geometry, "lda_vwn", system.n_electrons, filter_precision=precision)
+    mixing = pkg.MixingConfig(scheme="linear", alpha=0.3)
+    golden = _golden()
+    n0 = pkg.initial_density(step)
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
+
+    def solve(initial):
+        return pkg.solve_self_consistent(step, mixing, initial_density_override=initial)
+
+    for _ in range(max(0, args.warmup)):
+        solve(n0)
+    torch.cuda.synchronize()
+
+    # --- device-timed steps, inputs resident in HBM ---
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.cdftb_launch_count()
+    total_ms = 0.0
+    energies = []
+    stream = torch.cuda.current_stream()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        out = solve(n0)
+        end.record(stream)
+        end.synchronize()
+        total_ms += start.elapsed_time(end)
+        energies.append(out.energies["total"])
+    torch.cuda.synchronize()
+    launches = lib.cdftb_launch_count() - launches0
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    seconds = total_ms / 1e3
+    if dist is not None:
+        t = torch.tensor([seconds], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        seconds = float(t.item())
+    value = world * args.steps / seconds
+    error = max(abs(e - golden["total"]) for e in energies)
+
+    # --- end to end through the public API with host buffers ---
+    host_in = n0.cpu().pin_memory()
+    host_out = torch.empty_like(n0, device="cpu").pin_memory()
+    e2e_ms = 0.0
+    e2e_steps = max(1, min(args.steps, 2))
+    for _ in range(e2e_steps):
+        flush.fill_(1.0)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        dev_in = host_in.to(dev, non_blocking=True)
+        out = solve(dev_in)
+        host_out.copy_(out.density, non_blocking=True)
+        end.record(stream)
+        end.synchronize()
+        e2e_ms += start.elapsed_time(end)
+    e2e_s = e2e_ms / 1e3
+    if dist is not None:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * e2e_steps / e2e_s
+    bytes_in = host_in.numel() * host_in.element_size()
+    bytes_out = host_out.numel() * host_out.element_size() + 8 * 12
+
+    # --- roofline of the dominant kernel: one fused Chebyshev step (apply + recurrence) ---
+    ham = step.hamiltonian(step.potentials(n0), dtype=precision)
+    per_launch_s, algorithmic = filter_step_roofline(pkg, dev, grid, ham, 5, precision)
+    achieved = algorithmic / per_launch_s / 1e9
+    peak, peak_kind = _peaks()
+    tag = "f32" if precision == torch.float32 else "f64"
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": seconds * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-filter/f64" if precision == torch.float32 else "f64",
+        "data": "synthetic (the He atom system itself; no dataset)",
+        "config": {"workload": "He-LDA 65^3 SCF solve (box 16 bohr, h 0.25, linear mixing 0.3), one system per GPU",
+                   "form": args.form, "l2": "flushed (256 MiB write) before every step",
+                   "parallelism": f"replicas{world}", "energy_error_vs_reference_cpu_fp64_ha": error,
+                   "scf_iterations": out.scf_iterations, "applications_per_solve": out.applications},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_in, "d2h_bytes_per_step": bytes_out},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": _profile_traffic(tag), "kernel": f"stencil_kernel<{tag}> (one Chebyshev step, m=5)",
+                     "peak_kind": peak_kind},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        full_s, text = oracle_solve_estimate(system, oscf.build_geometry(system), golden)
+        result["cpu_baseline"] = {"value": 1.0 / full_s, "unit": UNIT, "cores": 1, "kind": "port", "sample": text}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

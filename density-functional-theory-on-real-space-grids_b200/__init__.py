@@ -9,7 +9,7 @@ and registers it as ``cdft_b200``.
 
 from __future__ import annotations
 
-from . import _lib
+from . import _lib, geometry, poisson, scf, xc
 from .eigen import (
     ChebyshevFilteredSubspace,
     EigenConfig,
@@ -21,9 +21,29 @@ from .eigen import (
     residual_norms,
 )
 from .grid import UniformGrid
+from .geometry import CuspFactor, CuspGeometry, CuspQuadrature, StepGeometry, build_cusp_geometry
 from .operators import CuspFactoredHamiltonian, Measure, lanczos_bounds, measure_cross, seeded_randn, weighted_divergence
+from .poisson import CoulombCutoffPoisson
+from .scf import (KohnShamStep, MixingConfig, SCFConfig, initial_density, solve_noninteracting,
+                  solve_self_consistent)
+from .xc import LDA, PBE, functional_by_name
 
 __all__ = [
+    "CoulombCutoffPoisson",
+    "CuspFactor",
+    "CuspGeometry",
+    "CuspQuadrature",
+    "KohnShamStep",
+    "LDA",
+    "MixingConfig",
+    "PBE",
+    "SCFConfig",
+    "StepGeometry",
+    "build_cusp_geometry",
+    "functional_by_name",
+    "initial_density",
+    "solve_noninteracting",
+    "solve_self_consistent",
     "ChebyshevFilteredSubspace",
     "CuspFactoredHamiltonian",
     "EigenConfig",

@@ -39,6 +39,7 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_version": (c_int, []),
     "cdftb_status_string": (c_char_p, [c_int]),
     "cdftb_last_cuda_error": (c_int, []),
+    "cdftb_launch_count": (ctypes.c_ulonglong, []),
     "cdftb_weighted_divergence_f64": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p, c_void_p,
                                               c_void_p, c_double, c_int, c_void_p]),
     "cdftb_cusp_apply": (c_int, [ctypes.POINTER(Operator), c_void_p, c_int, c_void_p, c_int, c_int64, c_int, c_void_p]),
@@ -58,6 +59,56 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_lanczos_update_f64": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int,
                                          c_void_p]),
     "cdftb_cast": (c_int, [c_void_p, c_int, c_void_p, c_int, c_int64, c_void_p]),
+    "cdftb_stencil_set_tile": (c_int, [c_int, c_int, c_int]),
+    "cdftb_poisson_plan_create": (c_int, [c_int, c_int, c_int, c_double, c_double, c_int, ctypes.POINTER(c_void_p),
+                                          ctypes.POINTER(c_int), ctypes.POINTER(c_double)]),
+    "cdftb_poisson_plan_destroy": (c_int, [c_void_p]),
+    "cdftb_poisson_kernel_table": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
+    "cdftb_poisson_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "cdftb_xc_lda_vwn_f64": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
+    "cdftb_xc_pbe_f64": (c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "cdftb_quadrature_stencils": (c_int, [c_void_p, c_int64, c_int, c_int, c_int, c_double, c_double, c_double, c_double,
+                                          c_void_p, c_void_p, c_void_p, c_void_p]),
+    "cdftb_lift_plan_scratch_bytes": (c_int64, [c_int64, c_int64]),
+    "cdftb_lift_plan_build": (c_int, [c_void_p, c_int64, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int64,
+                                      c_void_p]),
+    "cdftb_quadrature_interpolate_f64": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p, c_int,
+                                                 c_int64, c_void_p, c_int64, c_void_p]),
+    "cdftb_quadrature_lift_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_int,
+                                          c_int64, c_void_p, c_int64, c_void_p]),
+    "cdftb_cusp_coefficients_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    "cdftb_hartree_split_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int64, c_int, c_void_p,
+                                        c_void_p, c_void_p]),
+    "cdftb_potentials_node_lda_f64": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                              c_void_p, c_void_p, c_void_p]),
+    "cdftb_potentials_grid_lda_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                              c_void_p, c_int, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p,
+                                              c_void_p, c_void_p]),
+    "cdftb_row_sums_scratch_bytes": (c_int64, [c_int, c_int64]),
+    "cdftb_row_sums_f64": (c_int, [c_void_p, c_int, c_int64, c_void_p, c_void_p, c_int64, c_void_p]),
+    "cdftb_fd_derivative_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_double,
+                                        c_int64, c_int, c_double, c_void_p]),
+    "cdftb_geometry_cusp_fields": (c_int, [c_int, c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_double, c_double,
+                                           c_double, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                           c_void_p]),
+    "cdftb_geometry_face_weights": (c_int, [c_int, c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_double, c_double,
+                                            c_double, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "cdftb_geometry_node_fields": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p,
+                                           c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "cdftb_geometry_grid_far": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_double,
+                                        c_double, c_double, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "cdftb_geometry_lumped_far": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_double,
+                                          c_double, c_double, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                          c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                          c_void_p, c_double, c_double, c_void_p, c_void_p, c_void_p]),
+    "cdftb_geometry_bare_terms": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_double, c_void_p,
+                                          c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "cdftb_geometry_step_fields": (c_int, [c_int, c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_double, c_double,
+                                           c_double, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "cdftb_geometry_initial_density": (c_int, [c_int, c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_double,
+                                               c_double, c_double, c_double, c_void_p, c_void_p, c_void_p, c_void_p,
+                                               c_void_p]),
+    "cdftb_scale_f64": (c_int, [c_void_p, c_int64, c_double, c_void_p]),
 }
 
 

@@ -6,6 +6,7 @@
 namespace cdftb {
 
 thread_local int g_last_cuda_error = 0;
+unsigned long long g_launch_count = 0;
 
 StaggeredTaps staggered_taps(int accuracy) {
     // The exact rationals solving sum_k c_k (k + 1/2)^m = delta_{m,1}, k = -p .. p-1
@@ -74,6 +75,8 @@ extern "C" const char* cdftb_status_string(int status) {
 }
 
 extern "C" int cdftb_last_cuda_error(void) { return g_last_cuda_error; }
+
+extern "C" unsigned long long cdftb_launch_count(void) { return __atomic_load_n(&g_launch_count, __ATOMIC_RELAXED); }
 
 extern "C" int cdftb_cast(const void* in, int in_dtype, void* out, int out_dtype, int64_t count,
                           cdftb_stream_t stream) {

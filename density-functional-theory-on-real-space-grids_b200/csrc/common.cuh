@@ -10,8 +10,11 @@ namespace cdftb {
 
 // The last failed CUDA call's error, per host thread (cdftb_last_cuda_error).
 extern thread_local int g_last_cuda_error;
+// Kernels this library has launched in this process (cdftb_launch_count).
+extern unsigned long long g_launch_count;
 
 inline int check_launch() {
+    __atomic_fetch_add(&g_launch_count, 1ull, __ATOMIC_RELAXED);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         g_last_cuda_error = static_cast<int>(e);

@@ -19,8 +19,6 @@ namespace cdftb {
 namespace {
 
 constexpr int TZ = 32;
-constexpr int TY = 8;
-constexpr int THREADS = TZ * TY;
 
 enum Mode { MODE_DIV = 0, MODE_KINETIC = 1, MODE_APPLY = 2, MODE_CHEB_FIRST = 3, MODE_CHEB = 4 };
 
@@ -50,15 +48,125 @@ struct StencilArgs {
     double taps[8];
 };
 
-template <typename T, int P>
-__global__ void __launch_bounds__(THREADS) stencil_kernel(const StencilArgs a) {
-    constexpr int H = 2 * P - 1;  // halo reach of the composite stencil
-    constexpr int K = 2 * P;      // taps per staggered derivative
-    constexpr int PW = TZ + 2 * H;
-    constexpr int PH = TY + 2 * H;
-    __shared__ T s_phi[PH][PW];
-    __shared__ T s_fy[TY + K - 1][TZ];
-    __shared__ T s_fz[TY][TZ + K - 1];
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src, bool pred, int bytes) {
+    const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    const int src_size = pred ? bytes : 0;  // src-size 0 zero-fills the destination
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(gmem_src), "r"(src_size));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(gmem_src), "r"(src_size));
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+template <typename T, int P, int TYV>
+struct StencilLayout {
+    static constexpr int H = 2 * P - 1;
+    static constexpr int K = 2 * P;
+    static constexpr int PW = TZ + 2 * H;
+    static constexpr int PH = TYV + 2 * H;
+    static constexpr int NPHI = PH * PW;
+    static constexpr int NW1 = (TYV + K - 1) * TZ;
+    static constexpr int NW2 = TYV * (TZ + K - 1);
+    static constexpr int NT = TYV * TZ;
+    // stage: phi | w1 | w2 | w0 | inv | pot | prev
+    static constexpr int OFF_W1 = NPHI;
+    static constexpr int OFF_W2 = OFF_W1 + NW1;
+    static constexpr int OFF_W0 = OFF_W2 + NW2;
+    static constexpr int OFF_INV = OFF_W0 + NT;
+    static constexpr int OFF_POT = OFF_INV + NT;
+    static constexpr int OFF_PREV = OFF_POT + NT;
+    static constexpr int STAGE = OFF_PREV + NT;
+    static constexpr int NS = 3;
+    static constexpr int OFF_FY = NS * STAGE;
+    static constexpr int OFF_FZ = OFF_FY + NW1;
+    static constexpr int TOTAL = OFF_FZ + NW2;
+    static constexpr size_t BYTES = sizeof(T) * TOTAL;
+};
+
+// Issue the asynchronous copies of everything step q reads into its pipeline stage. Out-of-range
+// elements are zero-filled by the copy itself (the Dirichlet halo, and the missing faces).
+template <typename T, int P, int TYV>
+__device__ __forceinline__ void stage_loads(const StencilArgs& a, T* st, int q, int xa, int xe, int y0, int z0,
+                                            int64_t base, int64_t pot_base, int tid, int ty, int tz) {
+    using L = StencilLayout<T, P, TYV>;
+    constexpr int H = L::H, K = L::K, PW = L::PW, THR = TZ * TYV;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const T* in = static_cast<const T*>(a.in);
+    const bool plane_in = (q >= 0) && (q < nx);
+    for (int idx = tid; idx < L::NPHI; idx += THR) {
+        const int r = idx / PW;
+        const int c = idx - r * PW;
+        const int gy = y0 - H + r;
+        const int gz = z0 - H + c;
+        const bool ok = plane_in && gy >= 0 && gy < ny && gz >= 0 && gz < nz;
+        const T* src = ok ? in + base + (static_cast<int64_t>(q) * ny + gy) * nz + gz : in;
+        cp_async(st + idx, src, ok, sizeof(T));
+    }
+    if (q >= xa && q <= xe) {
+        const T* w1 = static_cast<const T*>(a.w1);
+        const T* w2 = static_cast<const T*>(a.w2);
+        for (int idx = tid; idx < L::NW1; idx += THR) {
+            const int r = idx / TZ;
+            const int c = idx - r * TZ;
+            const int g = y0 - P + r;
+            const int gz = z0 + c;
+            const bool ok = gz < nz && g >= -P && g <= ny + P - 1;
+            const T* src = ok ? w1 + (static_cast<int64_t>(q) * (ny + K) + g + P) * nz + gz : w1;
+            cp_async(st + L::OFF_W1 + idx, src, ok, sizeof(T));
+        }
+        for (int idx = tid; idx < L::NW2; idx += THR) {
+            const int r = idx / (TZ + K - 1);
+            const int c = idx - r * (TZ + K - 1);
+            const int g = z0 - P + c;
+            const int gy = y0 + r;
+            const bool ok = gy < ny && g >= -P && g <= nz + P - 1;
+            const T* src = ok ? w2 + (static_cast<int64_t>(q) * ny + gy) * (nz + K) + g + P : w2;
+            cp_async(st + L::OFF_W2 + idx, src, ok, sizeof(T));
+        }
+    }
+    const int y = y0 + ty;
+    const int z = z0 + tz;
+    const bool valid = (y < ny) && (z < nz);
+    const int f = q - P;
+    if (q >= xa && f <= nx + P - 1) {
+        const T* w0 = static_cast<const T*>(a.w0);
+        const T* src = valid ? w0 + (static_cast<int64_t>(f + P) * ny + y) * nz + z : w0;
+        cp_async(st + L::OFF_W0 + tid, src, valid, sizeof(T));
+    }
+    const int i = q - H;
+    if (i >= xa && i <= xe && a.mode >= MODE_KINETIC) {
+        const int64_t point = (static_cast<int64_t>(i) * ny + y) * nz + z;
+        const T* inv = static_cast<const T*>(a.inv_w);
+        cp_async(st + L::OFF_INV + tid, valid ? inv + point : inv, valid, sizeof(T));
+        if (a.mode >= MODE_APPLY) {
+            const T* pot = static_cast<const T*>(a.pot);
+            cp_async(st + L::OFF_POT + tid, valid ? pot + pot_base + point : pot, valid, sizeof(T));
+        }
+        if (a.mode == MODE_CHEB) {
+            const T* prev = static_cast<const T*>(a.prev);
+            cp_async(st + L::OFF_PREV + tid, valid ? prev + base + point : prev, valid, sizeof(T));
+        }
+    }
+}
+
+template <typename T, int P, int TYV>
+__global__ void __launch_bounds__(TZ* TYV) stencil_kernel(const StencilArgs a) {
+    using L = StencilLayout<T, P, TYV>;
+    constexpr int H = L::H;
+    constexpr int K = L::K;
+    constexpr int PW = L::PW;
+    constexpr int NS = L::NS;
+    constexpr int THR = TZ * TYV;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    T* s_fy = smem + L::OFF_FY;
+    T* s_fz = smem + L::OFF_FZ;
 
     const int tz = threadIdx.x;
     const int ty = threadIdx.y;
@@ -66,7 +174,7 @@ __global__ void __launch_bounds__(THREADS) stencil_kernel(const StencilArgs a) {
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int64_t n_points = static_cast<int64_t>(nx) * ny * nz;
     const int tile = blockIdx.x;
-    const int y0 = (tile / a.tiles_z) * TY;
+    const int y0 = (tile / a.tiles_z) * TYV;
     const int z0 = (tile % a.tiles_z) * TZ;
     const int xa = blockIdx.y * a.xchunk;
     const int xe = min(xa + a.xchunk, nx) - 1;
@@ -101,55 +209,58 @@ __global__ void __launch_bounds__(THREADS) stencil_kernel(const StencilArgs a) {
         }
     }
 
-    for (int q = xa - H; q <= xe + H; ++q) {
-        __syncthreads();
-        const bool plane_in = (q >= 0) && (q < nx);
-        for (int idx = tid; idx < PH * PW; idx += THREADS) {
-            const int r = idx / PW;
-            const int c = idx - r * PW;
-            const int gy = y0 - H + r;
-            const int gz = z0 - H + c;
-            T v = T(0);
-            if (plane_in && gy >= 0 && gy < ny && gz >= 0 && gz < nz)
-                v = load_as<T>(a.in, a.in_dtype, base + (static_cast<int64_t>(q) * ny + gy) * nz + gz);
-            s_phi[r][c] = v;
+    const int q_first = xa - H;
+    const int q_last = xe + H;
+#pragma unroll
+    for (int s = 0; s < NS - 1; ++s) {
+        const int q = q_first + s;
+        if (q <= q_last) stage_loads<T, P, TYV>(a, smem + s * L::STAGE, q, xa, xe, y0, z0, base, pot_base, tid, ty, tz);
+        cp_async_commit();
+    }
+
+    for (int q = q_first; q <= q_last; ++q) {
+        const int step = q - q_first;
+        {
+            const int qn = q + NS - 1;
+            if (qn <= q_last)
+                stage_loads<T, P, TYV>(a, smem + ((step + NS - 1) % NS) * L::STAGE, qn, xa, xe, y0, z0, base, pot_base,
+                                       tid, ty, tz);
+            cp_async_commit();
         }
+        cp_async_wait<NS - 1>();
         __syncthreads();
+        const T* st = smem + (step % NS) * L::STAGE;
+        const T* s_phi = st;
+
 #pragma unroll
         for (int k = 0; k < K - 1; ++k) phiq[k] = phiq[k + 1];
-        phiq[K - 1] = s_phi[ty + H][tz + H];
+        phiq[K - 1] = s_phi[(ty + H) * PW + tz + H];
 
+        const int f = q - P;
+        const int i = q - H;
         const bool out_plane = (q >= xa) && (q <= xe);
+        const T w0v = st[L::OFF_W0 + tid];
+        const T invv = st[L::OFF_INV + tid];
+        const T potv = st[L::OFF_POT + tid];
+        const T prevv = st[L::OFF_PREV + tid];
         if (out_plane) {
-            // y faces g = y0 - P + r, r in [0, TY + K - 1): node g + 1 + (k - P) is smem row r + k.
-            for (int idx = tid; idx < (TY + K - 1) * TZ; idx += THREADS) {
+            const T* w1s = st + L::OFF_W1;
+            const T* w2s = st + L::OFF_W2;
+            for (int idx = tid; idx < L::NW1; idx += THR) {
                 const int r = idx / TZ;
                 const int c = idx - r * TZ;
-                const int g = y0 - P + r;
-                const int gz = z0 + c;
-                T f = T(0);
-                if (gz < nz && g >= -P && g <= ny + P - 1) {
-                    T s = T(0);
+                T sum = T(0);
 #pragma unroll
-                    for (int k = 0; k < K; ++k) s += taps[k] * s_phi[r + k][c + H];
-                    f = load_as<T>(a.w1, a.geo_dtype, (static_cast<int64_t>(q) * (ny + K) + g + P) * nz + gz) * s;
-                }
-                s_fy[r][c] = f;
+                for (int k = 0; k < K; ++k) sum += taps[k] * s_phi[(r + k) * PW + c + H];
+                s_fy[idx] = w1s[idx] * sum;
             }
-            // z faces g = z0 - P + c: node is smem column c + k.
-            for (int idx = tid; idx < TY * (TZ + K - 1); idx += THREADS) {
+            for (int idx = tid; idx < L::NW2; idx += THR) {
                 const int r = idx / (TZ + K - 1);
                 const int c = idx - r * (TZ + K - 1);
-                const int g = z0 - P + c;
-                const int gy = y0 + r;
-                T f = T(0);
-                if (gy < ny && g >= -P && g <= nz + P - 1) {
-                    T s = T(0);
+                T sum = T(0);
 #pragma unroll
-                    for (int k = 0; k < K; ++k) s += taps[k] * s_phi[r + H][c + k];
-                    f = load_as<T>(a.w2, a.geo_dtype, (static_cast<int64_t>(q) * ny + gy) * (nz + K) + g + P) * s;
-                }
-                s_fz[r][c] = f;
+                for (int k = 0; k < K; ++k) sum += taps[k] * s_phi[(r + H) * PW + c + k];
+                s_fz[idx] = w2s[idx] * sum;
             }
         }
         __syncthreads();
@@ -158,8 +269,8 @@ __global__ void __launch_bounds__(THREADS) stencil_kernel(const StencilArgs a) {
             T yt = T(0), zt = T(0);
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                yt += taps[k] * s_fy[ty + K - 1 - k][tz];
-                zt += taps[k] * s_fz[ty][tz + K - 1 - k];
+                yt += taps[k] * s_fy[(ty + K - 1 - k) * TZ + tz];
+                zt += taps[k] * s_fz[ty * (TZ + K - 1) + tz + K - 1 - k];
             }
             yz = yt + zt;
         }
@@ -167,20 +278,17 @@ __global__ void __launch_bounds__(THREADS) stencil_kernel(const StencilArgs a) {
         for (int k = 0; k < K - 1; ++k) yzq[k] = yzq[k + 1];
         yzq[K - 1] = yz;
 
-        // x face f = q - P reads planes q - H .. q = phiq[0 .. K-1].
         T fx = T(0);
-        const int f = q - P;
         if (q >= xa && valid && f <= nx + P - 1) {
-            T s = T(0);
+            T sum = T(0);
 #pragma unroll
-            for (int k = 0; k < K; ++k) s += taps[k] * phiq[k];
-            fx = load_as<T>(a.w0, a.geo_dtype, (static_cast<int64_t>(f + P) * ny + y) * nz + z) * s;
+            for (int k = 0; k < K; ++k) sum += taps[k] * phiq[k];
+            fx = w0v * sum;
         }
 #pragma unroll
         for (int k = 0; k < K - 1; ++k) fq[k] = fq[k + 1];
         fq[K - 1] = fx;
 
-        const int i = q - H;
         if (valid && i >= xa && i <= xe) {
             T xt = T(0);
 #pragma unroll
@@ -191,49 +299,68 @@ __global__ void __launch_bounds__(THREADS) stencil_kernel(const StencilArgs a) {
             if (a.mode == MODE_DIV) {
                 result = div;
             } else {
-                const T kin = (div * T(0.5)) * load_as<T>(a.inv_w, a.geo_dtype, point);
+                const T kin = (div * T(0.5)) * invv;
                 if (a.mode == MODE_KINETIC) {
                     result = kin;
                 } else {
                     const T phi = phiq[0];
-                    const T applied = kin + phi * load_as<T>(a.pot, a.geo_dtype, pot_base + point);
+                    const T applied = kin + phi * potv;
                     if (a.mode == MODE_APPLY) {
                         result = applied;
                     } else {
                         result = (applied - c_coef * phi) * a_coef;
-                        if (a.mode == MODE_CHEB) result -= b_coef * load_as<T>(a.prev, a.prev_dtype, base + point);
+                        if (a.mode == MODE_CHEB) result -= b_coef * prevv;
                     }
                 }
             }
             store_as<T>(a.out, a.out_dtype, base + point, result);
         }
     }
+    cp_async_wait<0>();
 }
 
+// Slab tile shape, process-wide: TY rows of 32 z-columns per CTA, and the shortest x chunk. Set by
+// cdftb_stencil_set_tile (the host autotuner); 8 and 12 until then.
+int g_tile_ty = 8;
+int g_min_chunk = 12;
+int g_target_ctas_per_sm = 4;
+
 int choose_xchunk(int nx, int64_t ctas_per_plane_set) {
-    // Enough CTAs for about four per SM on 148 SMs; every chunk re-reads 2(2p-1) halo planes, so
-    // chunks are not made shorter than 12 planes.
-    const int64_t target = 4 * 148;
+    // Enough CTAs for a few per SM on 148 SMs; every chunk re-reads 2(2p-1) halo planes, so chunks
+    // are not made shorter than g_min_chunk planes.
+    const int64_t target = static_cast<int64_t>(g_target_ctas_per_sm) * 148;
     int64_t chunks = ceil_div(target, ctas_per_plane_set);
-    const int64_t max_chunks = ceil_div(nx, 12);
+    const int64_t max_chunks = ceil_div(nx, g_min_chunk);
     if (chunks > max_chunks) chunks = max_chunks;
     if (chunks < 1) chunks = 1;
     return static_cast<int>(ceil_div(nx, chunks));
 }
 
-template <typename T>
-int launch_typed(StencilArgs& a, int accuracy, cudaStream_t stream) {
-    const int tiles_y = static_cast<int>(ceil_div(a.ny, TY));
+template <typename T, int P, int TYV>
+int launch_one(const StencilArgs& part, dim3 grid, cudaStream_t stream) {
+    using L = StencilLayout<T, P, TYV>;
+    static bool configured = false;  // one attribute call per instantiation and process
+    if (!configured) {
+        int st = check(cudaFuncSetAttribute(stencil_kernel<T, P, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(L::BYTES)));
+        if (st != CDFTB_OK) return st;
+        configured = true;
+    }
+    stencil_kernel<T, P, TYV><<<grid, dim3(TZ, TYV), L::BYTES, stream>>>(part);
+    return check_launch();
+}
+
+template <typename T, int TYV>
+int launch_typed_ty(StencilArgs& a, int accuracy, cudaStream_t stream) {
+    const int tiles_y = static_cast<int>(ceil_div(a.ny, TYV));
     a.tiles_z = static_cast<int>(ceil_div(a.nz, TZ));
     const int64_t tiles = static_cast<int64_t>(tiles_y) * a.tiles_z;
     if (a.xchunk <= 0) a.xchunk = choose_xchunk(a.nx, tiles * a.batch);
     const int chunks = static_cast<int>(ceil_div(a.nx, a.xchunk));
-    dim3 block(TZ, TY);
+    const int64_t n_points = static_cast<int64_t>(a.nx) * a.ny * a.nz;
     for (int64_t first = 0; first < a.batch; first += 65535) {
         StencilArgs part = a;
         const int64_t count = (a.batch - first) < 65535 ? (a.batch - first) : 65535;
-        const int64_t n_points = static_cast<int64_t>(a.nx) * a.ny * a.nz;
-        // Offset the batch by advancing the pointers (types differ, so by bytes).
         auto adv = [&](const void* p, int dtype) -> const void* {
             return p ? static_cast<const char*>(p) + first * n_points * (dtype == CDFTB_F64 ? 8 : 4) : p;
         };
@@ -242,24 +369,32 @@ int launch_typed(StencilArgs& a, int accuracy, cudaStream_t stream) {
         part.out = const_cast<void*>(adv(a.out, a.out_dtype));
         part.batch = count;
         if (first > 0 && a.mode >= MODE_APPLY) {
-            // Re-base the group index: only valid when the split falls on a group boundary.
             if (first % a.orb_per_group != 0) return CDFTB_ERR_CAPACITY;
             const int64_t g0 = first / a.orb_per_group;
             part.pot = static_cast<const char*>(a.pot) + g0 * a.pot_stride * (a.geo_dtype == CDFTB_F64 ? 8 : 4);
             if (a.coef) part.coef = a.coef + g0 * a.degree * 3;
         }
         dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(chunks), static_cast<unsigned>(count));
+        int st;
         switch (accuracy) {
-            case 2: stencil_kernel<T, 1><<<grid, block, 0, stream>>>(part); break;
-            case 4: stencil_kernel<T, 2><<<grid, block, 0, stream>>>(part); break;
-            case 6: stencil_kernel<T, 3><<<grid, block, 0, stream>>>(part); break;
-            case 8: stencil_kernel<T, 4><<<grid, block, 0, stream>>>(part); break;
+            case 2: st = launch_one<T, 1, TYV>(part, grid, stream); break;
+            case 4: st = launch_one<T, 2, TYV>(part, grid, stream); break;
+            case 6: st = launch_one<T, 3, TYV>(part, grid, stream); break;
+            case 8: st = launch_one<T, 4, TYV>(part, grid, stream); break;
             default: return CDFTB_ERR_ARGUMENT;
         }
-        int st = check_launch();
         if (st != CDFTB_OK) return st;
     }
     return CDFTB_OK;
+}
+
+template <typename T>
+int launch_typed(StencilArgs& a, int accuracy, cudaStream_t stream) {
+    switch (g_tile_ty) {
+        case 4: return launch_typed_ty<T, 4>(a, accuracy, stream);
+        case 16: return launch_typed_ty<T, 16>(a, accuracy, stream);
+        default: return launch_typed_ty<T, 8>(a, accuracy, stream);
+    }
 }
 
 int launch(StencilArgs& a, int accuracy, double spacing, int compute_dtype, cudaStream_t stream) {
@@ -275,6 +410,10 @@ int launch(StencilArgs& a, int accuracy, double spacing, int compute_dtype, cuda
     // The reference multiplies each slice by (c_k * (1/h)) (divergence.py:112, 121).
     const double scale = 1.0 / spacing;
     for (int k = 0; k < 8; ++k) a.taps[k] = k < accuracy ? t.c[k] * scale : 0.0;
+    // The staged copies move raw elements: inputs, the previous iterate and the geometry must be
+    // in the arithmetic type; only the output may differ.
+    if (a.in_dtype != compute_dtype || a.geo_dtype != compute_dtype) return CDFTB_ERR_ARGUMENT;
+    if (a.mode == MODE_CHEB && a.prev_dtype != compute_dtype) return CDFTB_ERR_ARGUMENT;
     if (compute_dtype == CDFTB_F64) return launch_typed<double>(a, accuracy, stream);
     if (compute_dtype == CDFTB_F32) return launch_typed<float>(a, accuracy, stream);
     return CDFTB_ERR_ARGUMENT;
@@ -301,6 +440,15 @@ StencilArgs args_from_operator(const cdftb_operator* op) {
 }  // namespace cdftb
 
 using namespace cdftb;
+
+extern "C" int cdftb_stencil_set_tile(int tile_y, int min_chunk, int ctas_per_sm) {
+    if (tile_y != 4 && tile_y != 8 && tile_y != 16) return CDFTB_ERR_ARGUMENT;
+    if (min_chunk < 1 || ctas_per_sm < 1) return CDFTB_ERR_ARGUMENT;
+    g_tile_ty = tile_y;
+    g_min_chunk = min_chunk;
+    g_target_ctas_per_sm = ctas_per_sm;
+    return CDFTB_OK;
+}
 
 extern "C" int cdftb_weighted_divergence_f64(const double* box, double* out, int64_t batch, int nx, int ny, int nz,
                                              const double* w0, const double* w1, const double* w2, double spacing,
@@ -340,36 +488,43 @@ extern "C" int cdftb_chebyshev_filter(const cdftb_operator* op, const void* bloc
                                       int out_dtype, void* work, int64_t batch, const double* coefficients,
                                       int degree, cdftb_stream_t stream) {
     if (!op || !block || !out || !work || !coefficients || degree < 1) return CDFTB_ERR_ARGUMENT;
+    if (batch == 0) return CDFTB_OK;
     const int64_t n_points = static_cast<int64_t>(op->nx) * op->ny * op->nz;
     const int esize = op->dtype == CDFTB_F64 ? 8 : 4;
-    // Step k (1-based) writes buffer (degree - k) mod 3: buffer 0 is `out`, so the last step lands
-    // there, and three consecutive steps never share a buffer.
-    void* bufs[3] = {out, work, static_cast<char*>(work) + batch * n_points * esize};
-    const int dts[3] = {out_dtype, op->dtype, op->dtype};
-    const void* y = block;
-    int y_dt = in_dtype;
+    const int dt = op->dtype;
+    char* w = static_cast<char*>(work);
+    void* buf_a = w;
+    void* buf_b = w + batch * n_points * esize;
+    const void* x = block;
+    if (in_dtype != dt) {
+        // The float filter of the mixed form reads the double block once, as a cast copy.
+        void* xc = w + 2 * batch * n_points * esize;
+        int st = cdftb_cast(block, in_dtype, xc, dt, batch * n_points, stream);
+        if (st != CDFTB_OK) return st;
+        x = xc;
+    }
+    // Y_1 -> A, Y_2 -> B, then each Y_{k+1} overwrites Y_{k-1} in place (a point's previous value is
+    // read only by the thread writing that point); the last step writes `out` in out_dtype.
+    const void* y = x;
     const void* prev = nullptr;
-    int prev_dt = in_dtype;
     for (int k = 1; k <= degree; ++k) {
-        const int target = (degree - k) % 3;
+        void* target = (k == degree) ? out : ((k % 2 == 1) ? buf_a : buf_b);
         StencilArgs a = args_from_operator(op);
         a.in = y;
-        a.in_dtype = y_dt;
+        a.in_dtype = dt;
         a.prev = prev;
-        a.prev_dtype = prev_dt;
-        a.out = bufs[target];
-        a.out_dtype = dts[target];
+        a.prev_dtype = dt;
+        a.out = target;
+        a.out_dtype = (k == degree) ? out_dtype : dt;
         a.batch = batch;
         a.coef = coefficients;
         a.degree = degree;
         a.step = k - 1;
         a.mode = (k == 1) ? MODE_CHEB_FIRST : MODE_CHEB;
-        int st = launch(a, op->accuracy, op->spacing, op->dtype, as_stream(stream));
+        int st = launch(a, op->accuracy, op->spacing, dt, as_stream(stream));
         if (st != CDFTB_OK) return st;
         prev = y;
-        prev_dt = y_dt;
-        y = bufs[target];
-        y_dt = dts[target];
+        y = target;
     }
     return CDFTB_OK;
 }

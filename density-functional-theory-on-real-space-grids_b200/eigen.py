@@ -66,7 +66,7 @@ def filter_with_table(hamiltonian, block: torch.Tensor, table: torch.Tensor, deg
     if work_dtype != hamiltonian.dtype:
         raise ValueError("the filter runs in the Hamiltonian's dtype; build it with dtype=float32 for the mixed form")
     out = torch.empty_like(x)
-    work = torch.empty((2, batch, n), dtype=work_dtype, device=x.device)
+    work = torch.empty((3, batch, n), dtype=work_dtype, device=x.device)
     op = hamiltonian.operator(potential, orbitals_per_group=orbitals_per_group)
     hamiltonian.note_applications(degree)
     call("cdftb_chebyshev_filter", ctypes.byref(op), ptr(x), _lib.dtype_code(x), ptr(out), _lib.dtype_code(out),

@@ -131,9 +131,17 @@ class CuspFactoredHamiltonian:
         self._apply_count = 0
         self.dtype = dtype
         faces = factor.face_weights(grid.fd_order)
-        self._faces = tuple(f.to(dtype).contiguous() for f in faces)
-        self._inv = inverse_weight.to(dtype).contiguous()
-        self._pot_cast = self._potential if dtype == torch.float64 else self._potential.to(dtype)
+        if dtype == torch.float64:
+            self._faces = tuple(f.contiguous() for f in faces)
+            self._inv = inverse_weight.contiguous()
+        else:
+            # float copies of the geometry, made once per geometry and dtype
+            cache = factor.__dict__.setdefault("_cast_cache", {})
+            key = (dtype, inverse_weight.data_ptr())
+            if key not in cache:
+                cache[key] = (tuple(cast(f.contiguous(), dtype) for f in faces), cast(inverse_weight.contiguous(), dtype))
+            self._faces, self._inv = cache[key]
+        self._pot_cast = self._potential if dtype == torch.float64 else cast(self._potential, dtype)
 
     # -- the seam --
     @property
@@ -178,6 +186,8 @@ class CuspFactoredHamiltonian:
         if phi.shape[-1] != self.grid.n_points:
             raise ValueError(f"orbitals have {phi.shape[-1]} points, grid has {self.grid.n_points}")
         x = phi.contiguous()
+        if x.dtype != self.dtype:
+            x = cast(x, self.dtype)
         batch = x.numel() // self.grid.n_points
         out = torch.empty_like(x)
         op = self.operator(potential)
@@ -215,6 +225,16 @@ class CuspFactoredHamiltonian:
     def external_energy_direct_tensor(self, rho: torch.Tensor) -> torch.Tensor:
         cross, potential = self.quadrature.external_energy_parts(rho, self.factor)
         return cross + 2.0 * potential
+
+
+def cast(x: torch.Tensor, dtype: torch.dtype) -> torch.Tensor:
+    """Cast a device block between float64 and float32 with the library's cast kernel."""
+    if x.dtype == dtype:
+        return x
+    x = x.contiguous()
+    out = torch.empty(x.shape, dtype=dtype, device=x.device)
+    call("cdftb_cast", ptr(x), _lib.dtype_code(x), ptr(out), _lib.dtype_code(out), x.numel(), stream_handle(x.device))
+    return out
 
 
 def seeded_randn(shape, generator, *, device, dtype=torch.float64) -> torch.Tensor:

@@ -36,6 +36,8 @@ int cdftb_version(void);
 const char* cdftb_status_string(int status);
 /* The cudaError_t of the last failed CUDA call made by this library on this host thread. */
 int cdftb_last_cuda_error(void);
+/* Number of kernels this library has launched in this process (for launch accounting). */
+unsigned long long cdftb_launch_count(void);
 
 /*
  * The cusp-factorised operator A = (1/2 w) sum_d D_d^T [f^2_face,d D_d .] + V on one grid.
@@ -66,17 +68,22 @@ int cdftb_weighted_divergence_f64(const double* box, double* out, int64_t batch,
                                   int accuracy, cdftb_stream_t stream);
 
 /* (a2) out = A phi for a batch of orbitals (src/cdft/operators/hamiltonian.py:251-318,
- * apply / apply_with_potential / kinetic_apply). in_dtype/out_dtype select double or float
- * for phi/out; the arithmetic runs in the operator's dtype. kinetic_only = 1 drops the V phi term
- * (hamiltonian.py:303 kinetic_apply). */
+ * apply / apply_with_potential / kinetic_apply). phi must be in the operator's dtype; out may be
+ * double or float (out_dtype). kinetic_only = 1 drops the V phi term (hamiltonian.py:303). */
 int cdftb_cusp_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* out, int out_dtype,
                      int64_t batch, int kinetic_only, cdftb_stream_t stream);
+
+/* Slab tile of the apply/filter kernels, process-wide: tile_y rows (4, 8 or 16) of 32 z columns per
+ * CTA, x chunks no shorter than min_chunk planes, about ctas_per_sm CTAs per SM. Chosen by the
+ * host autotuner; no reference counterpart (the reference has no kernels of its own). */
+int cdftb_stencil_set_tile(int tile_y, int min_chunk, int ctas_per_sm);
 
 /* (b) The scaled Chebyshev filter of degree `degree` (src/cdft/eigen/chefsi.py:81-160,
  * chebyshev_filter / chebyshev_recurrence, with fused.py:391 chebyshev_update fused into each apply).
  * coefficients: device table (groups, degree, 3) of rows (c, a_k, b_k) from chefsi.py:116
- * chebyshev_coefficients, one table per potential group. block and out are in_dtype/out_dtype;
- * work holds two blocks of the operator's dtype (2 * batch * N elements). */
+ * chebyshev_coefficients, one table per potential group. block and out are in_dtype/out_dtype
+ * (a double block with a float operator is cast once); work holds three blocks of the operator's
+ * dtype (3 * batch * N elements). The input block is never written. */
 int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
                            void* work, int64_t batch, const double* coefficients, int degree,
                            cdftb_stream_t stream);
@@ -128,6 +135,130 @@ int cdftb_lanczos_update_f64(int mode, double* w, const double* v, const double*
 
 /* Cast between double and float blocks (the precision boundary of the mixed form). */
 int cdftb_cast(const void* in, int in_dtype, void* out, int out_dtype, int64_t count, cdftb_stream_t stream);
+
+
+/* ---- (c) Coulomb-cutoff Poisson (src/cdft/operators/poisson.py:21-107) ---- */
+
+/* Plan for one grid: pads every axis to fft_friendly(ceil(pad_factor n)) (poisson.py:36-40), builds
+ * the truncated kernel K(G) (poisson.py:43-64) and two transform buffers for up to max_batch
+ * densities. Allocates device memory (the only allocating calls are *_create). Writes the padded
+ * shape (3 ints) and the cutoff radius. */
+int cdftb_poisson_plan_create(int nx, int ny, int nz, double spacing, double pad_factor, int max_batch,
+                              void** plan, int* padded_shape, double* cutoff_radius);
+int cdftb_poisson_plan_destroy(void* plan);
+/* The device kernel table K (padded0, padded1, padded2/2+1) of a plan. */
+int cdftb_poisson_kernel_table(void* plan, const double** table);
+/* v = irfftn(rfftn(pad(rho)) K)[:n] for `batch` densities (batch x N each): CoulombCutoffPoisson.solve
+ * (poisson.py:66-84). */
+int cdftb_poisson_solve(void* plan, const double* density, double* potential, int batch, cdftb_stream_t stream);
+
+/* ---- (d) exchange-correlation, spin-restricted (src/cdft/xc/base.py:115-189) ---- */
+
+/* Slater + VWN5 (xc/lda.py:113-159, 201-217; dispatch name lda_vwn): e = e_xc per volume, v = de/dn. */
+int cdftb_xc_lda_vwn_f64(const double* density, int64_t points, double* e, double* v, cdftb_stream_t stream);
+/* PBE exchange + correlation (xc/gga.py:43-90; dispatch name pbe): e, v = de/dn, vs = de/dsigma. */
+int cdftb_xc_pbe_f64(const double* density, const double* sigma, int64_t points, double* e, double* v, double* vs,
+                     cdftb_stream_t stream);
+
+/* ---- (d4) cusp-aware quadrature interpolant (src/cdft/operators/quadrature.py:506-650) ---- */
+
+/* Stencil corner (m x 3 ints) and the three 8-point Lagrange weight vectors (m x 24) of every point
+ * (quadrature.py:56-93, 524-541); *bad_flag is set if a stencil leaves the grid. */
+int cdftb_quadrature_stencils(const double* points, int64_t m, int nx, int ny, int nz, double ox, double oy,
+                              double oz, double spacing, int* base, double* w1d, int* bad_flag,
+                              cdftb_stream_t stream);
+/* CSR of L^T (row_ptr: N+1 int64, col: 512 m node indices sorted by (grid point, node)), built by a
+ * device radix sort in caller scratch (quadrature.py:580-608). */
+int64_t cdftb_lift_plan_scratch_bytes(int64_t m, int64_t n_points);
+int cdftb_lift_plan_build(const int* base, int64_t m, int nx, int ny, int nz, long long* row_ptr, int* col,
+                          void* scratch, int64_t scratch_bytes, cdftb_stream_t stream);
+/* out[f][node] = (L field_f)[node] for nf <= 5 fields (quadrature.py:613-620 interpolate). */
+int cdftb_quadrature_interpolate_f64(const int* base, const double* w1d, int64_t m, int nx, int ny, int nz,
+                                     const double* fields, int nf, int64_t field_stride, double* out,
+                                     int64_t out_stride, cdftb_stream_t stream);
+/* out[f] = L^T x_f for nf <= 5 node vectors (quadrature.py:628-638 lift). */
+int cdftb_quadrature_lift_f64(const int* base, const double* w1d, const long long* row_ptr, const int* col, int nx,
+                              int ny, int nz, const double* node_values, int nf, int64_t x_stride, double* out,
+                              int64_t out_stride, cdftb_stream_t stream);
+
+/* ---- (c2, s1) the Kohn-Sham potentials (src/cdft/scf/step.py:224-313) ---- */
+
+/* c = S^{-1} (nucleus_f2 * rho(R_a)) per system (step.py:240-242). */
+int cdftb_cusp_coefficients_f64(const double* rho_at_nuclei, const double* nucleus_f2, const double* overlap,
+                                int n_atoms, int batch, double* coefficients, cdftb_stream_t stream);
+/* rho = n / f^2, n_smooth = n - sum_a c_a exp(-2 Z_a s_a) (step.py:235-244). */
+int cdftb_hartree_split_f64(const double* density, const double* f2, const double* cusp_grid,
+                            const double* coefficients, int n_atoms, int64_t n_points, int batch, double* rho,
+                            double* n_smooth, cdftb_stream_t stream);
+/* Node side, LDA: from [rho_node, vsmooth_node] -> lift inputs [w f2 vH, w f2 v_xc] and w e_xc
+ * (step.py:247-261 with the interpolant fused in by the caller). */
+int cdftb_potentials_node_lda_f64(const double* fields, int64_t m, const double* weights, const double* f2_node,
+                                  const double* v1s_node, const double* coefficients, int n_atoms, int batch,
+                                  double* lift_inputs, double* xc_energy_density, cdftb_stream_t stream);
+/* Grid side, LDA: effective = (hartree_w + xc_w)/omega, v_hartree, terms [3][N] = (hartree_w rho,
+ * xc_w rho, far_w e_xc), v_xc (optional) (step.py:245-303). */
+int cdftb_potentials_grid_lda_f64(const double* density, const double* rho, const double* f2,
+                                  const double* far_weights, const double* mass_weights, const double* v_smooth,
+                                  const double* v1s_grid, const double* coefficients, int n_atoms,
+                                  const double* lifted, int64_t n_points, int batch, double* effective,
+                                  double* v_hartree, double* terms, double* v_xc, cdftb_stream_t stream);
+/* Deterministic row sums of a rows x len array (the energy integrals). */
+int64_t cdftb_row_sums_scratch_bytes(int rows, int64_t len);
+int cdftb_row_sums_f64(const double* a, int rows, int64_t len, double* out, void* scratch, int64_t scratch_bytes,
+                       cdftb_stream_t stream);
+/* out (+)= sign * d/d(axis) in, central weights `coefficients` (accuracy+1 taps), zero halo
+ * (src/cdft/operators/laplacian.py:111-130, grid.py:745-758). */
+int cdftb_fd_derivative_f64(const double* in, double* out, int nx, int ny, int nz, int axis, int accuracy,
+                            const double* coefficients, double spacing, int64_t batch, int accumulate, double sign,
+                            cdftb_stream_t stream);
+
+/* ---- geometry on the device (src/cdft/operators/cusp.py, quadrature.py, scf/step.py:129-165) ----
+ * In these entry points `charges`, `positions` and `spheres` are HOST arrays (a few numbers per
+ * nucleus, passed to the kernels by value); every other pointer is device memory. */
+
+/* u, grad u (3 x N), f^2 and W = -|grad u|^2/2 with the 4^3 cell average within 2h (cusp.py:46-145).
+ * gl4 = four Gauss-Legendre offsets (times h/2) then their weights (times 1/2). */
+int cdftb_geometry_cusp_fields(int n_atoms, const double* charges, const double* positions, int nx, int ny, int nz,
+                               double ox, double oy, double oz, double spacing, const double* gl4, double* u,
+                               double* grad_u, double* f2, double* transformed_potential, int* n_averaged,
+                               cdftb_stream_t stream);
+/* f^2 at the staggered faces of each axis (cusp.py:168-214); *underflow set if u > 354. */
+int cdftb_geometry_face_weights(int n_atoms, const double* charges, const double* positions, int nx, int ny, int nz,
+                                double ox, double oy, double oz, double spacing, int accuracy, double* w0, double* w1,
+                                double* w2, int* underflow, cdftb_stream_t stream);
+/* Node partition P, weights = base P, f^2, grad u and W at the sphere nodes (quadrature.py:296-308,
+ * 360-419). spheres: per nucleus (centre xyz, radius, taper centre, taper width). */
+int cdftb_geometry_node_fields(int n_atoms, const double* charges, const double* positions, const double* spheres,
+                               double cell_width, const double* node_points, const int* owner,
+                               const double* base_weights, int64_t m, double* partition, double* weights,
+                               double* f2, double* grad_u, double* transformed_potential, cdftb_stream_t stream);
+/* far = prod_a (1 - p_a), far_w = h^3 far, plain_far = far_w f^2 on the grid (quadrature.py:312-319). */
+int cdftb_geometry_grid_far(int n_atoms, const double* charges, const double* positions, const double* spheres, int nx,
+                            int ny, int nz, double ox, double oy, double oz, double spacing, const double* f2,
+                            double* far, double* far_weights, double* plain_far, cdftb_stream_t stream);
+/* Lumped far mass weights of overlapping spheres on the refined lattice (quadrature.py:421-497). */
+int cdftb_geometry_lumped_far(int n_atoms, const double* charges, const double* positions, const double* spheres,
+                              int nx, int ny, int nz, double ox, double oy, double oz, double spacing, int refine,
+                              const double* fine_x, const double* fine_y, const double* fine_z, const double* mx,
+                              const int* lox, const int* hix, const double* my, const int* loy, const int* hiy,
+                              const double* mz, const int* loz, const int* hiz, const double* plain_far, double margin,
+                              double width, double* work, double* lumped_far, cdftb_stream_t stream);
+/* omega, W~/omega, h^3/omega and the measure from lifted = [lift(w f2), lift(w W f2)]
+ * (quadrature.py:327, 731-753); *nonpositive set if some omega <= 0. */
+int cdftb_geometry_bare_terms(const double* lifted, const double* far_mass, const double* far_weights,
+                              const double* transformed_potential, const double* f2, int64_t n_points, double spacing,
+                              double* mass, double* potential, double* inverse_weight, double* quadrature,
+                              int* nonpositive, cdftb_stream_t stream);
+/* exp(-2 Z_a s) and the 1s potential on the grid and at the nodes (step.py:154-156). */
+int cdftb_geometry_step_fields(int n_atoms, const double* charges, const double* positions, int nx, int ny, int nz,
+                               double ox, double oy, double oz, double spacing, const double* node_points, int64_t m,
+                               double* cusp_grid, double* v1s_grid, double* v1s_node, cdftb_stream_t stream);
+/* Hydrogenic superposition and its charge terms omega * total / f^2 (src/cdft/scf/loop.py:173-193). */
+int cdftb_geometry_initial_density(int n_atoms, const double* charges, const double* positions, int nx, int ny, int nz,
+                                   double ox, double oy, double oz, double spacing, double zeta_scale, const double* f2,
+                                   const double* mass, double* total, double* charge_terms, cdftb_stream_t stream);
+/* a <- s a. */
+int cdftb_scale_f64(double* a, int64_t n, double s, cdftb_stream_t stream);
 
 #ifdef __cplusplus
 }

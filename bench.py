@@ -44,6 +44,8 @@ def _args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("native", "reference"), default="native")
     p.add_argument("--form", choices=("mixed", "fp64"), default="mixed")
+    p.add_argument("--batch", type=int, default=None,
+                   help="systems solved together per GPU (default 32 for the mixed form, 1 for fp64)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--kernel-only", action="store_true",
                    help="time only the fused Chebyshev step on a He grid of --edge points (for profiling)")
@@ -150,6 +152,34 @@ def filter_step_roofline(pkg, dev, grid, hamiltonian, m: int, precision, reps: i
     per_launch_s = total / (reps * degree)
     s_bytes = 4 if precision == torch.float32 else 8
     algorithmic = grid.n_points * s_bytes * (3 * m + 5)
+    return per_launch_s, algorithmic
+
+
+def batched_filter_roofline(pkg, dev, grid, bham, m: int, precision, reps: int = 5, degree: int = 20):
+    """Average device time of one fused Chebyshev step over a batch of systems (m orbitals each)."""
+    import torch
+
+    b = bham.batch
+    block = torch.randn((b, m, grid.n_points), dtype=torch.float64, device=dev)
+    rows = [pkg.chebyshev_coefficients(degree, 1.0, 100.0, -3.0)] * b
+    table = torch.tensor(rows, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
+    for _ in range(2):
+        bham.filter(block, table, degree)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    total = 0.0
+    for _ in range(reps):
+        flush.fill_(1.0)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        bham.filter(block, table, degree)
+        end.record(stream)
+        end.synchronize()
+        total += start.elapsed_time(end) / 1e3
+    per_launch_s = total / (reps * degree)
+    s_bytes = 4 if precision == torch.float32 else 8
+    algorithmic = grid.n_points * s_bytes * (3 * b * m + b + 4)
     return per_launch_s, algorithmic
 
 
@@ -274,14 +304,27 @@ def main() -> None:
     grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev)
     geometry = pkg.build_cusp_geometry(grid, system.charges, system.positions)
     precision = torch.float32 if args.form == "mixed" else torch.float64
-    step = pkg.KohnShamStep(geometry, "lda_vwn", system.n_electrons, filter_precision=precision)
+    batch = args.batch if args.batch is not None else (32 if args.form == "mixed" else 1)
     mixing = pkg.MixingConfig(scheme="linear", alpha=0.3)
     golden = _golden()
-    n0 = pkg.initial_density(step)
     flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
+    if batch == 1:
+        step = pkg.KohnShamStep(geometry, "lda_vwn", system.n_electrons, filter_precision=precision)
+        n0 = pkg.initial_density(step)
 
-    def solve(initial):
-        return pkg.solve_self_consistent(step, mixing, initial_density_override=initial)
+        def solve(initial):
+            out = pkg.solve_self_consistent(step, mixing, initial_density_override=initial)
+            return [out.energies["total"]], out.density, out.scf_iterations, out.applications
+    else:
+        # independent systems: the same atom from different seeded random starts (seed = rank * batch + b)
+        seeds = [rank * batch + k for k in range(batch)]
+        step = pkg.batch.BatchedKohnShamStep(geometry, "lda_vwn", system.n_electrons, batch, seeds=seeds,
+                                             filter_precision=precision)
+        n0 = step.initial_density()
+
+        def solve(initial):
+            out = pkg.batch.solve_self_consistent_batch(step, mixing, initial_density=initial)
+            return ([e["total"] for e in out.energies], out.density, max(out.scf_iterations), out.applications)
 
     for _ in range(max(0, args.warmup)):
         solve(n0)
@@ -297,15 +340,16 @@ def main() -> None:
     total_ms = 0.0
     energies = []
     stream = torch.cuda.current_stream()
+    iterations = applications = None
     for _ in range(args.steps):
         flush.fill_(1.0)
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
-        out = solve(n0)
+        totals, _, iterations, applications = solve(n0)
         end.record(stream)
         end.synchronize()
         total_ms += start.elapsed_time(end)
-        energies.append(out.energies["total"])
+        energies.extend(totals)
     torch.cuda.synchronize()
     launches = lib.cdftb_launch_count() - launches0
     if dist is not None:
@@ -316,12 +360,12 @@ def main() -> None:
         t = torch.tensor([seconds], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         seconds = float(t.item())
-    value = world * args.steps / seconds
+    value = world * batch * args.steps / seconds
     error = max(abs(e - golden["total"]) for e in energies)
 
     # --- end to end through the public API with host buffers ---
     host_in = n0.cpu().pin_memory()
-    host_out = torch.empty_like(n0, device="cpu").pin_memory()
+    host_out = torch.empty(n0.shape, dtype=torch.float64).pin_memory()
     e2e_ms = 0.0
     e2e_steps = max(1, min(args.steps, 2))
     for _ in range(e2e_steps):
@@ -329,8 +373,8 @@ def main() -> None:
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
         dev_in = host_in.to(dev, non_blocking=True)
-        out = solve(dev_in)
-        host_out.copy_(out.density, non_blocking=True)
+        _, density, _, _ = solve(dev_in)
+        host_out.copy_(density.reshape(host_out.shape), non_blocking=True)
         end.record(stream)
         end.synchronize()
         e2e_ms += start.elapsed_time(end)
@@ -339,13 +383,18 @@ def main() -> None:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = world * e2e_steps / e2e_s
+    e2e_value = world * batch * e2e_steps / e2e_s
     bytes_in = host_in.numel() * host_in.element_size()
-    bytes_out = host_out.numel() * host_out.element_size() + 8 * 12
+    bytes_out = host_out.numel() * host_out.element_size() + 8 * 12 * batch
 
-    # --- roofline of the dominant kernel: one fused Chebyshev step (apply + recurrence) ---
-    ham = step.hamiltonian(step.potentials(n0), dtype=precision)
-    per_launch_s, algorithmic = filter_step_roofline(pkg, dev, grid, ham, 5, precision)
+    # --- roofline of the dominant kernel: one fused Chebyshev step (apply + recurrence) over the batch ---
+    effective = (step.potentials(n0).effective if batch == 1 else step.potentials(n0).effective)
+    if batch == 1:
+        ham = step.hamiltonian(step.potentials(n0), dtype=precision)
+        per_launch_s, algorithmic = filter_step_roofline(pkg, dev, grid, ham, 5, precision)
+    else:
+        bham = step.hamiltonian(effective, dtype=precision)
+        per_launch_s, algorithmic = batched_filter_roofline(pkg, dev, grid, bham, 5, precision)
     achieved = algorithmic / per_launch_s / 1e9
     peak, peak_kind = _peaks()
     tag = "f32" if precision == torch.float32 else "f64"
@@ -355,14 +404,16 @@ def main() -> None:
         "ms_per_step": seconds * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32-filter/f64" if precision == torch.float32 else "f64",
         "data": "synthetic (the He atom system itself; no dataset)",
-        "config": {"workload": "He-LDA 65^3 SCF solve (box 16 bohr, h 0.25, linear mixing 0.3), one system per GPU",
-                   "form": args.form, "l2": "flushed (256 MiB write) before every step",
+        "config": {"workload": "He-LDA 65^3 SCF solve (box 16 bohr, h 0.25, linear mixing 0.3)",
+                   "form": args.form, "systems_per_gpu": batch, "l2": "flushed (256 MiB write) before every step",
                    "parallelism": f"replicas{world}", "energy_error_vs_reference_cpu_fp64_ha": error,
-                   "scf_iterations": out.scf_iterations, "applications_per_solve": out.applications},
+                   "scf_iterations": iterations, "applications_per_step": applications},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_in, "d2h_bytes_per_step": bytes_out},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": _profile_traffic(tag), "kernel": f"stencil_kernel<{tag}> (one Chebyshev step, m=5)",
+                     "traffic": _profile_traffic(tag),
+                     "kernel": f"stencil_kernel<{tag}> (one Chebyshev step, {batch} systems x 5 orbitals)",
+                     "algorithmic_bytes_per_launch": algorithmic, "us_per_launch": per_launch_s * 1e6,
                      "peak_kind": peak_kind},
         "clocks": clocks,
     }

@@ -1,0 +1,709 @@
+"""Many independent systems in one set of launches: the batched SCF.
+
+B systems that share one geometry (one grid, one set of nuclei; e.g. an ensemble of seeded starts or
+perturbed runs) advance in lockstep: every field operation of an SCF iteration is one library call
+over all B systems (the stencil launches B x m orbitals with one potential and one Chebyshev
+coefficient table per system; the reductions, small dense steps, Poisson passes, interpolant, lift
+and assembly kernels all carry a system index), while the control flow -- bounds reuse, eigensolver
+stop tests, mixers, fallback ladder, convergence -- is kept per system on the host exactly as in
+``src/cdft/scf/loop.py`` and ``src/cdft/eigen/chefsi.py``. A system that has converged leaves the
+active set: later launches run on the compacted remainder, so its result is the one a solve of that
+system alone gives. The host reads a handful of scalars per system once per eigensolver iteration
+and once per SCF iteration, in one transfer for the whole batch.
+
+Spin-restricted LDA; the GGA potentials and the level-shift rung of the fallback ladder run in the
+single-system driver (:mod:`.scf`).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import F32, F64, call, ptr, stream_handle
+from .eigen import BOUND_REUSE_RITZ_FRACTION, EigenConfig, chebyshev_coefficients
+from .geometry import CuspGeometry, gradient, row_sums
+from .operators import cast, measure_cross, rowwise_inner
+from .poisson import CoulombCutoffPoisson
+from .rng import SeededStream
+from .scf import (FILTER_STEPS_PER_ITERATION, BoundReusePolicy, LinearMixer, MixingConfig, PulayMixer, SCFConfig,
+                  aufbau_occupations, nuclear_repulsion)
+from .xc import functional_by_name
+
+
+class BatchedHamiltonian:
+    """``A`` on B systems of one geometry: B diagonal potentials, blocks ``(B, k, N)``."""
+
+    def __init__(self, grid, factor, quadrature, potentials: torch.Tensor, dtype=torch.float64):
+        self.grid = grid
+        self.quadrature = quadrature
+        self.dtype = dtype
+        self.potentials = potentials.contiguous()  # (B, N) float64
+        faces = factor.face_weights(grid.fd_order)
+        inv = quadrature.bare_operator_terms()[1]
+        if dtype == torch.float64:
+            self._faces = tuple(f.contiguous() for f in faces)
+            self._inv = inv
+            self._pot = self.potentials
+        else:
+            cache = factor.__dict__.setdefault("_cast_cache", {})
+            key = (dtype, inv.data_ptr())
+            if key not in cache:
+                cache[key] = (tuple(cast(f.contiguous(), dtype) for f in faces), cast(inv.contiguous(), dtype))
+            self._faces, self._inv = cache[key]
+            self._pot = cast(self.potentials, dtype)
+        self.q = quadrature.bare_operator_terms()[2].quadrature
+        self.applications = 0
+
+    @property
+    def batch(self) -> int:
+        return self.potentials.shape[0]
+
+    def _op(self, k: int) -> _lib.Operator:
+        op = _lib.Operator()
+        op.nx, op.ny, op.nz = self.grid.shape
+        op.accuracy = self.grid.fd_order
+        op.spacing = self.grid.spacing
+        op.dtype = F64 if self.dtype == torch.float64 else F32
+        op.face_weights = (ctypes.c_void_p * 3)(*(f.data_ptr() for f in self._faces))
+        op.inverse_weight = self._inv.data_ptr()
+        op.potential = self._pot.data_ptr()
+        op.potential_stride = self.grid.n_points
+        op.orbitals_per_group = int(k)
+        op.quadrature = self.q.data_ptr()
+        return op
+
+    def apply(self, phi: torch.Tensor, kinetic_only: bool = False) -> torch.Tensor:
+        """``A phi`` for ``(B, k, N)`` orbitals (system b uses potential b)."""
+        x = phi.contiguous()
+        if x.dtype != self.dtype:
+            x = cast(x, self.dtype)
+        k = x.shape[1]
+        out = torch.empty_like(x)
+        op = self._op(k)
+        call("cdftb_cusp_apply", ctypes.byref(op), ptr(x), _lib.dtype_code(x), ptr(out), _lib.dtype_code(out),
+             x.shape[0] * k, 1 if kinetic_only else 0, stream_handle(x.device))
+        if not kinetic_only:
+            self.applications += 1
+        return out
+
+    def filter(self, block: torch.Tensor, table: torch.Tensor, degree: int) -> torch.Tensor:
+        """The fused Chebyshev filter on ``(B, k, N)`` float64 blocks, one coefficient table per system."""
+        x = block.contiguous()
+        b, k, n = x.shape
+        out = torch.empty_like(x)
+        work = torch.empty((3, b * k, n), dtype=self.dtype, device=x.device)
+        op = self._op(k)
+        call("cdftb_chebyshev_filter", ctypes.byref(op), ptr(x), _lib.dtype_code(x), ptr(out), _lib.dtype_code(out),
+             ptr(work), b * k, ptr(table.contiguous()), degree, stream_handle(x.device))
+        self.applications += degree
+        return out
+
+    def subset(self, index: list[int]) -> "BatchedHamiltonian":
+        sub = BatchedHamiltonian.__new__(BatchedHamiltonian)
+        sub.__dict__.update(self.__dict__)
+        idx = torch.tensor(index, dtype=torch.long, device=self.potentials.device)
+        sub.potentials = self.potentials.index_select(0, idx).contiguous()
+        sub._pot = sub.potentials if self.dtype == torch.float64 else cast(sub.potentials, self.dtype)
+        sub.applications = 0
+        return sub
+
+
+class _RitzBuffers:
+    def __init__(self):
+        self._key = None
+
+    def get(self, b, m, device):
+        if self._key != (b, m, str(device)):
+            f = dict(dtype=torch.float64, device=device)
+            self.lower = torch.empty((b, m, m), **f)
+            self.info = torch.empty(b, dtype=torch.int32, device=device)
+            self.evals = torch.empty((b, m), **f)
+            self.rot = torch.empty((b, m, m), **f)
+            self._key = (b, m, str(device))
+        return self
+
+
+_RB = _RitzBuffers()
+
+
+def batched_rayleigh_ritz(h: BatchedHamiltonian, block: torch.Tensor):
+    """Rayleigh--Ritz for every system (``src/cdft/eigen/rayleigh_ritz.py:51-115``), one call per step.
+
+    Returns ``(evals (B, m), vectors (B, m, N), residual norms (B, m), orth error (B), cholesky info (B))``;
+    the residual uses ``U^T (A Q)`` (U orthogonal) instead of a second apply.
+    """
+    b, m, n = block.shape
+    dev = block.device
+    stream = stream_handle(dev)
+    q = h.q
+    flat = block.to(torch.float64).contiguous()
+    gram = measure_cross(flat, flat, q, b)
+    rb = _RB.get(b, m, dev)
+    call("cdftb_small_cholesky_f64", ptr(gram), ptr(rb.lower), ptr(rb.info), m, b, stream)
+    basis = torch.empty_like(flat)
+    call("cdftb_block_trsm_lower_f64", ptr(rb.lower), ptr(flat), m * n, ptr(basis), F64, m * n, m, n, b, stream)
+    applied = h.apply(basis)
+    sub = measure_cross(basis, applied, q, b)
+    call("cdftb_small_eigh_f64", ptr(sub), ptr(rb.evals), ptr(rb.rot), m, b, stream)
+    vectors = torch.empty_like(flat)
+    call("cdftb_block_rotate_f64", ptr(rb.rot), ptr(basis), m * n, ptr(vectors), F64, m * n, m, m, n, b, stream)
+    rot_applied = torch.empty_like(flat)
+    call("cdftb_block_rotate_f64", ptr(rb.rot), ptr(applied), m * n, ptr(rot_applied), F64, m * n, m, m, n, b, stream)
+    g2 = measure_cross(vectors, vectors, q, b)
+    eye = torch.eye(m, dtype=torch.float64, device=dev)
+    orth = (g2 - eye).abs().amax(dim=(1, 2))
+    evals = rb.evals.clone()
+    res = torch.empty_like(flat)
+    call("cdftb_block_residual_f64", ptr(rot_applied), ptr(vectors), ptr(evals), ptr(res), m, n, b, m * n, stream)
+    norms = rowwise_inner(res.reshape(b * m, n), res.reshape(b * m, n), q).reshape(b, m).clamp_min(0.0).sqrt()
+    return evals, vectors, norms, orth, rb.info.clone()
+
+
+def batched_lanczos(h: BatchedHamiltonian, starts: torch.Tensor, steps: int, safety: float) -> list[tuple[float, float]]:
+    """The Lanczos enclosure (``src/cdft/operators/hamiltonian.py:29-89``) for every system at once."""
+    b, n = starts.shape
+    q = h.q
+    dev = starts.device
+    stream = stream_handle(dev)
+    v = starts.to(torch.float64).clone().contiguous()
+    nrm = rowwise_inner(v, v, q).clamp_min(0.0).contiguous()
+    call("cdftb_lanczos_update_f64", 2, ptr(v), None, None, ptr(nrm), None, n, b, stream)
+    v_prev = torch.zeros_like(v)
+    beta_prev = torch.zeros(b, dtype=torch.float64, device=dev)
+    alphas, betas = [], []
+    for _ in range(steps):
+        w = h.apply(v.reshape(b, 1, n)).reshape(b, n).contiguous()
+        alpha = rowwise_inner(v, w, q).contiguous()
+        call("cdftb_lanczos_update_f64", 0, ptr(w), ptr(v), ptr(v_prev), ptr(alpha), ptr(beta_prev), n, b, stream)
+        c1 = rowwise_inner(w, v, q).contiguous()
+        c2 = rowwise_inner(w, v_prev, q).contiguous()
+        call("cdftb_lanczos_update_f64", 1, ptr(w), ptr(v), ptr(v_prev), ptr(c1), ptr(c2), n, b, stream)
+        wsq = rowwise_inner(w, w, q).clamp_min(0.0).contiguous()
+        beta = wsq.sqrt()
+        alphas.append(alpha)
+        betas.append(beta)
+        call("cdftb_lanczos_update_f64", 2, ptr(w), None, None, ptr(wsq), None, n, b, stream)
+        v_prev, v = v, w
+        beta_prev = beta
+    values = torch.stack([*alphas, *betas]).cpu().numpy()  # (2 steps, b)
+    out = []
+    for s in range(b):
+        a = list(values[:steps, s])
+        bt = list(values[steps:, s])
+        for index, value in enumerate(bt):
+            if value < 1e-12:
+                del a[index + 1:], bt[index + 1:]
+                break
+        size = len(a)
+        tri = np.zeros((size, size))
+        for i in range(size):
+            tri[i, i] = a[i]
+            if i + 1 < size:
+                tri[i, i + 1] = tri[i + 1, i] = bt[i]
+        ritz = np.linalg.eigvalsh(tri)
+        residual = bt[-1] if bt else 0.0
+        lo, hi = float(ritz[0]) - residual, float(ritz[-1]) + residual
+        centre, half = 0.5 * (hi + lo), 0.5 * (hi - lo) * safety
+        out.append((centre - half, centre + half))
+    return out
+
+
+@dataclass
+class _EigenState:
+    spectrum: tuple | None = None
+    source: str = "unset"
+    shift: float = 0.0
+    next_lower: float = 0.0
+    previous: np.ndarray | None = None
+    top_fraction: float = float("-inf")
+    converged: bool = False
+    iterations: int = 0
+    stop_reason: str = "iteration limit"
+    float_filter: bool = False
+
+
+def _fraction(value, low, high):
+    width = high - low
+    return (value - low) / width if width > 0.0 else float("inf")
+
+
+def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_states: int, config: EigenConfig,
+                   initial: torch.Tensor | None, streams: list[SeededStream], bounds: list, max_iterations: int,
+                   switch_residual: float | None):
+    """CheFSI for every system of ``h`` (``src/cdft/eigen/chefsi.py:442-585``, ``ritz_stop=False``).
+
+    ``bounds[b]`` is ``None`` (run Lanczos) or ``(lower, upper, shift)``. Returns per-system
+    eigenvalues ``(B, n_states)``, eigenvectors ``(B, n_states, N)``, residuals ``(B, n_states)``,
+    and the per-system states (bounds used, source, iterations, stop reason).
+    """
+    b = h.batch
+    n = h.grid.n_points
+    dev = h.potentials.device
+    extra = max(config.n_extra_states, int(config.extra_states_fraction * n_states))
+    m = min(n_states + extra, n)
+    blocks = []
+    for s in range(b):
+        if initial is None:
+            blocks.append(streams[s].randn((m, n)))
+        else:
+            blk = initial[s].to(torch.float64).reshape(-1, n)
+            if blk.shape[0] < m:
+                blk = torch.cat([blk, streams[s].randn((m - blk.shape[0], n))], dim=0)
+            blocks.append(blk)
+    block = torch.stack(blocks)
+    states = [_EigenState(float_filter=h32 is not None) for _ in range(b)]
+    need = [s for s in range(b) if bounds[s] is None]
+    if need:
+        starts = torch.stack([streams[s].randn(n) for s in need])
+        sub = h if len(need) == b else h.subset(need)
+        for s, bb in zip(need, batched_lanczos(sub, starts, config.lanczos_steps, config.bound_safety)):
+            states[s].spectrum = bb
+            states[s].source = "lanczos"
+        h.applications += sub.applications if sub is not h else 0
+    evals, vectors, residual, _, _ = batched_rayleigh_ritz(h, block)
+    top = m - 1
+    tops = evals[:, top].tolist()
+    for s in range(b):
+        st = states[s]
+        st.next_lower = tops[s]
+        if bounds[s] is not None:
+            lo, hi, shift = bounds[s]
+            st.spectrum = (lo - shift, hi + shift)
+            st.source = "reused"
+            st.shift = shift
+    previous = evals.clone()
+    out_evals = evals.clone()
+    out_vectors = vectors.clone()
+    out_res = residual.clone()
+    active = list(range(b))
+    for iteration in range(1, max_iterations + 1):
+        # per-system filter intervals (and a fresh Lanczos where a carried bound is rejected)
+        redo = []
+        for s in active:
+            st = states[s]
+            lower = st.next_lower
+            lo, hi = st.spectrum
+            frac = _fraction(lower, lo, hi)
+            if st.source == "reused" and not frac < BOUND_REUSE_RITZ_FRACTION:
+                redo.append(s)
+        if redo:
+            starts = torch.stack([streams[s].randn(n) for s in redo])
+            sub = h.subset(redo)
+            for s, bb in zip(redo, batched_lanczos(sub, starts, config.lanczos_steps, config.bound_safety)):
+                states[s].spectrum = bb
+                states[s].source = "lanczos (reuse rejected)"
+            h.applications += sub.applications
+        rows = []
+        use_float = []
+        for s in active:
+            st = states[s]
+            lo, hi = st.spectrum
+            lower = st.next_lower
+            st.top_fraction = max(st.top_fraction, _fraction(lower, lo, hi))
+            lower = min(max(lower, lo + 1e-8), hi - 1e-8)
+            rows.append(chebyshev_coefficients(config.chebyshev_degree, lower, hi, lo))
+            use_float.append(st.float_filter)
+        table = torch.tensor(rows, dtype=torch.float64).pin_memory().to(dev, non_blocking=True)
+        full = len(active) == b
+        sel = None if full else torch.tensor(active, dtype=torch.long, device=dev)
+        hv = h if full else h.subset(active)
+        cur = vectors if full else vectors.index_select(0, sel)
+        # float filter while every active system is still in its float phase (the batch shares a launch)
+        if h32 is not None and all(use_float):
+            hf = h32 if full else h32.subset(active)
+            filtered = hf.filter(cur, table, config.chebyshev_degree)
+        else:
+            filtered = hv.filter(cur, table, config.chebyshev_degree)
+        ev, vec, res, orth, info = batched_rayleigh_ritz(hv, filtered)
+        prev = previous if full else previous.index_select(0, sel)
+        drift = (ev[:, :n_states] - prev[:, :n_states]).abs().amax(dim=1)
+        worst = res[:, :n_states].amax(dim=1)
+        host = torch.stack([worst, drift, orth, ev[:, top], info.to(torch.float64)]).cpu().numpy()
+        if (host[4] != 0).any():
+            raise RuntimeError("a filtered block lost rank (Cholesky failed) in the batched solver; "
+                               "solve that system with the single-system driver")
+        if full:
+            vectors, evals, residual = vec, ev, res
+        else:
+            vectors = vectors.index_copy(0, sel, vec)
+            evals = evals.index_copy(0, sel, ev)
+            residual = residual.index_copy(0, sel, res)
+        previous = evals.clone()
+        still = []
+        done = []
+        for j, s in enumerate(active):
+            st = states[s]
+            st.iterations = iteration
+            st.next_lower = float(host[3, j])
+            if host[0, j] < config.residual_tol:
+                st.converged = True
+                st.stop_reason = "residual below residual_tol"
+                done.append(s)
+            else:
+                still.append(s)
+            if st.float_filter and switch_residual is not None and host[0, j] < switch_residual:
+                st.float_filter = False
+        if done:
+            idx = torch.tensor(done, dtype=torch.long, device=dev)
+            out_evals = out_evals.index_copy(0, idx, evals.index_select(0, idx))
+            out_vectors = out_vectors.index_copy(0, idx, vectors.index_select(0, idx))
+            out_res = out_res.index_copy(0, idx, residual.index_select(0, idx))
+        active = still
+        if not active:
+            break
+    if active:
+        idx = torch.tensor(active, dtype=torch.long, device=dev)
+        out_evals = out_evals.index_copy(0, idx, evals.index_select(0, idx))
+        out_vectors = out_vectors.index_copy(0, idx, vectors.index_select(0, idx))
+        out_res = out_res.index_copy(0, idx, residual.index_select(0, idx))
+    return (out_evals[:, :n_states].contiguous(), out_vectors[:, :n_states].contiguous(),
+            out_res[:, :n_states].contiguous(), states)
+
+
+@dataclass
+class BatchedPotentials:
+    effective: torch.Tensor        # (B, N)
+    v_hartree: torch.Tensor        # (B, N)
+    hartree_energy: torch.Tensor   # (B,)
+    xc_energy: torch.Tensor        # (B,)
+    xc_double_counting: torch.Tensor  # (B,)
+
+
+class BatchedKohnShamStep:
+    """The KS map for B systems sharing one geometry (``src/cdft/scf/step.py`` semantics per system)."""
+
+    FLOAT_FILTER_SWITCH_RESIDUAL = 1.0e-4
+
+    def __init__(self, geometry: CuspGeometry, functional: str, n_electrons: float, batch: int,
+                 eigen: EigenConfig | None = None, *, seeds=None, pad_factor: float = 2.5,
+                 filter_precision: torch.dtype = torch.float64) -> None:
+        self.geometry = geometry
+        self.grid = geometry.grid
+        self.factor = geometry.factor
+        self.quadrature = geometry.quadrature
+        self.functional = functional_by_name(functional)
+        if self.functional.rung != 1:
+            raise NotImplementedError("the batched driver runs LDA; use the single-system driver for a GGA")
+        self.batch = int(batch)
+        self.n_electrons = float(n_electrons)
+        self.n_states = max(1, int(-(-self.n_electrons // 2.0)))
+        self.eigen = eigen or EigenConfig()
+        self.seeds = list(seeds) if seeds is not None else list(range(self.batch))
+        if len(self.seeds) != self.batch:
+            raise ValueError("one seed per system")
+        self.ion_ion = nuclear_repulsion(geometry.charges, geometry.positions)
+        self.poisson = CoulombCutoffPoisson(self.grid, pad_factor=pad_factor, max_batch=self.batch)
+        self.filter_precision = filter_precision
+        self.f2 = self.factor.weight
+        self.bare_potential = self.quadrature.bare_operator_terms()[0]
+        self.occ = torch.from_numpy(aufbau_occupations(self.n_states, self.n_electrons)[0]).to(self.grid.device)
+
+    def potentials(self, density: torch.Tensor) -> BatchedPotentials:
+        """(``src/cdft/scf/step.py:224-313``) for ``(B, N)`` total densities, LDA."""
+        g = self.geometry
+        q = self.quadrature
+        grid = self.grid
+        n = grid.n_points
+        m = q.n_nodes
+        na = len(g.charges)
+        b = density.shape[0]
+        dev = grid.device
+        stream = stream_handle(dev)
+        f = dict(dtype=torch.float64, device=dev)
+        n_grid = density.to(torch.float64).contiguous()
+        fields = torch.empty((2, b, n), **f)  # [rho | v_smooth]
+        rho = fields[0]
+        n_smooth = torch.empty((b, n), **f)
+        call("cdftb_hartree_split_f64", ptr(n_grid), ptr(self.f2), None, None, 0, n, b, ptr(rho), ptr(n_smooth), stream)
+        rho_nuc = torch.empty((b, na), **f)
+        call("cdftb_quadrature_interpolate_f64", ptr(g.step.nuclei_base), ptr(g.step.nuclei_w1d), na, *grid.shape,
+             ptr(rho), b, n, ptr(rho_nuc), na, stream)
+        coef = torch.empty((b, na), **f)
+        call("cdftb_cusp_coefficients_f64", ptr(rho_nuc), ptr(g.step.nucleus_f2), ptr(g.step.overlap), na, b,
+             ptr(coef), stream)
+        call("cdftb_hartree_split_f64", ptr(n_grid), ptr(self.f2), ptr(g.step.cusp_grid), ptr(coef), na, n, b,
+             ptr(rho), ptr(n_smooth), stream)
+        self.poisson.solve_batch(n_smooth, out=fields[1])
+        node = torch.empty((2, b, m), **f)
+        call("cdftb_quadrature_interpolate_f64", ptr(q.base), ptr(q.w1d), m, *grid.shape, ptr(fields), 2 * b, n,
+             ptr(node), m, stream)
+        lift_in = torch.empty((b, 2, m), **f)
+        e_w = torch.empty((b, m), **f)
+        call("cdftb_potentials_node_lda_f64", ptr(node), m, ptr(q.weights), ptr(q.f2), ptr(g.step.v1s_node),
+             ptr(coef), na, b, ptr(lift_in), ptr(e_w), stream)
+        lifted = q._lift_raw(lift_in, 2 * b)
+        effective = torch.empty((b, n), **f)
+        v_hartree = torch.empty((b, n), **f)
+        terms = torch.empty((b, 3, n), **f)
+        call("cdftb_potentials_grid_lda_f64", ptr(n_grid), ptr(rho), ptr(self.f2), ptr(q.far_weights),
+             ptr(q.mass_weights), ptr(fields[1]), ptr(g.step.v1s_grid), ptr(coef), na, ptr(lifted), n, b,
+             ptr(effective), ptr(v_hartree), ptr(terms), None, stream)
+        sums = row_sums(terms)  # (b, 3)
+        node_sum = row_sums(e_w)  # (b,)
+        return BatchedPotentials(effective=effective, v_hartree=v_hartree, hartree_energy=0.5 * sums[:, 0],
+                                 xc_energy=node_sum + sums[:, 2], xc_double_counting=sums[:, 1])
+
+    def hamiltonian(self, effective: torch.Tensor, dtype=torch.float64) -> BatchedHamiltonian:
+        return BatchedHamiltonian(self.grid, self.factor, self.quadrature, self.bare_potential[None, :] + effective,
+                                  dtype=dtype)
+
+    def output_density(self, vectors: torch.Tensor):
+        rho_out = (self.occ[None, :, None] * vectors.pow(2)).sum(dim=1)  # (B, N)
+        return rho_out * self.f2[None, :], rho_out
+
+    def external_parts(self, rho: torch.Tensor):
+        """``((1/2)Q[f^2 grad rho . grad u], Q[f^2 rho W])`` per system (hamiltonian.py:557-574)."""
+        q = self.quadrature
+        factor = self.factor
+        b, n = rho.shape
+        grad = gradient(self.grid, rho)  # (B, 3, N)
+        fields = torch.cat([rho[:, None], grad], dim=1).contiguous()  # (B, 4, N)
+        node = q.interpolate(fields)  # (B, 4, M)
+        rho_node, grad_node = node[:, 0], node[:, 1:]
+        cross_node = q.f2[None] * (grad_node * q.grad_u[None]).sum(dim=1)
+        cross_grid = factor.weight[None] * (grad * factor.grad_u[None]).sum(dim=1)
+        cross = 0.5 * (row_sums(q.weights[None] * cross_node) + row_sums(q.far_weights[None] * cross_grid))
+        pot = (row_sums(q.weights[None] * (q.f2[None] * rho_node * q.transformed_potential[None]))
+               + row_sums(q.far_weights[None] * (factor.weight[None] * rho * factor.transformed_potential[None])))
+        return cross, pot
+
+    def energy_terms(self, evals, vectors, rho_out, p_in: BatchedPotentials, p_out: BatchedPotentials):
+        """(``src/cdft/scf/step.py:398-439``) per system, as (B,) device tensors."""
+        q = self.quadrature
+        b, k, n = vectors.shape
+        band = (self.occ[None] * evals).sum(dim=1)
+        h = BatchedHamiltonian(self.grid, self.factor, self.quadrature,
+                               self.bare_potential[None].expand(b, n).contiguous())
+        kin = h.apply(vectors, kinetic_only=True)
+        kinetic_form = rowwise_inner(vectors.reshape(b * k, n), kin.reshape(b * k, n), h.q).reshape(b, k)
+        first = (self.occ[None] * kinetic_form).sum(dim=1)
+        cross, pot = self.external_parts(rho_out)
+        kinetic = first - cross - pot
+        dc_out = row_sums(p_in.effective * q.mass_weights[None] * rho_out)
+        kpe = band - dc_out
+        harris = band - p_in.hartree_energy - p_in.xc_double_counting + p_in.xc_energy + self.ion_ion
+        total = kpe + p_out.hartree_energy + p_out.xc_energy + self.ion_ion
+        external = total - kinetic - p_out.hartree_energy - p_out.xc_energy - self.ion_ion
+        return {"total": total, "kinetic": kinetic, "external": external, "hartree": p_out.hartree_energy,
+                "xc": p_out.xc_energy, "harris_foulkes": harris, "band": band, "external_direct": cross + 2.0 * pot}
+
+    def initial_density(self) -> torch.Tensor:
+        from .scf import KohnShamStep, initial_density
+
+        one = initial_density(_InitialDensityView(self))
+        return one.expand(self.batch, -1).contiguous()
+
+
+class _InitialDensityView:
+    """The attributes :func:`scf.initial_density` reads, taken from a batched step."""
+
+    def __init__(self, step: BatchedKohnShamStep):
+        self.geometry = step.geometry
+        self.grid = step.grid
+        self._f2_grid = step.f2
+        self.quadrature = step.quadrature
+        self.n_electrons = step.n_electrons
+
+
+@dataclass
+class _SystemState:
+    mixer: object
+    policy: BoundReusePolicy
+    rung: int = 0
+    worsened: int = 0
+    previous_residual: float = float("inf")
+    energies: list = field(default_factory=list)
+    residuals: list = field(default_factory=list)
+    converged: bool = False
+    iterations: int = 0
+    applications: int = 0
+    float_phase: bool = False
+    refinement_from: int | None = None
+    rung_changed: bool = False
+    fallback_events: list = field(default_factory=list)
+
+
+@dataclass
+class BatchedOutcome:
+    energies: list            # per system dict of floats
+    eigenvalues: list         # per system list
+    scf_iterations: list
+    converged: list
+    applications: float
+    density: torch.Tensor     # (B, N)
+    measurements: dict = field(default_factory=dict)
+
+
+def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig | None = None,
+                                scf: SCFConfig | None = None, *, initial_density: torch.Tensor | None = None,
+                                max_iterations: int | None = None) -> BatchedOutcome:
+    """``src/cdft/scf/loop.py:255-550`` for B systems at once (see the module docstring).
+
+    With ``step.filter_precision == torch.float32`` each system filters in float until it meets the
+    convergence test, then refines in float64 until the test passes again (the FP64 refinement
+    sweep); the final full diagonalisation filters in float64.
+    """
+    started = time.perf_counter()
+    mixing = mixing or MixingConfig()
+    scf = scf or SCFConfig()
+    b = step.batch
+    dev = step.grid.device
+    q = step.quadrature
+    mass, f2 = q.mass_weights, step.f2
+    inner_weights = (mass / f2 ** 2).contiguous()
+    mixed = step.filter_precision == torch.float32
+
+    def make(alpha, scheme=None):
+        scheme = scheme or mixing.scheme
+        if scheme == "linear":
+            return LinearMixer(alpha)
+        period = mixing.pulay_period if scheme == "periodic_pulay" else 1
+        return PulayMixer(alpha, mixing.history, period, inner_weights)
+
+    systems = [_SystemState(mixer=make(mixing.alpha), policy=BoundReusePolicy(), float_phase=mixed) for _ in range(b)]
+    n_in = (initial_density if initial_density is not None else step.initial_density()).to(torch.float64).clone()
+    if n_in.shape[0] != b:
+        n_in = n_in.expand(b, -1).contiguous()
+    initial_block = None
+    previous_effective = None
+    limit = scf.max_iterations if max_iterations is None else max_iterations
+    active = list(range(b))
+    last_p_in = [None] * b
+    last_vectors = [None] * b
+    p_in_all = None
+    for iteration in range(1, limit + 1):
+        if not active:
+            break
+        sel = torch.tensor(active, dtype=torch.long, device=dev)
+        full = len(active) == b
+        nin = n_in if full else n_in.index_select(0, sel)
+        p_in = step.potentials(nin)
+        h = step.hamiltonian(p_in.effective)
+        float_now = [systems[s].float_phase for s in active]
+        h32 = step.hamiltonian(p_in.effective, dtype=torch.float32) if all(float_now) else None
+        hints = []
+        shifts = None
+        if previous_effective is not None:
+            prev = previous_effective if full else previous_effective.index_select(0, sel)
+            shifts = (p_in.effective - prev).abs().amax(dim=1).tolist()
+        for j, s in enumerate(active):
+            st = systems[s]
+            reason = st.policy.decide(residual_rose=st.worsened > 0, rung_changed=st.rung_changed, level_shift=False)
+            if reason is None and shifts is not None:
+                hints.append((st.policy.bounds[0], st.policy.bounds[1], shifts[j]))
+            else:
+                hints.append(None)
+            st.policy._pending_reason = reason
+        streams = [SeededStream(step.seeds[s], dev) for s in active]
+        init = None if initial_block is None else (initial_block if full else initial_block.index_select(0, sel))
+        steps_cap = step.eigen.max_iterations if init is None else FILTER_STEPS_PER_ITERATION
+        switch = step.FLOAT_FILTER_SWITCH_RESIDUAL if init is None else None
+        h.applications = 0
+        evals, vectors, _, estates = batched_chefsi(h, h32, step.n_states, step.eigen, init, streams, hints, steps_cap,
+                                                    switch)
+        for j, s in enumerate(active):
+            st = systems[s]
+            es = estates[j]
+            info = {"eigen_spectral_bounds": list(es.spectrum), "eigen_top_ritz_fraction": es.top_fraction,
+                    "eigen_bounds_source": es.source, "eigen_bounds_shift": es.shift}
+            st.policy.observe(st.policy._pending_reason, info)
+            st.rung_changed = False
+        n_out, rho_out = step.output_density(vectors)
+        p_out = step.potentials(n_out)
+        terms = step.energy_terms(evals, vectors, rho_out, p_in, p_out)
+        residual = n_out - nin
+        res_norm = row_sums(mass[None] * (residual.abs() / f2[None]))
+        keys = list(terms)
+        host = torch.stack([*terms.values(), res_norm]).cpu().numpy()  # (len(keys)+1, S)
+        # mixing (per system: linear in one batched expression when all are linear)
+        n_next = torch.empty_like(nin)
+        for j, s in enumerate(active):
+            n_next[j] = systems[s].mixer.mix(nin[j:j + 1], n_out[j:j + 1], iteration)[0]
+        new_active = []
+        for j, s in enumerate(active):
+            st = systems[s]
+            st.iterations = iteration
+            st.applications += h.applications
+            total = float(host[keys.index("total"), j])
+            rn = float(host[-1, j])
+            st.energies.append(total)
+            st.residuals.append(rn)
+            de = abs(st.energies[-1] - st.energies[-2]) if len(st.energies) > 1 else float("inf")
+            last_p_in[s] = (p_in, j)
+            last_vectors[s] = vectors[j]
+            if iteration >= scf.min_iterations and de < scf.energy_tol and rn < scf.density_tol:
+                if st.float_phase:
+                    st.float_phase = False
+                    st.refinement_from = iteration + 1
+                else:
+                    st.converged = True
+                    continue
+            st.worsened = st.worsened + 1 if rn > st.previous_residual else 0
+            st.previous_residual = rn
+            if scf.fallback_ladder and st.worsened >= 3 and st.rung + 1 < 4:
+                st.rung += 1
+                if st.rung == 3:
+                    raise RuntimeError("the level-shift rung is not batched; solve this system with the "
+                                       "single-system driver")
+                st.mixer = make(0.5 * mixing.alpha) if st.rung == 1 else LinearMixer(0.5 * mixing.alpha)
+                st.fallback_events.append(f"iteration {iteration}: stepping down to rung {st.rung}")
+                st.worsened = 0
+                st.rung_changed = True
+                n_next[j] = nin[j] + 0.5 * mixing.alpha * residual[j]
+            new_active.append(s)
+        # write back the per-system state of this iteration
+        if full:
+            n_in = n_next
+            previous_effective = p_in.effective
+            initial_block = vectors
+        else:
+            n_in = n_in.index_copy(0, sel, n_next)
+            previous_effective = previous_effective.index_copy(0, sel, p_in.effective)
+            initial_block = initial_block.index_copy(0, sel, vectors)
+        if previous_effective is None:
+            previous_effective = p_in.effective
+        active = new_active
+    # final full diagonalisation of every system at its last input potential (fresh Lanczos, float64)
+    eff = torch.stack([last_p_in[s][0].effective[last_p_in[s][1]] for s in range(b)])
+    init = torch.stack([last_vectors[s] for s in range(b)])
+    h = step.hamiltonian(eff)
+    h.applications = 0
+    streams = [SeededStream(step.seeds[s], dev) for s in range(b)]
+    evals, vectors, residuals, estates = batched_chefsi(h, None, step.n_states, step.eigen, init, streams, [None] * b,
+                                                        step.eigen.max_iterations, None)
+    p_in_final = BatchedPotentials(
+        effective=eff,
+        v_hartree=torch.stack([last_p_in[s][0].v_hartree[last_p_in[s][1]] for s in range(b)]),
+        hartree_energy=torch.stack([last_p_in[s][0].hartree_energy[last_p_in[s][1]] for s in range(b)]),
+        xc_energy=torch.stack([last_p_in[s][0].xc_energy[last_p_in[s][1]] for s in range(b)]),
+        xc_double_counting=torch.stack([last_p_in[s][0].xc_double_counting[last_p_in[s][1]] for s in range(b)]))
+    n_out, rho_out = step.output_density(vectors)
+    p_out = step.potentials(n_out)
+    terms = step.energy_terms(evals, vectors, rho_out, p_in_final, p_out)
+    charge = row_sums(mass[None] * rho_out)
+    keys = list(terms)
+    host = torch.stack([*terms.values(), charge]).cpu().numpy()
+    ev = evals.cpu().numpy()
+    energies = [{k: float(host[i, s]) for i, k in enumerate(keys)} for s in range(b)]
+    final_converged = [bool(es.converged) for es in estates]
+    apps = sum(st.applications for st in systems) + h.applications
+    measurements = {
+        "batch": b,
+        "charge_error": [abs(float(host[-1, s]) - step.n_electrons) for s in range(b)],
+        "fp64_refinement_from_iteration": [st.refinement_from for st in systems],
+        "filter_precision": "float32" if mixed else "float64",
+        "energy_history": [st.energies for st in systems],
+        "fallbacks": [st.fallback_events for st in systems],
+        "fused_kernels": {"tier": "native-sm100a", "library": _lib.LIBRARY_PATH.name},
+        "wall_s": time.perf_counter() - started,
+    }
+    return BatchedOutcome(energies=energies, eigenvalues=[list(ev[s]) for s in range(b)],
+                          scf_iterations=[st.iterations for st in systems],
+                          converged=[st.converged and final_converged[s] for s, st in enumerate(systems)],
+                          applications=float(apps), density=n_out, measurements=measurements)

@@ -94,7 +94,8 @@ __global__ void hartree_split_kernel(const double* __restrict__ n, const double*
 
 // Node side of potentials(), LDA: x_H = w f2 vH, x_xc = w f2 v_xc (the lift inputs of the lumped
 // Hartree and XC weights) and e_w = w e_xc (the node part of the XC energy).
-// fields: [rho_node, vsmooth_node] (each m); outputs x [2][m], e_w [m].
+// fields: rho_node (batch x m) followed by vsmooth_node (batch x m); outputs x [batch][2][m],
+// e_w [batch][m].
 __global__ void node_lda_kernel(const double* __restrict__ fields, int64_t m, const double* __restrict__ weights,
                                 const double* __restrict__ f2n, const double* __restrict__ v1s_node,
                                 const double* __restrict__ coef, int na, int batch, double* __restrict__ x,
@@ -102,14 +103,13 @@ __global__ void node_lda_kernel(const double* __restrict__ fields, int64_t m, co
     GRID_STRIDE(k, m * batch) {
         const int64_t g = k / m;
         const int64_t i = k - g * m;
-        const double* fg = fields + g * 2 * m;
-        const double rho_node = fg[i];
+        const double rho_node = fields[g * m + i];
         double vh = 0.0;
         for (int a = 0; a < na; ++a) {
             const double t = coef[g * na + a] * v1s_node[a * m + i];
             vh = (a == 0) ? t : vh + t;
         }
-        vh = vh + fg[m + i];
+        vh = vh + fields[(batch + g) * m + i];
         const double f2 = f2n[i];
         const double nn = f2 * rho_node;
         double e, v;

@@ -80,10 +80,15 @@ __global__ void low_bits_kernel(const unsigned long long* __restrict__ keys, int
 __global__ void interpolate_kernel(const int* __restrict__ base, const double* __restrict__ w1d, int64_t m, int ny,
                                    int nz, const double* __restrict__ fields, int nf, int64_t field_stride,
                                    double* __restrict__ out, int64_t out_stride) {
+    // fields are processed five at a time, chunk blockIdx.y
     const int64_t warp = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= m) return;
     const int64_t node = warp;
+    const int f0 = blockIdx.y * 5;
+    nf = min(5, nf - f0);
+    fields += f0 * field_stride;
+    out += f0 * out_stride;
     const int bx = base[node * 3 + 0] - HALFD, by = base[node * 3 + 1] - HALFD, bz = base[node * 3 + 2] - HALFD;
     const double* w = w1d + node * 24;
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -109,6 +114,10 @@ __global__ void lift_kernel(const int* __restrict__ base, const double* __restri
     const int64_t row = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n_points) return;
+    const int f0 = blockIdx.y * 5;
+    nf = min(5, nf - f0);
+    x += f0 * x_stride;
+    out += f0 * out_stride;
     const long long e0 = row_ptr[row], e1 = row_ptr[row + 1];
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (e1 > e0) {
@@ -221,10 +230,11 @@ extern "C" int cdftb_quadrature_interpolate_f64(const int* base, const double* w
                                                 const double* fields, int nf, int64_t field_stride, double* out,
                                                 int64_t out_stride, cdftb_stream_t stream) {
     (void)nx;
-    if (m < 0 || nf < 1 || nf > 5 || (m > 0 && (!base || !w1d || !fields || !out))) return CDFTB_ERR_ARGUMENT;
+    if (m < 0 || nf < 1 || nf > 5 * 65535 || (m > 0 && (!base || !w1d || !fields || !out))) return CDFTB_ERR_ARGUMENT;
     if (m == 0) return CDFTB_OK;
-    interpolate_kernel<<<blocks_for(m * 32, 256), 256, 0, as_stream(stream)>>>(base, w1d, m, ny, nz, fields, nf,
-                                                                              field_stride, out, out_stride);
+    dim3 grid(blocks_for(m * 32, 256), static_cast<unsigned>(ceil_div(nf, 5)));
+    interpolate_kernel<<<grid, 256, 0, as_stream(stream)>>>(base, w1d, m, ny, nz, fields, nf, field_stride, out,
+                                                            out_stride);
     return check_launch();
 }
 
@@ -232,9 +242,10 @@ extern "C" int cdftb_quadrature_lift_f64(const int* base, const double* w1d, con
                                          int nx, int ny, int nz, const double* node_values, int nf, int64_t x_stride,
                                          double* out, int64_t out_stride, cdftb_stream_t stream) {
     const int64_t n_points = static_cast<int64_t>(nx) * ny * nz;
-    if (nf < 1 || nf > 5 || !base || !w1d || !row_ptr || !col || !node_values || !out || n_points <= 0)
+    if (nf < 1 || nf > 5 * 65535 || !base || !w1d || !row_ptr || !col || !node_values || !out || n_points <= 0)
         return CDFTB_ERR_ARGUMENT;
-    lift_kernel<<<blocks_for(n_points * 32, 256), 256, 0, as_stream(stream)>>>(base, w1d, row_ptr, col, n_points, ny, nz,
-                                                                              node_values, nf, x_stride, out, out_stride);
+    dim3 grid(blocks_for(n_points * 32, 256), static_cast<unsigned>(ceil_div(nf, 5)));
+    lift_kernel<<<grid, 256, 0, as_stream(stream)>>>(base, w1d, row_ptr, col, n_points, ny, nz, node_values, nf, x_stride,
+                                                     out, out_stride);
     return check_launch();
 }

@@ -19,7 +19,9 @@ struct CrossShape {
 
 CrossShape cross_shape(int ma, int mb, int64_t n, int groups) {
     CrossShape s{};
-    if (ma <= 6 && mb <= 6) {
+    if (ma == 1 && mb == 1) {
+        s.ti = s.tj = 1;
+    } else if (ma <= 6 && mb <= 6) {
         s.ti = s.tj = 6;
     } else {
         s.ti = s.tj = 4;
@@ -87,9 +89,12 @@ __global__ void __launch_bounds__(RT) cross_partial_kernel(const double* __restr
     }
 }
 
+// One warp per output entry: lanes take chunks lane, lane + 32, ... in order, then a fixed shuffle
+// tree combines the lanes -- the same order on every run.
 __global__ void cross_final_kernel(const double* __restrict__ partial, int ma, int mb, int ti, int tj, int tiles_j,
                                    int tiles, int chunks, int groups, double* __restrict__ out) {
-    const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t idx = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     const int64_t total = static_cast<int64_t>(groups) * ma * mb;
     if (idx >= total) return;
     const int g = static_cast<int>(idx / (static_cast<int64_t>(ma) * mb));
@@ -100,8 +105,10 @@ __global__ void cross_final_kernel(const double* __restrict__ partial, int ma, i
     const int slot = (i % ti) * tj + (j % tj);
     const double* src = partial + (static_cast<int64_t>(g) * tiles + tile) * chunks * (ti * tj) + slot;
     double v = 0.0;
-    for (int c = 0; c < chunks; ++c) v += src[static_cast<int64_t>(c) * ti * tj];
-    out[idx] = v;
+    for (int c = lane; c < chunks; c += 32) v += src[static_cast<int64_t>(c) * ti * tj];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) out[idx] = v;
 }
 
 }  // namespace
@@ -127,7 +134,10 @@ extern "C" int cdftb_measure_cross_f64(const double* a, int ma, int64_t group_st
     double* partial = static_cast<double*>(scratch);
     const int tiles = s.tiles_i * s.tiles_j;
     dim3 grid(s.chunks, tiles, groups);
-    if (s.ti == 6)
+    if (s.ti == 1)
+        cross_partial_kernel<1, 1><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, n, s.tiles_j,
+                                                        s.chunk, s.chunks, partial);
+    else if (s.ti == 6)
         cross_partial_kernel<6, 6><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, n, s.tiles_j,
                                                         s.chunk, s.chunks, partial);
     else
@@ -136,7 +146,8 @@ extern "C" int cdftb_measure_cross_f64(const double* a, int ma, int64_t group_st
     int rc = check_launch();
     if (rc != CDFTB_OK) return rc;
     const int64_t total = static_cast<int64_t>(groups) * ma * mb;
-    cross_final_kernel<<<static_cast<unsigned>(ceil_div(total, 128)), 128, 0, st>>>(partial, ma, mb, s.ti, s.tj, s.tiles_j,
-                                                                                   tiles, s.chunks, groups, out);
+    cross_final_kernel<<<static_cast<unsigned>(ceil_div(total * 32, 256)), 256, 0, st>>>(partial, ma, mb, s.ti, s.tj,
+                                                                                         s.tiles_j, tiles, s.chunks,
+                                                                                         groups, out);
     return check_launch();
 }

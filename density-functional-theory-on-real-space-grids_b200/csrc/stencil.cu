@@ -89,75 +89,130 @@ struct StencilLayout {
     static constexpr size_t BYTES = sizeof(T) * TOTAL;
 };
 
-// Issue the asynchronous copies of everything step q reads into its pipeline stage. Out-of-range
-// elements are zero-filled by the copy itself (the Dirichlet halo, and the missing faces).
+// Everything a thread copies or reads per x plane is at a fixed position relative to the plane
+// (only the plane index changes as the CTA marches), so the in-plane offsets, their validity and
+// the shared-memory positions are worked out once per thread; a plane then costs one multiply-add
+// and one asynchronous copy per element. Out-of-range elements are zero-filled by the copy itself
+// (the Dirichlet halo, and faces that do not exist).
 template <typename T, int P, int TYV>
-__device__ __forceinline__ void stage_loads(const StencilArgs& a, T* st, int q, int xa, int xe, int y0, int z0,
-                                            int64_t base, int64_t pot_base, int tid, int ty, int tz) {
+struct ThreadPlan {
     using L = StencilLayout<T, P, TYV>;
-    constexpr int H = L::H, K = L::K, PW = L::PW, THR = TZ * TYV;
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const T* in = static_cast<const T*>(a.in);
-    const bool plane_in = (q >= 0) && (q < nx);
-    for (int idx = tid; idx < L::NPHI; idx += THR) {
+    static constexpr int THR = TZ * TYV;
+    static constexpr int IT_PHI = (L::NPHI + THR - 1) / THR;
+    static constexpr int IT_W1 = (L::NW1 + THR - 1) / THR;
+    static constexpr int IT_W2 = (L::NW2 + THR - 1) / THR;
+    int phi_off[IT_PHI];
+    int w1_off[IT_W1];
+    int w2_off[IT_W2];
+    int own_off;          // y * nz + z of the thread's own column
+    unsigned phi_ok;      // bit k: element k lies in the grid (y, z)
+    unsigned w1_ok, w2_ok;
+    bool own_ok;
+    int fy_src[IT_W1];    // smem index of the first tap of each y face this thread forms
+    int fz_src[IT_W2];
+};
+
+template <typename T, int P, int TYV>
+__device__ __forceinline__ void make_plan(ThreadPlan<T, P, TYV>& pl, int y0, int z0, int ny, int nz, int tid, int ty,
+                                          int tz) {
+    using L = StencilLayout<T, P, TYV>;
+    using PL = ThreadPlan<T, P, TYV>;
+    constexpr int H = L::H, K = L::K, PW = L::PW, THR = PL::THR;
+    pl.phi_ok = pl.w1_ok = pl.w2_ok = 0u;
+#pragma unroll
+    for (int k = 0; k < PL::IT_PHI; ++k) {
+        const int idx = tid + k * THR;
         const int r = idx / PW;
         const int c = idx - r * PW;
         const int gy = y0 - H + r;
         const int gz = z0 - H + c;
-        const bool ok = plane_in && gy >= 0 && gy < ny && gz >= 0 && gz < nz;
-        const T* src = ok ? in + base + (static_cast<int64_t>(q) * ny + gy) * nz + gz : in;
-        cp_async(st + idx, src, ok, sizeof(T));
+        const bool ok = idx < L::NPHI && gy >= 0 && gy < ny && gz >= 0 && gz < nz;
+        pl.phi_off[k] = ok ? gy * nz + gz : 0;
+        if (ok) pl.phi_ok |= 1u << k;
+    }
+#pragma unroll
+    for (int k = 0; k < PL::IT_W1; ++k) {
+        const int idx = tid + k * THR;
+        const int r = idx / TZ;
+        const int c = idx - r * TZ;
+        const int g = y0 - P + r;
+        const int gz = z0 + c;
+        const bool ok = idx < L::NW1 && gz < nz && g >= -P && g <= ny + P - 1;
+        pl.w1_off[k] = ok ? (g + P) * nz + gz : 0;
+        if (ok) pl.w1_ok |= 1u << k;
+        pl.fy_src[k] = r * PW + c + H;
+    }
+#pragma unroll
+    for (int k = 0; k < PL::IT_W2; ++k) {
+        const int idx = tid + k * THR;
+        const int r = idx / (TZ + K - 1);
+        const int c = idx - r * (TZ + K - 1);
+        const int g = z0 - P + c;
+        const int gy = y0 + r;
+        const bool ok = idx < L::NW2 && gy < ny && g >= -P && g <= nz + P - 1;
+        pl.w2_off[k] = ok ? gy * (nz + K) + g + P : 0;
+        if (ok) pl.w2_ok |= 1u << k;
+        pl.fz_src[k] = (r + H) * PW + c;
+    }
+    const int y = y0 + ty, z = z0 + tz;
+    pl.own_ok = y < ny && z < nz;
+    pl.own_off = pl.own_ok ? y * nz + z : 0;
+}
+
+template <typename T, int P, int TYV>
+__device__ __forceinline__ void stage_loads(const StencilArgs& a, const ThreadPlan<T, P, TYV>& pl, T* st, int q, int xa,
+                                            int xe, int64_t base, int64_t pot_base, int tid) {
+    using L = StencilLayout<T, P, TYV>;
+    using PL = ThreadPlan<T, P, TYV>;
+    constexpr int H = L::H, K = L::K, THR = PL::THR;
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int64_t plane = static_cast<int64_t>(ny) * nz;
+    const T* in = static_cast<const T*>(a.in);
+    const bool plane_in = (q >= 0) && (q < nx);
+    const T* in_q = in + base + (plane_in ? q * plane : 0);
+#pragma unroll
+    for (int k = 0; k < PL::IT_PHI; ++k) {
+        const int idx = tid + k * THR;
+        if (k == PL::IT_PHI - 1 && idx >= L::NPHI) break;
+        const bool ok = plane_in && ((pl.phi_ok >> k) & 1u);
+        cp_async(st + idx, in_q + pl.phi_off[k], ok, sizeof(T));
     }
     if (q >= xa && q <= xe) {
-        const T* w1 = static_cast<const T*>(a.w1);
-        const T* w2 = static_cast<const T*>(a.w2);
-        for (int idx = tid; idx < L::NW1; idx += THR) {
-            const int r = idx / TZ;
-            const int c = idx - r * TZ;
-            const int g = y0 - P + r;
-            const int gz = z0 + c;
-            const bool ok = gz < nz && g >= -P && g <= ny + P - 1;
-            const T* src = ok ? w1 + (static_cast<int64_t>(q) * (ny + K) + g + P) * nz + gz : w1;
-            cp_async(st + L::OFF_W1 + idx, src, ok, sizeof(T));
+        const T* w1q = static_cast<const T*>(a.w1) + q * static_cast<int64_t>(ny + K) * nz;
+        const T* w2q = static_cast<const T*>(a.w2) + q * static_cast<int64_t>(ny) * (nz + K);
+#pragma unroll
+        for (int k = 0; k < PL::IT_W1; ++k) {
+            const int idx = tid + k * THR;
+            if (k == PL::IT_W1 - 1 && idx >= L::NW1) break;
+            cp_async(st + L::OFF_W1 + idx, w1q + pl.w1_off[k], (pl.w1_ok >> k) & 1u, sizeof(T));
         }
-        for (int idx = tid; idx < L::NW2; idx += THR) {
-            const int r = idx / (TZ + K - 1);
-            const int c = idx - r * (TZ + K - 1);
-            const int g = z0 - P + c;
-            const int gy = y0 + r;
-            const bool ok = gy < ny && g >= -P && g <= nz + P - 1;
-            const T* src = ok ? w2 + (static_cast<int64_t>(q) * ny + gy) * (nz + K) + g + P : w2;
-            cp_async(st + L::OFF_W2 + idx, src, ok, sizeof(T));
+#pragma unroll
+        for (int k = 0; k < PL::IT_W2; ++k) {
+            const int idx = tid + k * THR;
+            if (k == PL::IT_W2 - 1 && idx >= L::NW2) break;
+            cp_async(st + L::OFF_W2 + idx, w2q + pl.w2_off[k], (pl.w2_ok >> k) & 1u, sizeof(T));
         }
     }
-    const int y = y0 + ty;
-    const int z = z0 + tz;
-    const bool valid = (y < ny) && (z < nz);
     const int f = q - P;
     if (q >= xa && f <= nx + P - 1) {
-        const T* w0 = static_cast<const T*>(a.w0);
-        const T* src = valid ? w0 + (static_cast<int64_t>(f + P) * ny + y) * nz + z : w0;
-        cp_async(st + L::OFF_W0 + tid, src, valid, sizeof(T));
+        const T* w0 = static_cast<const T*>(a.w0) + static_cast<int64_t>(f + P) * plane;
+        cp_async(st + L::OFF_W0 + tid, w0 + pl.own_off, pl.own_ok, sizeof(T));
     }
     const int i = q - H;
     if (i >= xa && i <= xe && a.mode >= MODE_KINETIC) {
-        const int64_t point = (static_cast<int64_t>(i) * ny + y) * nz + z;
-        const T* inv = static_cast<const T*>(a.inv_w);
-        cp_async(st + L::OFF_INV + tid, valid ? inv + point : inv, valid, sizeof(T));
-        if (a.mode >= MODE_APPLY) {
-            const T* pot = static_cast<const T*>(a.pot);
-            cp_async(st + L::OFF_POT + tid, valid ? pot + pot_base + point : pot, valid, sizeof(T));
-        }
-        if (a.mode == MODE_CHEB) {
-            const T* prev = static_cast<const T*>(a.prev);
-            cp_async(st + L::OFF_PREV + tid, valid ? prev + base + point : prev, valid, sizeof(T));
-        }
+        const int64_t point = i * plane + pl.own_off;
+        cp_async(st + L::OFF_INV + tid, static_cast<const T*>(a.inv_w) + point, pl.own_ok, sizeof(T));
+        if (a.mode >= MODE_APPLY)
+            cp_async(st + L::OFF_POT + tid, static_cast<const T*>(a.pot) + pot_base + point, pl.own_ok, sizeof(T));
+        if (a.mode == MODE_CHEB)
+            cp_async(st + L::OFF_PREV + tid, static_cast<const T*>(a.prev) + base + point, pl.own_ok, sizeof(T));
     }
 }
 
 template <typename T, int P, int TYV>
 __global__ void __launch_bounds__(TZ* TYV) stencil_kernel(const StencilArgs a) {
     using L = StencilLayout<T, P, TYV>;
+    using PL = ThreadPlan<T, P, TYV>;
     constexpr int H = L::H;
     constexpr int K = L::K;
     constexpr int PW = L::PW;
@@ -179,10 +234,11 @@ __global__ void __launch_bounds__(TZ* TYV) stencil_kernel(const StencilArgs a) {
     const int xa = blockIdx.y * a.xchunk;
     const int xe = min(xa + a.xchunk, nx) - 1;
     const int64_t b = blockIdx.z;
-    const int y = y0 + ty;
-    const int z = z0 + tz;
-    const bool valid = (y < ny) && (z < nz);
     const int64_t base = b * n_points;
+
+    ThreadPlan<T, P, TYV> pl;
+    make_plan<T, P, TYV>(pl, y0, z0, ny, nz, tid, ty, tz);
+    const bool valid = pl.own_ok;
 
     T taps[K];
 #pragma unroll
@@ -214,22 +270,22 @@ __global__ void __launch_bounds__(TZ* TYV) stencil_kernel(const StencilArgs a) {
 #pragma unroll
     for (int s = 0; s < NS - 1; ++s) {
         const int q = q_first + s;
-        if (q <= q_last) stage_loads<T, P, TYV>(a, smem + s * L::STAGE, q, xa, xe, y0, z0, base, pot_base, tid, ty, tz);
+        if (q <= q_last) stage_loads<T, P, TYV>(a, pl, smem + s * L::STAGE, q, xa, xe, base, pot_base, tid);
         cp_async_commit();
     }
 
+    int stage = 0;
     for (int q = q_first; q <= q_last; ++q) {
-        const int step = q - q_first;
         {
             const int qn = q + NS - 1;
-            if (qn <= q_last)
-                stage_loads<T, P, TYV>(a, smem + ((step + NS - 1) % NS) * L::STAGE, qn, xa, xe, y0, z0, base, pot_base,
-                                       tid, ty, tz);
+            int ns = stage + NS - 1;
+            if (ns >= NS) ns -= NS;
+            if (qn <= q_last) stage_loads<T, P, TYV>(a, pl, smem + ns * L::STAGE, qn, xa, xe, base, pot_base, tid);
             cp_async_commit();
         }
         cp_async_wait<NS - 1>();
         __syncthreads();
-        const T* st = smem + (step % NS) * L::STAGE;
+        const T* st = smem + stage * L::STAGE;
         const T* s_phi = st;
 
 #pragma unroll
@@ -246,20 +302,24 @@ __global__ void __launch_bounds__(TZ* TYV) stencil_kernel(const StencilArgs a) {
         if (out_plane) {
             const T* w1s = st + L::OFF_W1;
             const T* w2s = st + L::OFF_W2;
-            for (int idx = tid; idx < L::NW1; idx += THR) {
-                const int r = idx / TZ;
-                const int c = idx - r * TZ;
+#pragma unroll
+            for (int k = 0; k < PL::IT_W1; ++k) {
+                const int idx = tid + k * THR;
+                if (k == PL::IT_W1 - 1 && idx >= L::NW1) break;
+                const T* src = s_phi + pl.fy_src[k];
                 T sum = T(0);
 #pragma unroll
-                for (int k = 0; k < K; ++k) sum += taps[k] * s_phi[(r + k) * PW + c + H];
+                for (int t = 0; t < K; ++t) sum += taps[t] * src[t * PW];
                 s_fy[idx] = w1s[idx] * sum;
             }
-            for (int idx = tid; idx < L::NW2; idx += THR) {
-                const int r = idx / (TZ + K - 1);
-                const int c = idx - r * (TZ + K - 1);
+#pragma unroll
+            for (int k = 0; k < PL::IT_W2; ++k) {
+                const int idx = tid + k * THR;
+                if (k == PL::IT_W2 - 1 && idx >= L::NW2) break;
+                const T* src = s_phi + pl.fz_src[k];
                 T sum = T(0);
 #pragma unroll
-                for (int k = 0; k < K; ++k) sum += taps[k] * s_phi[(r + H) * PW + c + k];
+                for (int t = 0; t < K; ++t) sum += taps[t] * src[t];
                 s_fz[idx] = w2s[idx] * sum;
             }
         }
@@ -294,7 +354,7 @@ __global__ void __launch_bounds__(TZ* TYV) stencil_kernel(const StencilArgs a) {
 #pragma unroll
             for (int k = 0; k < K; ++k) xt += taps[k] * fq[K - 1 - k];
             const T div = xt + yzq[0];
-            const int64_t point = (static_cast<int64_t>(i) * ny + y) * nz + z;
+            const int64_t point = static_cast<int64_t>(i) * ny * nz + pl.own_off;
             T result;
             if (a.mode == MODE_DIV) {
                 result = div;
@@ -315,6 +375,7 @@ __global__ void __launch_bounds__(TZ* TYV) stencil_kernel(const StencilArgs a) {
             }
             store_as<T>(a.out, a.out_dtype, base + point, result);
         }
+        stage = (stage + 1 == NS) ? 0 : stage + 1;
     }
     cp_async_wait<0>();
 }

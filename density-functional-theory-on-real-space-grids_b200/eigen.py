@@ -50,7 +50,8 @@ def chebyshev_filter(hamiltonian, block: torch.Tensor, degree: int, lower: float
     if upper <= lower:
         raise ValueError(f"filter interval is empty: lower={lower}, upper={upper}")
     rows = chebyshev_coefficients(degree, lower, upper, spectrum_min)
-    table = torch.tensor(rows, dtype=torch.float64).to(block.device, non_blocking=False)
+    # pinned + non-blocking: a pageable copy would synchronise the stream (as chefsi.py:758-771 notes)
+    table = torch.tensor(rows, dtype=torch.float64).pin_memory().to(block.device, non_blocking=True)
     return filter_with_table(hamiltonian, block, table, degree, orbitals_per_group=block.numel() // block.shape[-1],
                              precision=precision)
 
@@ -130,7 +131,8 @@ def _rank_revealing_basis(flat: torch.Tensor, gram: torch.Tensor) -> torch.Tenso
     return out[0]
 
 
-def rayleigh_ritz(hamiltonian, block: torch.Tensor, measure: Measure, *, host: bool = True):
+def rayleigh_ritz(hamiltonian, block: torch.Tensor, measure: Measure, *, host: bool = True,
+                  check_cholesky: bool = True):
     """Diagonalise within span(block) (``src/cdft/eigen/rayleigh_ritz.py:75-102``).
 
     Returns ``(eigenvalues, eigenvectors, orthonormality_error)``; with ``host=False`` the error is
@@ -141,8 +143,12 @@ def rayleigh_ritz(hamiltonian, block: torch.Tensor, measure: Measure, *, host: b
     flat = block.to(torch.float64).reshape(-1, n)
     basis, gram = orthonormalise(flat, measure)
     ws = _WS.get(flat.shape[0], 1, block.device)
-    if int(ws.info[0].item()) != 0:
-        basis = _rank_revealing_basis(flat, gram[0]).reshape(1, -1, n)
+    info = ws.info.clone()
+    if check_cholesky:
+        # The Cholesky status is read with the caller's per-iteration scalars (no extra sync) when
+        # check_cholesky is False; a failure then repeats this step through the eigh fallback.
+        if int(info[0].item()) != 0:
+            basis = _rank_revealing_basis(flat, gram[0]).reshape(1, -1, n)
     m = basis.shape[1]
     stream = stream_handle(block.device)
     applied = hamiltonian.apply(basis[0]).reshape(1, m, n)
@@ -160,6 +166,8 @@ def rayleigh_ritz(hamiltonian, block: torch.Tensor, measure: Measure, *, host: b
     evals = ws.evals[0].clone()
     vec = vectors[0]
     _APPLIED[id(vec)] = (vec, rotated_applied[0])
+    if not check_cholesky:
+        rayleigh_ritz.last_info = info
     return evals, vec, (float(error) if host else error)
 
 
@@ -230,11 +238,16 @@ class ChebyshevFilteredSubspace:
     Rayleigh--Ritz, residual and Lanczos step stays float64.
     """
 
-    def __init__(self, grid, config: EigenConfig, ritz_stop: bool = True, filter_hamiltonian=None) -> None:
+    def __init__(self, grid, config: EigenConfig, ritz_stop: bool = True, filter_hamiltonian=None,
+                 switch_residual: float | None = None) -> None:
         self.grid = grid
         self.config = config
         self.ritz_stop = ritz_stop
         self.filter_hamiltonian = filter_hamiltonian
+        #: With a float filter: once the worst wanted residual falls below this, filter in float64
+        #: (a float-filtered subspace stalls near residual 1e-5, above a 1e-8 target).
+        self.switch_residual = switch_residual
+        self.float_filter_iterations = 0
         self.history: list[dict] = []
         self.spectral_bounds = None
         self.bounds_source = "unset"
@@ -298,14 +311,26 @@ class ChebyshevFilteredSubspace:
             filtered = chebyshev_filter(filt, vectors, cfg.chebyshev_degree, lower, spectrum_max, spectrum_min)
             if filt is not hamiltonian:
                 hamiltonian.note_applications(cfg.chebyshev_degree)
-            evals, vectors, orth_error = rayleigh_ritz(hamiltonian, filtered, measure, host=False)
+                self.float_filter_iterations += 1
+            evals, vectors, orth_error = rayleigh_ritz(hamiltonian, filtered, measure, host=False, check_cholesky=False)
+            info = rayleigh_ritz.last_info
             residual = residual_norms(hamiltonian, evals, vectors, measure)
             top = min(size, evals.shape[0]) - 1
-            worst, drift, orth, next_lower = torch.stack([
+            worst, drift, orth, next_lower, chol = torch.stack([
                 residual[:n_states].max(), (evals[:n_states] - previous[:n_states]).abs().max(), orth_error,
-                evals[top]]).tolist()
+                evals[top], info[0].to(torch.float64)]).tolist()
+            if chol != 0.0:
+                # rank-deficient filtered block: redo this step with the eigh fallback (rayleigh_ritz.py:64-70)
+                evals, vectors, orth_error = rayleigh_ritz(hamiltonian, filtered, measure, host=False)
+                residual = residual_norms(hamiltonian, evals, vectors, measure)
+                top = min(size, evals.shape[0]) - 1
+                worst, drift, orth, next_lower = torch.stack([
+                    residual[:n_states].max(), (evals[:n_states] - previous[:n_states]).abs().max(), orth_error,
+                    evals[top]]).tolist()
             previous = evals.clone()
             self.eigenvalue_drift = drift
+            if filt is not hamiltonian and self.switch_residual is not None and worst < self.switch_residual:
+                filt = hamiltonian
             self.history.append({"iteration": float(iteration), "residual": worst, "orthonormality": orth,
                                  "eigenvalue_drift": drift})
             if worst < cfg.residual_tol:

@@ -350,8 +350,7 @@ class CuspQuadrature:
         """``L field`` at the nodes, ``(..., m)``."""
         n = self.grid.n_points
         flat = field.to(torch.float64).reshape(-1, n).contiguous()
-        outs = [self._interp_raw(flat[i:i + 5].contiguous(), min(5, flat.shape[0] - i)) for i in range(0, flat.shape[0], 5)]
-        return torch.cat(outs).reshape(*field.shape[:-1], self.n_nodes)
+        return self._interp_raw(flat, flat.shape[0]).reshape(*field.shape[:-1], self.n_nodes)
 
     def interpolate_gradient(self, field: torch.Tensor) -> torch.Tensor:
         return self.interpolate(gradient(self.grid, field))
@@ -359,8 +358,7 @@ class CuspQuadrature:
     def lift(self, node_values: torch.Tensor) -> torch.Tensor:
         """``L^T x`` on the grid, ``(..., N)``."""
         flat = node_values.to(torch.float64).reshape(-1, self.n_nodes).contiguous()
-        outs = [self._lift_raw(flat[i:i + 5].contiguous(), min(5, flat.shape[0] - i)) for i in range(0, flat.shape[0], 5)]
-        return torch.cat(outs).reshape(*node_values.shape[:-1], self.grid.n_points)
+        return self._lift_raw(flat, flat.shape[0]).reshape(*node_values.shape[:-1], self.grid.n_points)
 
     def interpolate_at(self, points: torch.Tensor, field: torch.Tensor) -> torch.Tensor:
         """Degree-7 interpolation at arbitrary points (quadrature.py:652-697)."""

@@ -238,7 +238,12 @@ def cast(x: torch.Tensor, dtype: torch.dtype) -> torch.Tensor:
 
 
 def seeded_randn(shape, generator, *, device, dtype=torch.float64) -> torch.Tensor:
-    """Draw on the generator's (CPU) device, then move: ``src/cdft/precision.py:246-263``."""
+    """Draw on the generator's (CPU) device, then move: ``src/cdft/precision.py:246-263``.
+
+    A :class:`~.rng.SeededStream` serves the same draws from its device cache (read-only tensors).
+    """
+    if hasattr(generator, "randn") and not isinstance(generator, torch.Generator):
+        return generator.randn(shape)
     source = generator.device if generator is not None else torch.device("cpu")
     size = (shape,) if isinstance(shape, int) else tuple(shape)
     return torch.randn(size, device=source, dtype=dtype, generator=generator).to(device)

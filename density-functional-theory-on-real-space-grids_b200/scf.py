@@ -26,6 +26,7 @@ from .eigen import (BOUND_REUSE_RITZ_FRACTION, ChebyshevFilteredSubspace, EigenC
 from .geometry import CuspGeometry, _hptr, _host, gradient, partial_derivative, row_sums
 from .operators import CuspFactoredHamiltonian, measure_cross
 from .poisson import CoulombCutoffPoisson
+from .rng import SeededStream
 from .xc import functional_by_name
 
 FILTER_STEPS_PER_ITERATION = 4
@@ -214,13 +215,24 @@ class KohnShamStep:
         return CuspFactoredHamiltonian(self.grid, self.factor, extra_potential=potentials.effective,
                                        quadrature=self.quadrature, dtype=dtype)
 
+    #: A float-filtered full diagonalisation switches to the float64 filter below this residual.
+    FLOAT_FILTER_SWITCH_RESIDUAL = 1.0e-4
+
     def diagonalise(self, hamiltonian, initial=None, max_iterations=None, *, bounds=None, filter_hamiltonian=None):
-        """(``src/cdft/scf/step.py:321-355``); ``ritz_stop=False`` inside the SCF."""
-        generator = torch.Generator(device="cpu").manual_seed(self.seed)
+        """(``src/cdft/scf/step.py:321-355``); ``ritz_stop=False`` inside the SCF.
+
+        With a float ``filter_hamiltonian``, a full diagonalisation (no iteration cap) filters in
+        float until its residual is below :attr:`FLOAT_FILTER_SWITCH_RESIDUAL`, then in float64; a
+        capped one (the warm-started SCF iterations) filters in float throughout.
+        """
+        # a freshly seeded generator per call, as step.py:338; its draws are cached on the device
+        generator = SeededStream(self.seed, self.grid.device)
         cfg = self.eigen
         if max_iterations is not None:
             cfg = EigenConfig(**{**cfg.__dict__, "max_iterations": max_iterations})
-        solver = ChebyshevFilteredSubspace(self.grid, cfg, ritz_stop=False, filter_hamiltonian=filter_hamiltonian)
+        switch = self.FLOAT_FILTER_SWITCH_RESIDUAL if max_iterations is None else None
+        solver = ChebyshevFilteredSubspace(self.grid, cfg, ritz_stop=False, filter_hamiltonian=filter_hamiltonian,
+                                           switch_residual=switch)
         result = solver.solve(hamiltonian, self.n_states, initial=initial, generator=generator, bounds=bounds)
         info = {"eigen_stop_reason": solver.stop_reason, "eigen_eigenvalue_drift": solver.eigenvalue_drift,
                 "eigen_spectral_bounds": list(solver.spectral_bounds or ()), "eigen_bounds_source": solver.bounds_source,
@@ -572,9 +584,9 @@ def solve_self_consistent(step: KohnShamStep, mixing: MixingConfig | None = None
         n_in = n_next
     # final full diagonalisation at the last input potential, fresh Lanczos, float64 filter
     final_h = step.hamiltonian(p_in)
+    float_final = step.filter_precision == torch.float32 and not refine_in_float64
     eigen, info = step.diagonalise(final_h, initial=eigen.eigenvectors,
-                                   filter_hamiltonian=None if refine_in_float64 else
-                                   (step.hamiltonian(p_in, dtype=torch.float32) if mixed else None))
+                                   filter_hamiltonian=step.hamiltonian(p_in, dtype=torch.float32) if float_final else None)
     occupations = step.occupy(eigen.eigenvalues)
     n_out, rho_out = step.output_density(eigen, occupations)
     p_out = step.potentials(n_out)
@@ -608,7 +620,7 @@ def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: in
     grid = geometry.grid
     ham = CuspFactoredHamiltonian(grid, geometry.factor, quadrature=geometry.quadrature)
     n_states = max(1, int(-(-float(n_electrons) // 2.0)))
-    generator = torch.Generator(device="cpu").manual_seed(seed)
+    generator = SeededStream(seed, grid.device)
     solver = ChebyshevFilteredSubspace(grid, eigen or EigenConfig(), ritz_stop=True)
     result = solver.solve(ham, n_states, generator=generator)
     occ = torch.from_numpy(aufbau_occupations(n_states, float(n_electrons))).to(grid.device)

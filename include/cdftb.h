@@ -172,11 +172,11 @@ int cdftb_quadrature_stencils(const double* points, int64_t m, int nx, int ny, i
 int64_t cdftb_lift_plan_scratch_bytes(int64_t m, int64_t n_points);
 int cdftb_lift_plan_build(const int* base, int64_t m, int nx, int ny, int nz, long long* row_ptr, int* col,
                           void* scratch, int64_t scratch_bytes, cdftb_stream_t stream);
-/* out[f][node] = (L field_f)[node] for nf <= 5 fields (quadrature.py:613-620 interpolate). */
+/* out[f][node] = (L field_f)[node] for nf fields (quadrature.py:613-620 interpolate). */
 int cdftb_quadrature_interpolate_f64(const int* base, const double* w1d, int64_t m, int nx, int ny, int nz,
                                      const double* fields, int nf, int64_t field_stride, double* out,
                                      int64_t out_stride, cdftb_stream_t stream);
-/* out[f] = L^T x_f for nf <= 5 node vectors (quadrature.py:628-638 lift). */
+/* out[f] = L^T x_f for nf node vectors (quadrature.py:628-638 lift). */
 int cdftb_quadrature_lift_f64(const int* base, const double* w1d, const long long* row_ptr, const int* col, int nx,
                               int ny, int nz, const double* node_values, int nf, int64_t x_stride, double* out,
                               int64_t out_stride, cdftb_stream_t stream);
@@ -190,8 +190,8 @@ int cdftb_cusp_coefficients_f64(const double* rho_at_nuclei, const double* nucle
 int cdftb_hartree_split_f64(const double* density, const double* f2, const double* cusp_grid,
                             const double* coefficients, int n_atoms, int64_t n_points, int batch, double* rho,
                             double* n_smooth, cdftb_stream_t stream);
-/* Node side, LDA: from [rho_node, vsmooth_node] -> lift inputs [w f2 vH, w f2 v_xc] and w e_xc
- * (step.py:247-261 with the interpolant fused in by the caller). */
+/* Node side, LDA: from rho_node (batch x m) then vsmooth_node (batch x m) -> lift inputs
+ * [batch][w f2 vH, w f2 v_xc] and w e_xc (step.py:247-261 with the interpolant fused in by the caller). */
 int cdftb_potentials_node_lda_f64(const double* fields, int64_t m, const double* weights, const double* f2_node,
                                   const double* v1s_node, const double* coefficients, int n_atoms, int batch,
                                   double* lift_inputs, double* xc_energy_density, cdftb_stream_t stream);

@@ -172,8 +172,10 @@ def test_he25_lda_scf_mixed_precision(pkg, he25, golden_values):
     out = pkg.solve_self_consistent(step, pkg.MixingConfig(scheme="linear", alpha=0.3))
     ref = golden_values["he25_lda_linear"]
     assert out.converged
+    # The energy is variational (the 1e-8 Ha target); the eigenvalue is first order in the density,
+    # which both solves converge only to the SCF's 1e-6 electron tolerance.
     assert abs(out.energies["total"] - ref["total"]) < 1e-8
-    assert abs(out.eigenvalues[0] - ref["eigenvalues"][0]) < 1e-8
+    assert abs(out.eigenvalues[0] - ref["eigenvalues"][0]) < 1e-6
     assert out.measurements["filter_precision"] == "float32"
 
 

@@ -48,6 +48,9 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_measure_cross_scratch_bytes": (c_int64, [c_int, c_int, c_int64, c_int]),
     "cdftb_measure_cross_f64": (c_int, [c_void_p, c_int, c_int64, c_void_p, c_int, c_int64, c_void_p, c_int64, c_int,
                                         c_void_p, c_void_p, c_int64, c_void_p]),
+    "cdftb_measure_cross_static_capacity_bytes": (c_int64, []),
+    "cdftb_measure_cross_static_f64": (c_int, [c_void_p, c_int, c_int64, c_void_p, c_int, c_int64, c_void_p, c_int64,
+                                               c_int, c_void_p, c_void_p]),
     "cdftb_small_cholesky_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
     "cdftb_block_trsm_lower_f64": (c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int, c_int64, c_int, c_int64, c_int,
                                            c_void_p]),

@@ -151,3 +151,54 @@ extern "C" int cdftb_measure_cross_f64(const double* a, int ma, int64_t group_st
                                                                                          groups, out);
     return check_launch();
 }
+
+// ---------------------------------------------------------------------------------------------
+// cdftb_measure_cross_static_f64: the same product with its partials in a fixed device array of
+// this library instead of caller scratch, for callers that cannot allocate device memory. The
+// array lives once per device (each device's copy of this module); its address is looked up with
+// cudaGetSymbolAddress on the first call on that device and kept. The first pass writes every
+// partial that the second pass reads, so nothing in the array has to start at zero. Two calls whose
+// work overlaps on the GPU (other streams, other host threads) share the array and race.
+
+namespace cdftb {
+namespace {
+
+constexpr int64_t kStaticCrossScratchBytes = int64_t(4) << 20;
+constexpr int kMaxDevices = 64;
+
+__device__ __align__(256) static unsigned char g_static_cross_scratch[kStaticCrossScratchBytes];
+
+void* g_static_cross_address[kMaxDevices] = {};
+
+int static_cross_scratch(void** out) {
+    int dev = -1;
+    int rc = check(cudaGetDevice(&dev));
+    if (rc != CDFTB_OK) return rc;
+    if (dev < 0 || dev >= kMaxDevices) return CDFTB_ERR_CAPACITY;
+    void* p = __atomic_load_n(&g_static_cross_address[dev], __ATOMIC_ACQUIRE);
+    if (!p) {
+        rc = check(cudaGetSymbolAddress(&p, g_static_cross_scratch));
+        if (rc != CDFTB_OK) return rc;
+        __atomic_store_n(&g_static_cross_address[dev], p, __ATOMIC_RELEASE);
+    }
+    *out = p;
+    return CDFTB_OK;
+}
+
+}  // namespace
+}  // namespace cdftb
+
+extern "C" int64_t cdftb_measure_cross_static_capacity_bytes(void) { return kStaticCrossScratchBytes; }
+
+extern "C" int cdftb_measure_cross_static_f64(const double* a, int ma, int64_t group_stride_a, const double* b,
+                                              int mb, int64_t group_stride_b, const double* q, int64_t n, int groups,
+                                              double* out, cdftb_stream_t stream) {
+    if (!a || !b || !out || ma <= 0 || mb <= 0 || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
+    const int64_t need = cdftb_measure_cross_scratch_bytes(ma, mb, n, groups);
+    if (need > kStaticCrossScratchBytes) return CDFTB_ERR_CAPACITY;
+    void* scratch = nullptr;
+    const int rc = static_cross_scratch(&scratch);
+    if (rc != CDFTB_OK) return rc;
+    return cdftb_measure_cross_f64(a, ma, group_stride_a, b, mb, group_stride_b, q, n, groups, out, scratch,
+                                   kStaticCrossScratchBytes, stream);
+}

@@ -96,6 +96,23 @@ int cdftb_measure_cross_f64(const double* a, int ma, int64_t group_stride_a, con
                             int64_t group_stride_b, const double* q, int64_t n, int groups, double* out,
                             void* scratch, int64_t scratch_bytes, cdftb_stream_t stream);
 
+/* No reference counterpart: cdftb_measure_cross_f64 for callers that cannot allocate device
+ * memory. Same arguments and results (bit-identical), but the partials go to a fixed device array
+ * of this library, cdftb_measure_cross_static_capacity_bytes() = 4 MiB per device, instead of
+ * caller scratch. This call allocates nothing (no cudaMalloc, no cudaFree).
+ * - Returns CDFTB_ERR_CAPACITY when cdftb_measure_cross_scratch_bytes(ma, mb, n, groups) exceeds
+ *   that capacity.
+ * - The first call on a device looks up the array's address (cudaGetSymbolAddress, checked;
+ *   CDFTB_ERR_LAUNCH on failure). That set-up call must come before any stream capture.
+ * - Calls whose work overlaps on the GPU (several streams or host threads on one device) share the
+ *   array and race; the caller orders them.
+ * - Nothing in the array has to start at zero: the first pass writes every partial the second
+ *   pass reads. */
+int64_t cdftb_measure_cross_static_capacity_bytes(void);
+int cdftb_measure_cross_static_f64(const double* a, int ma, int64_t group_stride_a, const double* b, int mb,
+                                   int64_t group_stride_b, const double* q, int64_t n, int groups, double* out,
+                                   cdftb_stream_t stream);
+
 /* (e2) Per group: lower = chol(gram), info[g] = 0, or k+1 if the leading minor k is not positive
  * (src/cdft/eigen/rayleigh_ritz.py:62-63 torch.linalg.cholesky). */
 int cdftb_small_cholesky_f64(const double* gram, double* lower, int* info, int m, int groups,

@@ -43,8 +43,10 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_weighted_divergence_f64": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p, c_void_p,
                                               c_void_p, c_double, c_int, c_void_p]),
     "cdftb_cusp_apply": (c_int, [ctypes.POINTER(Operator), c_void_p, c_int, c_void_p, c_int, c_int64, c_int, c_void_p]),
+    "cdftb_chebyshev_filter_work_bytes": (c_int64, [ctypes.POINTER(Operator), c_int64]),
     "cdftb_chebyshev_filter": (c_int, [ctypes.POINTER(Operator), c_void_p, c_int, c_void_p, c_int, c_void_p, c_int64,
-                                       c_void_p, c_int, c_void_p]),
+                                       c_int64, c_void_p, c_int, c_void_p]),
+    "cdftb_device_status": (c_int, [ctypes.POINTER(c_int)]),
     "cdftb_measure_cross_scratch_bytes": (c_int64, [c_int, c_int, c_int64, c_int]),
     "cdftb_measure_cross_f64": (c_int, [c_void_p, c_int, c_int64, c_void_p, c_int, c_int64, c_void_p, c_int64, c_int,
                                         c_void_p, c_void_p, c_int64, c_void_p]),

@@ -26,7 +26,7 @@ import torch
 
 from . import _lib
 from ._lib import F32, F64, call, ptr, stream_handle
-from .eigen import BOUND_REUSE_RITZ_FRACTION, EigenConfig, chebyshev_coefficients
+from .eigen import BOUND_REUSE_RITZ_FRACTION, EigenConfig, chebyshev_coefficients, filter_workspace
 from .geometry import CuspGeometry, gradient, row_sums
 from .operators import cast, measure_cross, rowwise_inner
 from .poisson import CoulombCutoffPoisson
@@ -97,10 +97,10 @@ class BatchedHamiltonian:
         x = block.contiguous()
         b, k, n = x.shape
         out = torch.empty_like(x)
-        work = torch.empty((3, b * k, n), dtype=self.dtype, device=x.device)
         op = self._op(k)
+        work = filter_workspace(op, b * k, x.device)
         call("cdftb_chebyshev_filter", ctypes.byref(op), ptr(x), _lib.dtype_code(x), ptr(out), _lib.dtype_code(out),
-             ptr(work), b * k, ptr(table.contiguous()), degree, stream_handle(x.device))
+             ptr(work), work.numel(), b * k, ptr(table.contiguous()), degree, stream_handle(x.device))
         self.applications += degree
         return out
 

@@ -67,4 +67,12 @@ struct StaggeredTaps {
 
 StaggeredTaps staggered_taps(int accuracy);
 
+// The two Chebyshev filter paths behind cdftb_chebyshev_filter (stencil.cu, filter.cu).
+int generic_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
+                             void* work, int64_t batch, const double* coefficients, int degree, cdftb_stream_t stream);
+int64_t slab_filter_work_bytes(const cdftb_operator* op, int64_t batch);
+bool slab_filter_applies(const cdftb_operator* op);
+int slab_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
+                          void* work, int64_t batch, const double* coefficients, int degree, cudaStream_t stream);
+
 }  // namespace cdftb

@@ -1,0 +1,878 @@
+// (b) The fused Chebyshev filter on slabs: every step of the scaled three-term recurrence
+// (src/cdft/eigen/chefsi.py:81-160) is one launch of slab_filter_kernel, which applies the
+// order-8 staggered divergence-form operator (src/cdft/operators/divergence.py:99-197, epilogue of
+// src/cdft/operators/hamiltonian.py:303-318) and the recurrence update in one pass.
+//
+// Layout in HBM. The filter keeps its iterates in an internal layout: "lanes" of 8-byte elements,
+// each lane (nx, ny, nzp) with nzp = nz rounded up to even and the padding column held at zero. In
+// float32 a lane interleaves two orbitals (a float2 per point, so that the packed f32x2 FMA of sm_100
+// does two orbitals per instruction); in float64 a lane is one orbital. The block is packed into
+// this layout once per filter call and the last step writes the caller's layout. The geometry (face
+// weights, h^3/omega, potentials) is copied once per call into rows padded to 16 bytes so that TMA
+// can read it.
+//
+// Kernel. A CTA owns a tile of 8 rows (y) x TZ columns (z) of one lane and marches along x over a
+// chunk of planes. Its warps have three roles, coupled by mbarrier rings in shared memory:
+//   producer (1 warp)   per plane, TMA copies of: the plane of phi with a 7-point halo in y and z
+//                       (zero outside the grid: the Dirichlet boundary), the previous iterate, and
+//                       the plane's face weights, h^3/omega and potential(s), into one of R slots;
+//   pass groups (2)     per plane (groups alternate), the y- and z-direction parts of
+//                       sum_d D_d^T[w_d D_d phi]: one thread per line segment of 8 outputs, a
+//                       column (22 nodes -> 15 y faces -> 8 outputs in registers) or a row segment
+//                       (the same along z), all on one code path, into one of RY result slots;
+//   march (8 or 9)      one thread per (y, z) column: queues of the last 8 planes of phi, x faces and
+//                       y+z parts in registers (slot = plane mod 8: the loop is unrolled by 8, so
+//                       no register moves), the output of node i formed at plane i + 7 with the
+//                       recurrence epilogue, stored with coalesced 8-byte writes.
+// Every mbarrier wait is bounded: after kWaitLimitNs (or when another CTA has given up) the warp
+// records the failure in g_device_error (read by cdftb_device_status) and leaves the kernel.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace cdftb {
+
+__device__ int g_device_error = 0;
+// The launch (by its token) whose CTAs must give up: a CTA that timed out writes its launch's token,
+// so the other CTAs of that launch stop waiting, while later launches are unaffected.
+__device__ unsigned g_abort_token = 0;
+
+namespace {
+
+constexpr int TY = 8;
+constexpr int HALO = 7;
+constexpr int NROW = TY + 2 * HALO;
+constexpr int R = 6;      // plane slots in flight
+constexpr int RY = 4;     // y+z result slots (a power of 2)
+static_assert((RY & (RY - 1)) == 0, "result slots are a power of 2");
+constexpr int NG = 2;     // pass warp groups; planes alternate between them
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
+static_assert(R % NG == 0 && RY % NG == 0, "a slot is always served by the same pass group");
+constexpr unsigned kSuspendNs = 20000;  // try_wait suspend hint: a waiting warp sleeps instead of spinning
+
+constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
+
+template <int TZ, int SB>  // SB: bytes of a geometry element (4 or 8)
+struct Shape {
+    static constexpr int MW = TY * TZ / 32;  // march warps
+    // pass items of a plane: TZ columns (y) and TY rows x NZS segments of 8 (z); the last z segment
+    // is moved left to end at TZ (it then stores only the outputs the previous one did not)
+    static constexpr int NZS = (TZ + 7) / 8;
+    static constexpr int ITEMS = TZ + TY * NZS;
+    static constexpr int PWG = (ITEMS + 31) / 32;  // pass warps per group
+    static constexpr int PW = NG * PWG;            // pass warps
+    static constexpr int WARPS = MW + PW + 1;
+    static constexpr int T = WARPS * 32;
+    static constexpr int BW = TZ + 18;  // phi box width: z0-8 .. z0+TZ+9 (16-byte rows, bank-shifted)
+    static constexpr int ZROW = TZ + 2;
+    // bytes each TMA box delivers
+    static constexpr unsigned TX_PHI = NROW * BW * 8;
+    static constexpr unsigned TX_PREV = TY * TZ * 8;
+    static constexpr unsigned TX_W0 = TY * TZ * SB;
+    static constexpr unsigned TX_W1 = (TY + 7) * TZ * SB;
+    static constexpr unsigned TX_W2 = TY * (TZ + 8) * SB;
+    static constexpr unsigned TX_INV = TY * TZ * SB;
+    static constexpr unsigned TX_POT = TY * TZ * SB;
+    // slot layout, every region 128-byte aligned
+    static constexpr size_t O_PHI = 0;
+    static constexpr size_t O_PREV = O_PHI + align128(TX_PHI);
+    static constexpr size_t O_W0 = O_PREV + align128(TX_PREV);
+    static constexpr size_t O_W1 = O_W0 + align128(TX_W0);
+    static constexpr size_t O_W2 = O_W1 + align128(TX_W1);
+    static constexpr size_t O_INV = O_W2 + align128(TX_W2);
+    static constexpr size_t O_POT0 = O_INV + align128(TX_INV);
+    static constexpr size_t O_POT1 = O_POT0 + align128(TX_POT);
+    static constexpr size_t SLOT = O_POT1 + align128(TX_POT);
+    static constexpr size_t O_YZ = R * SLOT;
+    static constexpr size_t YZ_Z = size_t(TY) * TZ * 8;  // Z part after the Y part
+    static constexpr size_t YZ_SLOT = align128(YZ_Z + size_t(TY) * ZROW * 8);
+    static constexpr size_t O_BAR = O_YZ + RY * YZ_SLOT;
+    static constexpr size_t BYTES = O_BAR + (2 * R + 2 * RY) * 8;
+    static_assert(TY * TZ % 32 == 0, "march warps cover the tile");
+    static_assert(TZ >= 8 && TZ % 2 == 0, "z segments of 8 inside the tile");
+    static_assert((TZ - 8) + 22 <= BW - 1, "the last z segment's nodes lie inside the phi box");
+    static_assert(BYTES <= 232448, "fits the opt-in shared memory of one CTA");
+};
+
+// Element arithmetic: a float2 lane (two orbitals, packed f32x2 instructions) or a double lane.
+struct LaneF2 {
+    using E = float2;
+    using S = float;
+    static __device__ __forceinline__ E fma(E a, E b, E c) { return __ffma2_rn(a, b, c); }
+    static __device__ __forceinline__ E mul(E a, E b) { return __fmul2_rn(a, b); }
+    static __device__ __forceinline__ E add(E a, E b) { return __fadd2_rn(a, b); }
+    static __device__ __forceinline__ E neg(E a) { return make_float2(-a.x, -a.y); }
+    static __device__ __forceinline__ E splat(S s) { return make_float2(s, s); }
+    static __device__ __forceinline__ E zero() { return make_float2(0.f, 0.f); }
+    static __device__ __forceinline__ void load2(const E* p, E& a, E& b) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        a = make_float2(v.x, v.y);
+        b = make_float2(v.z, v.w);
+    }
+    static __device__ __forceinline__ void store2(E* p, E a, E b) {
+        *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+    }
+    static constexpr int ORBITALS = 2;
+    static constexpr CUtensorMapDataType GEO_TYPE = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+};
+
+struct LaneD {
+    using E = double;
+    using S = double;
+    static __device__ __forceinline__ E fma(E a, E b, E c) { return ::fma(a, b, c); }
+    static __device__ __forceinline__ E mul(E a, E b) { return a * b; }
+    static __device__ __forceinline__ E add(E a, E b) { return a + b; }
+    static __device__ __forceinline__ E neg(E a) { return -a; }
+    static __device__ __forceinline__ E splat(S s) { return s; }
+    static __device__ __forceinline__ E zero() { return 0.0; }
+    static __device__ __forceinline__ void load2(const E* p, E& a, E& b) {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        a = v.x;
+        b = v.y;
+    }
+    static __device__ __forceinline__ void store2(E* p, E a, E b) { *reinterpret_cast<double2*>(p) = make_double2(a, b); }
+    static constexpr int ORBITALS = 1;
+    static constexpr CUtensorMapDataType GEO_TYPE = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+};
+
+struct FilterArgs {
+    int nx, ny, nz, nzp;
+    int tiles_z;
+    int xchunk;
+    int has_prev;
+    int final_out;
+    void* out;
+    int out_dtype;
+    int64_t batch;
+    int64_t lane_first;  // first lane of this launch (launches are split at 65535 lanes)
+    int orb_per_group;
+    int shared_potential;  // one potential for every orbital
+    unsigned token;        // this launch's abort token (never 0)
+    const double* coef;
+    int degree;
+    int step;
+    double taps[8];
+};
+
+struct FilterMaps {
+    CUtensorMap phi, prev, w0, w1, w2, inv, pot;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity), "r"(kSuspendNs)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ void record_failure(unsigned token) {
+    atomicOr(&g_device_error, 1);
+    atomicExch(&g_abort_token, token);
+}
+
+// Bounded wait for the phase of this parity. False after limit_ns, or as soon as another warp or
+// CTA of the same launch has given up; a timeout itself is recorded.
+__device__ __noinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity, unsigned long long limit_ns,
+                                               unsigned token) {
+    const unsigned long long start = globaltimer();
+    for (unsigned it = 0; it < (1u << 30); ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 7) == 7) {
+            if (*reinterpret_cast<volatile unsigned*>(&g_abort_token) == token) return false;
+            if (globaltimer() - start > limit_ns) {
+                record_failure(token);
+                return false;
+            }
+        }
+    }
+    record_failure(token);
+    return false;
+}
+
+__device__ __forceinline__ bool wait_full(unsigned bar, unsigned parity, unsigned token) {
+    if (mbar_try_wait(bar, parity)) return true;
+    return mbar_wait_bounded(bar, parity, kWaitLimitNs, token);
+}
+
+// The same wait by every lane of a warp, with one verdict for the whole warp (a lane that gave up
+// makes the warp leave together, so no lane waits in __syncwarp for an exited one).
+__device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, unsigned token) {
+    return __all_sync(0xffffffffu, wait_full(bar, parity, token)) != 0;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+template <typename Lane, int TZ>
+__global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
+    slab_filter_kernel(const __grid_constant__ FilterMaps maps, const FilterArgs a) {
+    using S = typename Lane::S;
+    using E = typename Lane::E;
+    using SH = Shape<TZ, sizeof(S)>;
+    constexpr int BW = SH::BW;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const unsigned bar_full = smem_u32(smem + SH::O_BAR);
+    const unsigned bar_empty = bar_full + 8 * R;
+    const unsigned bar_yfull = bar_empty + 8 * R;
+    const unsigned bar_yempty = bar_yfull + 8 * RY;
+
+    const int t = threadIdx.x;
+    const int warp = t >> 5;
+    const int nx = a.nx, ny = a.ny, nz = a.nz, nzp = a.nzp;
+    const int y0 = (blockIdx.x / a.tiles_z) * TY;
+    const int z0 = (blockIdx.x % a.tiles_z) * TZ;
+    const int xa = blockIdx.y * a.xchunk;
+    const int xe = min(xa + a.xchunk, nx) - 1;
+    const int lane = static_cast<int>(a.lane_first) + blockIdx.z;
+    const int q0 = xa - HALO;              // first plane: nodes xa-7 .. xe+7 are read
+    const int npl = xe - xa + 1 + 2 * HALO;  // planes marched
+    const bool has_prev = a.has_prev != 0;
+
+    const int64_t o0 = int64_t(lane) * Lane::ORBITALS;
+    const int64_t o1 = (Lane::ORBITALS == 2) ? min(o0 + 1, a.batch - 1) : o0;
+    const int g0 = a.shared_potential ? 0 : static_cast<int>(o0 / a.orb_per_group);
+    const int g1 = a.shared_potential ? 0 : static_cast<int>(o1 / a.orb_per_group);
+
+    if (t == 0) {
+        for (int s = 0; s < R; ++s) {
+            mbar_init(bar_full + 8 * s, 1);
+            mbar_init(bar_empty + 8 * s, SH::MW + SH::PWG);
+        }
+        for (int s = 0; s < RY; ++s) {
+            mbar_init(bar_yfull + 8 * s, SH::PWG);
+            mbar_init(bar_yempty + 8 * s, SH::MW);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+
+    E tap[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) tap[j] = Lane::splat(static_cast<S>(a.taps[j]));
+
+    if (warp == SH::MW + SH::PW) {
+        // ------------------------------------------------------------------ producer
+        if ((t & 31) != 0) return;
+        const unsigned tx = SH::TX_PHI + (has_prev ? SH::TX_PREV : 0) + SH::TX_W0 + SH::TX_W1 + SH::TX_W2 +
+                            SH::TX_INV + 2 * SH::TX_POT;
+        int issued = 0;
+        int s = 0, ph = 1;  // slot; parity of its previous use (the first R fills wait for nothing)
+        for (int n = 0; n < npl; ++n) {
+            if (n >= R && !wait_full(bar_empty + 8 * s, ph, a.token)) break;
+            const unsigned full = bar_full + 8 * s;
+            unsigned char* slot = smem + s * SH::SLOT;
+            const int q = q0 + n;
+            mbar_expect_tx(full, tx);
+            tma_load_4d(slot + SH::O_PHI, &maps.phi, z0 - 8, y0 - HALO, q, lane, full);
+            if (has_prev) tma_load_4d(slot + SH::O_PREV, &maps.prev, z0, y0, q - HALO, lane, full);
+            tma_load_3d(slot + SH::O_W0, &maps.w0, z0, y0, q, full);  // x face q-4 is stored at index q
+            tma_load_3d(slot + SH::O_W1, &maps.w1, z0, y0, q, full);  // y faces y0-4 .. y0+10
+            tma_load_3d(slot + SH::O_W2, &maps.w2, z0, y0, q, full);  // z faces z0-4 .. z0+TZ+3
+            tma_load_3d(slot + SH::O_INV, &maps.inv, z0, y0, q - HALO, full);
+            tma_load_4d(slot + SH::O_POT0, &maps.pot, z0, y0, q - HALO, g0, full);
+            tma_load_4d(slot + SH::O_POT1, &maps.pot, z0, y0, q - HALO, g1, full);
+            issued = n + 1;
+            if (++s == R) {
+                s = 0;
+                ph ^= 1;
+            }
+        }
+        if (issued < npl) {
+            // Leaving early: let the copies already issued land first (bounded).
+            for (int n = max(0, issued - R); n < issued; ++n) {
+                const unsigned long long start = globaltimer();
+                for (unsigned it = 0; it < (1u << 24); ++it)
+                    if (mbar_try_wait(bar_full + 8 * (n % R), (n / R) & 1) || globaltimer() - start > 100000000ull)
+                        break;
+            }
+        }
+        return;
+    }
+
+    if (warp >= SH::MW) {
+        // ------------------------------------------------------------------ pass groups
+        const int grp = (warp - SH::MW) / SH::PWG;
+        const int it = t - (SH::MW + grp * SH::PWG) * 32;  // item of the plane this thread takes
+        // The item's line segment: 22 nodes at stride ns from node offset nb, 15 face weights at
+        // stride ws from weight offset wb (both relative to the slot), 8 outputs at stride os from
+        // output offset ob (relative to the result slot), the first `first` of them not stored.
+        bool active = false;
+        int nb = 0, ns = 0, wb = 0, ws = 0, ob = 0, os = 0, first = 0;
+        if (it < TZ) {
+            // y: column zc, nodes y0-7 .. y0+14, faces y0-4 .. y0+10, outputs y0 .. y0+7
+            const int zc = it;
+            active = z0 + zc < nz;
+            nb = zc + 8;
+            ns = BW;
+            wb = SH::O_W1 / sizeof(S) + zc;
+            ws = TZ;
+            ob = zc;
+            os = TZ;
+        } else if (it < SH::ITEMS) {
+            // z: row ry, outputs zs .. zs+7 (tile-relative), nodes zs-7 .. zs+14, faces zs-4 .. zs+10
+            const int zi = it - TZ;
+            const int ry = zi % TY;
+            const int seg = zi / TY;
+            const int zs = min(seg * 8, TZ - 8);
+            first = seg * 8 - zs;
+            active = y0 + ry < ny && z0 + zs < nz;
+            nb = (ry + HALO) * BW + zs + 1;
+            ns = 1;
+            wb = SH::O_W2 / sizeof(S) + ry * (TZ + 8) + zs;
+            ws = 1;
+            ob = int(SH::YZ_Z / sizeof(E)) + ry * SH::ZROW + zs;
+            os = 1;
+        }
+        int s = grp, ph = 0;  // slot and phase parity of plane n
+        for (int n = grp; n < npl; n += NG) {
+            if (!warp_wait(bar_full + 8 * s, ph, a.token)) return;
+            const int q = q0 + n;
+            if (q >= xa && q <= xe) {
+                const int m = q - xa;
+                const int ys = m & (RY - 1);
+                const unsigned uy = m / RY;
+                if (uy >= 1 && !warp_wait(bar_yempty + 8 * ys, (uy - 1) & 1, a.token)) return;
+                if (active) {
+                    const unsigned char* slot = smem + s * SH::SLOT;
+                    const E* nodes = reinterpret_cast<const E*>(slot) + nb;
+                    const S* w = reinterpret_cast<const S*>(slot) + wb;
+                    E* out = reinterpret_cast<E*>(smem + SH::O_YZ + ys * SH::YZ_SLOT) + ob;
+                    E v[NROW];
+#pragma unroll
+                    for (int r = 0; r < NROW; ++r) v[r] = nodes[r * ns];
+                    E f[TY + 7];
+#pragma unroll
+                    for (int rf = 0; rf < TY + 7; ++rf) {
+                        E sum = Lane::zero();
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) sum = Lane::fma(tap[j], v[rf + j], sum);
+                        f[rf] = Lane::mul(Lane::splat(w[rf * ws]), sum);
+                    }
+#pragma unroll
+                    for (int o = 0; o < TY; ++o) {
+                        E acc = Lane::zero();
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) acc = Lane::fma(tap[j], f[o + 7 - j], acc);
+                        if (o >= first) out[o * os] = acc;
+                    }
+                }
+                __syncwarp();
+                if ((t & 31) == 0) mbar_arrive(bar_yfull + 8 * ys);
+            } else {
+                __syncwarp();
+            }
+            if ((t & 31) == 0) mbar_arrive(bar_empty + 8 * s);
+            s += NG;
+            if (s >= R) {
+                s -= R;
+                ph ^= 1;
+            }
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------------- march
+    const int ty = t / TZ;
+    const int tz = t - ty * TZ;
+    const int y = y0 + ty;
+    const int z = z0 + tz;
+    const bool own_in = y < ny && z < nz;
+    const bool own_pad = y < ny && z < nzp;
+    const int64_t plane_n = int64_t(ny) * nz;
+    const int own = ty * TZ + tz;  // index in the (TY, TZ) boxes
+
+    E cc, ca, cb;
+    {
+        const int64_t c0 = o0 / a.orb_per_group;  // one coefficient table per orbital group
+        const int64_t c1 = o1 / a.orb_per_group;
+        const double* r0 = a.coef + (c0 * a.degree + a.step) * 3;
+        const double* r1 = a.coef + (c1 * a.degree + a.step) * 3;
+        if constexpr (Lane::ORBITALS == 2) {
+            cc = make_float2(static_cast<float>(r0[0]), static_cast<float>(r1[0]));
+            ca = make_float2(static_cast<float>(r0[1]), static_cast<float>(r1[1]));
+            cb = make_float2(static_cast<float>(r0[2]), static_cast<float>(r1[2]));
+        } else {
+            cc = r0[0];
+            ca = r0[1];
+            cb = r0[2];
+        }
+    }
+
+    E phq[8], fq[8], yzq[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        phq[j] = Lane::zero();
+        fq[j] = Lane::zero();
+        yzq[j] = Lane::zero();
+    }
+
+    int s = 0, sph = 0;  // slot and phase parity of plane n
+    for (int n0 = 0; n0 < npl; n0 += 8) {
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+            const int n = n0 + g;
+            if (n >= npl) break;
+            if (!warp_wait(bar_full + 8 * s, sph, a.token)) return;
+            const unsigned char* slot = smem + s * SH::SLOT;
+            const int q = q0 + n;
+            phq[g] = reinterpret_cast<const E*>(slot + SH::O_PHI)[(ty + HALO) * BW + tz + 8];
+            {
+                E sum = Lane::zero();
+#pragma unroll
+                for (int j = 0; j < 8; ++j) sum = Lane::fma(tap[j], phq[(g + 1 + j) & 7], sum);
+                const S wx = own_in ? reinterpret_cast<const S*>(slot + SH::O_W0)[own] : S(0);
+                fq[g] = Lane::mul(Lane::splat(wx), sum);  // x face q - 4
+            }
+            if (q >= xa && q <= xe) {
+                const int m = q - xa;
+                const int ys = m & (RY - 1);
+                if (!warp_wait(bar_yfull + 8 * ys, (m / RY) & 1, a.token)) return;
+                const unsigned char* yz = smem + SH::O_YZ + ys * SH::YZ_SLOT;
+                yzq[g] = Lane::add(reinterpret_cast<const E*>(yz)[own],
+                                   reinterpret_cast<const E*>(yz + SH::YZ_Z)[ty * SH::ZROW + tz]);
+                __syncwarp();
+                if ((t & 31) == 0) mbar_arrive(bar_yempty + 8 * ys);
+            }
+            const int i = q - HALO;
+            if (i >= xa && own_pad) {
+                E xt = Lane::zero();
+#pragma unroll
+                for (int j = 0; j < 8; ++j) xt = Lane::fma(tap[j], fq[(g - j) & 7], xt);
+                const E div = Lane::add(xt, yzq[(g + 1) & 7]);
+                const int64_t pt = int64_t(i) * plane_n + (own_in ? int64_t(y) * nz + z : 0);
+                E res;
+                if (own_in) {
+                    const E phi = phq[(g + 1) & 7];
+                    const S inv = reinterpret_cast<const S*>(slot + SH::O_INV)[own];
+                    const E kin = Lane::mul(Lane::mul(div, Lane::splat(S(0.5))), Lane::splat(inv));
+                    E potv;
+                    if constexpr (Lane::ORBITALS == 2)
+                        potv = make_float2(reinterpret_cast<const S*>(slot + SH::O_POT0)[own],
+                                           reinterpret_cast<const S*>(slot + SH::O_POT1)[own]);
+                    else
+                        potv = reinterpret_cast<const S*>(slot + SH::O_POT0)[own];
+                    const E applied = Lane::fma(phi, potv, kin);
+                    res = Lane::mul(Lane::fma(Lane::neg(cc), phi, applied), ca);
+                    if (has_prev)
+                        res = Lane::fma(Lane::neg(cb), reinterpret_cast<const E*>(slot + SH::O_PREV)[own], res);
+                } else {
+                    res = Lane::zero();  // the padding column stays zero
+                }
+                if (a.final_out) {
+                    if (own_in) {
+                        if constexpr (Lane::ORBITALS == 2) {
+                            store_as<float>(a.out, a.out_dtype, o0 * (plane_n * nx) + pt, res.x);
+                            if (o0 + 1 < a.batch)
+                                store_as<float>(a.out, a.out_dtype, (o0 + 1) * (plane_n * nx) + pt, res.y);
+                        } else {
+                            store_as<double>(a.out, a.out_dtype, o0 * (plane_n * nx) + pt, res);
+                        }
+                    }
+                } else {
+                    E* out = static_cast<E*>(a.out);
+                    out[(int64_t(lane) * nx + i) * (int64_t(ny) * nzp) + int64_t(y) * nzp + z] = res;
+                }
+            }
+            __syncwarp();
+            if ((t & 31) == 0) mbar_arrive(bar_empty + 8 * s);
+            if (++s == R) {
+                s = 0;
+                sph ^= 1;
+            }
+        }
+    }
+}
+
+// Internal layout from a caller block: lanes of (nx, ny, nzp), padding and missing orbitals zero.
+template <typename Lane>
+__global__ void pack_lanes_kernel(const void* __restrict__ in, int in_dtype, int64_t batch, int nx, int ny, int nz,
+                                  int nzp, int64_t lanes, typename Lane::E* __restrict__ out) {
+    using E = typename Lane::E;
+    const int64_t per_lane = int64_t(nx) * ny * nzp;
+    const int64_t total = lanes * per_lane;
+    const int64_t n_points = int64_t(nx) * ny * nz;
+    for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+         idx += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t l = idx / per_lane;
+        const int64_t r = idx - l * per_lane;
+        const int zp = static_cast<int>(r % nzp);
+        const int64_t xy = r / nzp;
+        E v = Lane::zero();
+        if (zp < nz) {
+            const int64_t pt = xy * nz + zp;
+            if constexpr (Lane::ORBITALS == 2) {
+                const int64_t o = 2 * l;
+                v.x = load_as<float>(in, in_dtype, o * n_points + pt);
+                v.y = (o + 1 < batch) ? load_as<float>(in, in_dtype, (o + 1) * n_points + pt) : 0.f;
+            } else {
+                v = load_as<double>(in, in_dtype, l * n_points + pt);
+            }
+        }
+        out[idx] = v;
+    }
+}
+
+// rows x cols -> rows x cols_pad (zeros in the padding), for the geometry copies TMA reads.
+template <typename S>
+__global__ void pad_rows_kernel(const S* __restrict__ src, int64_t rows, int cols, int cols_pad, int64_t src_stride,
+                                S* __restrict__ dst) {
+    const int64_t total = rows * cols_pad;
+    for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+         idx += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t r = idx / cols_pad;
+        const int c = static_cast<int>(idx - r * cols_pad);
+        dst[idx] = c < cols ? src[r * src_stride + c] : S(0);
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// A tiled map over a C-ordered array dims[rank-1] x ... x dims[0] (dims[0] contiguous).
+int encode_map(CUtensorMap* map, CUtensorMapDataType type, int esize, int rank, void* base, const int64_t* dims,
+               const unsigned* box) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return CDFTB_ERR_LAUNCH;
+    cuuint64_t gdim[5], gstride[4];
+    cuuint32_t bdim[5], estr[5];
+    int64_t stride = esize;
+    for (int d = 0; d < rank; ++d) {
+        gdim[d] = cuuint64_t(dims[d]);
+        bdim[d] = box[d];
+        estr[d] = 1;
+        if (d >= 1) gstride[d - 1] = cuuint64_t(stride);
+        stride *= dims[d];
+    }
+    const CUresult r = enc(map, type, rank, base, gdim, gstride, bdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? CDFTB_OK : CDFTB_ERR_ARGUMENT;
+}
+
+int64_t lanes_of(const cdftb_operator* op, int64_t batch) { return op->dtype == CDFTB_F32 ? (batch + 1) / 2 : batch; }
+
+int padded_z(int nz) { return nz + (nz & 1); }
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+int64_t systems_of(const cdftb_operator* op, int64_t batch) {
+    return op->potential_stride == 0 ? 1 : ceil_div(batch, op->orbitals_per_group);
+}
+
+// Element counts of the padded geometry copies: w0, w1, w2, inv, potentials.
+struct GeoPack {
+    int nzg, nz8g;
+    int64_t n_w0, n_w1, n_w2, n_inv, n_pot;
+    int64_t total() const { return n_w0 + n_w1 + n_w2 + n_inv + n_pot; }
+};
+
+GeoPack geo_pack(const cdftb_operator* op, int64_t batch) {
+    const int per16 = op->dtype == CDFTB_F32 ? 4 : 2;
+    GeoPack g{};
+    g.nzg = static_cast<int>(round_up(op->nz, per16));
+    g.nz8g = static_cast<int>(round_up(op->nz + 8, per16));
+    const int64_t nx = op->nx, ny = op->ny;
+    g.n_w0 = round_up((nx + 8) * ny * g.nzg, per16);
+    g.n_w1 = round_up(nx * (ny + 8) * g.nzg, per16);
+    g.n_w2 = round_up(nx * ny * g.nz8g, per16);
+    g.n_inv = round_up(nx * ny * g.nzg, per16);
+    g.n_pot = systems_of(op, batch) * nx * ny * g.nzg;
+    return g;
+}
+
+// The z tile (32 or 36 columns) that wastes the fewest columns of the padded row.
+int choose_tz(int nzp) {
+    const int64_t w32 = ceil_div(nzp, 32) * 32;
+    const int64_t w36 = ceil_div(nzp, 36) * 36;
+    return w36 < w32 ? 36 : 32;
+}
+
+// x chunks: one CTA per SM is resident and a CTA's time grows with the planes it marches (its
+// chunk plus 14 halo planes), so pick the chunk count that minimises waves x planes.
+int choose_chunk(int nx, int64_t ctas_per_chunkset, int sms) {
+    int best = nx;
+    int64_t best_cost = -1;
+    for (int chunks = 1; chunks <= 16; ++chunks) {
+        const int len = static_cast<int>(ceil_div(nx, chunks));
+        if (chunks > 1 && len < 8) break;
+        const int64_t waves = ceil_div(ctas_per_chunkset * ceil_div(nx, len), sms);
+        const int64_t cost = waves * (len + 2 * HALO);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = len;
+        }
+    }
+    return best;
+}
+
+int sm_count() {
+    static int count = 0;
+    if (count == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || count <= 0)
+            count = 148;
+    }
+    return count;
+}
+
+template <typename Lane, int TZ>
+int launch_slab(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream) {
+    using SH = Shape<TZ, sizeof(typename Lane::S)>;
+    static bool configured = false;
+    if (!configured) {
+        int st = check(cudaFuncSetAttribute(slab_filter_kernel<Lane, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(SH::BYTES)));
+        if (st != CDFTB_OK) return st;
+        configured = true;
+    }
+    const int tiles_y = static_cast<int>(ceil_div(a.ny, TY));
+    a.tiles_z = static_cast<int>(ceil_div(a.nzp, TZ));
+    const int64_t tiles = int64_t(tiles_y) * a.tiles_z;
+    a.xchunk = choose_chunk(a.nx, tiles * lanes, sm_count());
+    const int chunks = static_cast<int>(ceil_div(a.nx, a.xchunk));
+    static unsigned next_token = 0;
+    for (int64_t first = 0; first < lanes; first += 65535) {
+        const int64_t count = (lanes - first) < 65535 ? (lanes - first) : 65535;
+        a.lane_first = first;
+        next_token = (next_token + 1) & 0x7fffffffu;
+        if (next_token == 0) next_token = 1;
+        a.token = next_token;
+        dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(chunks), static_cast<unsigned>(count));
+        slab_filter_kernel<Lane, TZ><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
+        int st = check_launch();
+        if (st != CDFTB_OK) return st;
+    }
+    return CDFTB_OK;
+}
+
+template <typename S>
+int pad_rows(const void* src, int64_t rows, int cols, int cols_pad, S* dst, cudaStream_t stream) {
+    const int64_t total = rows * cols_pad;
+    const unsigned blocks = static_cast<unsigned>(std::min<int64_t>(ceil_div(total, 256), 148 * 16));
+    pad_rows_kernel<S><<<blocks, 256, 0, stream>>>(static_cast<const S*>(src), rows, cols, cols_pad, cols, dst);
+    return check_launch();
+}
+
+template <typename Lane>
+int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype, void* work,
+                int64_t batch, const double* coefficients, int degree, cudaStream_t stream) {
+    using S = typename Lane::S;
+    const int nx = op->nx, ny = op->ny, nz = op->nz;
+    const int nzp = padded_z(nz);
+    const int64_t lanes = lanes_of(op, batch);
+    const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
+    char* w = static_cast<char*>(work);
+    void* buf[3] = {w, w + lanes * lane_bytes, w + 2 * lanes * lane_bytes};
+    const GeoPack gp = geo_pack(op, batch);
+    S* geo = reinterpret_cast<S*>(w + 3 * lanes * lane_bytes);
+    S* w0p = geo;
+    S* w1p = w0p + gp.n_w0;
+    S* w2p = w1p + gp.n_w1;
+    S* invp = w2p + gp.n_w2;
+    S* potp = invp + gp.n_inv;
+    const int64_t nsys = systems_of(op, batch);
+    int st;
+    {
+        const int64_t total = lanes * int64_t(nx) * ny * nzp;
+        const unsigned blocks = static_cast<unsigned>(std::min<int64_t>(ceil_div(total, 256), 148 * 16));
+        pack_lanes_kernel<Lane><<<blocks, 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
+                                                            static_cast<typename Lane::E*>(buf[2]));
+        if ((st = check_launch()) != CDFTB_OK) return st;
+    }
+    if ((st = pad_rows<S>(op->face_weights[0], int64_t(nx + 8) * ny, nz, gp.nzg, w0p, stream)) != CDFTB_OK) return st;
+    if ((st = pad_rows<S>(op->face_weights[1], int64_t(nx) * (ny + 8), nz, gp.nzg, w1p, stream)) != CDFTB_OK) return st;
+    if ((st = pad_rows<S>(op->face_weights[2], int64_t(nx) * ny, nz + 8, gp.nz8g, w2p, stream)) != CDFTB_OK) return st;
+    if ((st = pad_rows<S>(op->inverse_weight, int64_t(nx) * ny, nz, gp.nzg, invp, stream)) != CDFTB_OK) return st;
+    for (int64_t g = 0; g < nsys; ++g) {
+        const void* src = static_cast<const S*>(op->potential) + g * op->potential_stride;
+        if ((st = pad_rows<S>(src, int64_t(nx) * ny, nz, gp.nzg, potp + g * int64_t(nx) * ny * gp.nzg, stream)) !=
+            CDFTB_OK)
+            return st;
+    }
+
+    const int tz = choose_tz(nzp);
+    const CUtensorMapDataType gt = Lane::GEO_TYPE;
+    const int sb = sizeof(S);
+    FilterMaps maps[3];
+    for (int b = 0; b < 3; ++b) {
+        const int64_t lane_dims[4] = {nzp, ny, nx, lanes};
+        const unsigned phi_box[4] = {unsigned(tz + 18), unsigned(NROW), 1, 1};
+        const unsigned prev_box[4] = {unsigned(tz), unsigned(TY), 1, 1};
+        if ((st = encode_map(&maps[b].phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf[b], lane_dims, phi_box)) !=
+            CDFTB_OK)
+            return st;
+        if ((st = encode_map(&maps[b].prev, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf[b], lane_dims, prev_box)) !=
+            CDFTB_OK)
+            return st;
+    }
+    FilterMaps geo_maps{};
+    {
+        const unsigned tile_box[3] = {unsigned(tz), unsigned(TY), 1};
+        const int64_t d_w0[3] = {gp.nzg, ny, nx + 8};
+        const int64_t d_w1[3] = {gp.nzg, ny + 8, nx};
+        const unsigned b_w1[3] = {unsigned(tz), unsigned(TY + 7), 1};
+        const int64_t d_w2[3] = {gp.nz8g, ny, nx};
+        const unsigned b_w2[3] = {unsigned(tz + 8), unsigned(TY), 1};
+        const int64_t d_inv[3] = {gp.nzg, ny, nx};
+        const int64_t d_pot[4] = {gp.nzg, ny, nx, nsys};
+        const unsigned b_pot[4] = {unsigned(tz), unsigned(TY), 1, 1};
+        if ((st = encode_map(&geo_maps.w0, gt, sb, 3, w0p, d_w0, tile_box)) != CDFTB_OK) return st;
+        if ((st = encode_map(&geo_maps.w1, gt, sb, 3, w1p, d_w1, b_w1)) != CDFTB_OK) return st;
+        if ((st = encode_map(&geo_maps.w2, gt, sb, 3, w2p, d_w2, b_w2)) != CDFTB_OK) return st;
+        if ((st = encode_map(&geo_maps.inv, gt, sb, 3, invp, d_inv, tile_box)) != CDFTB_OK) return st;
+        if ((st = encode_map(&geo_maps.pot, gt, sb, 4, potp, d_pot, b_pot)) != CDFTB_OK) return st;
+    }
+    StaggeredTaps taps = staggered_taps(8);
+    FilterArgs a{};
+    a.nx = nx;
+    a.ny = ny;
+    a.nz = nz;
+    a.nzp = nzp;
+    a.batch = batch;
+    a.orb_per_group = op->orbitals_per_group;
+    a.shared_potential = op->potential_stride == 0;
+    a.coef = coefficients;
+    a.degree = degree;
+    const double scale = 1.0 / op->spacing;  // taps c_k * (1/h), divergence.py:112, 121
+    for (int j = 0; j < 8; ++j) a.taps[j] = taps.c[j] * scale;
+    // Y_1 -> buf0, Y_2 -> buf1, then Y_{k+1} overwrites Y_{k-1} in place (a point's previous value
+    // is read only by the CTA that writes that point); the packed block is buf2.
+    int y = 2, prev = -1;
+    for (int k = 1; k <= degree; ++k) {
+        const int dst = (k == 1) ? 0 : (k == 2 ? 1 : prev);
+        a.has_prev = prev >= 0;
+        a.step = k - 1;
+        a.final_out = k == degree;
+        a.out = a.final_out ? out : buf[dst];
+        a.out_dtype = out_dtype;
+        FilterMaps m = geo_maps;
+        m.phi = maps[y].phi;
+        m.prev = maps[prev >= 0 ? prev : y].prev;
+        st = tz == 36 ? launch_slab<Lane, 36>(m, a, lanes, stream) : launch_slab<Lane, 32>(m, a, lanes, stream);
+        if (st != CDFTB_OK) return st;
+        prev = y;
+        y = dst;
+    }
+    return CDFTB_OK;
+}
+
+}  // namespace
+
+int64_t slab_filter_work_bytes(const cdftb_operator* op, int64_t batch) {
+    const int64_t sb = op->dtype == CDFTB_F32 ? 4 : 8;
+    return 3 * lanes_of(op, batch) * int64_t(op->nx) * op->ny * padded_z(op->nz) * 8 + geo_pack(op, batch).total() * sb;
+}
+
+bool slab_filter_applies(const cdftb_operator* op) {
+    return op->accuracy == 8 && (op->dtype == CDFTB_F32 || op->dtype == CDFTB_F64) && op->nx > 0 && op->ny > 0 &&
+           op->nz > 0;
+}
+
+int slab_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
+                          void* work, int64_t batch, const double* coefficients, int degree, cudaStream_t stream) {
+    if (op->dtype == CDFTB_F32)
+        return slab_filter<LaneF2>(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
+    return slab_filter<LaneD>(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
+}
+
+}  // namespace cdftb
+
+extern "C" int cdftb_device_status(int* flags) {
+    if (!flags) return CDFTB_ERR_ARGUMENT;
+    int v = 0;
+    int st = cdftb::check(cudaMemcpyFromSymbol(&v, cdftb::g_device_error, sizeof(int)));
+    if (st != CDFTB_OK) return st;
+    *flags = v;
+    if (v) {
+        const int zero = 0;
+        st = cdftb::check(cudaMemcpyToSymbol(cdftb::g_device_error, &zero, sizeof(int)));
+        if (st != CDFTB_OK) return st;
+    }
+    return v ? CDFTB_ERR_TIMEOUT : CDFTB_OK;
+}
+
+extern "C" int64_t cdftb_chebyshev_filter_work_bytes(const cdftb_operator* op, int64_t batch) {
+    if (!op || batch <= 0 || op->nx <= 0 || op->ny <= 0 || op->nz <= 0) return 0;
+    if (cdftb::slab_filter_applies(op)) return cdftb::slab_filter_work_bytes(op, batch);
+    const int64_t esize = op->dtype == CDFTB_F64 ? 8 : 4;
+    return 3 * batch * int64_t(op->nx) * op->ny * op->nz * esize;
+}
+
+extern "C" int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out,
+                                      int out_dtype, void* work, int64_t work_bytes, int64_t batch,
+                                      const double* coefficients, int degree, cdftb_stream_t stream) {
+    if (!op || !block || !out || !work || !coefficients || degree < 1 || batch < 0) return CDFTB_ERR_ARGUMENT;
+    if (batch == 0) return CDFTB_OK;
+    if (op->nx <= 0 || op->ny <= 0 || op->nz <= 0 || !(op->spacing > 0.0)) return CDFTB_ERR_ARGUMENT;
+    if (work_bytes < cdftb_chebyshev_filter_work_bytes(op, batch)) return CDFTB_ERR_ARGUMENT;
+    if (op->dtype != CDFTB_F64 && op->dtype != CDFTB_F32) return CDFTB_ERR_ARGUMENT;
+    if ((in_dtype != CDFTB_F64 && in_dtype != CDFTB_F32) || (out_dtype != CDFTB_F64 && out_dtype != CDFTB_F32))
+        return CDFTB_ERR_ARGUMENT;
+    if (!op->face_weights[0] || !op->face_weights[1] || !op->face_weights[2] || !op->inverse_weight ||
+        !op->potential || op->orbitals_per_group <= 0)
+        return CDFTB_ERR_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(work) % 16 != 0) return CDFTB_ERR_ARGUMENT;
+    if (cdftb::slab_filter_applies(op))
+        return cdftb::slab_chebyshev_filter(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree,
+                                            cdftb::as_stream(stream));
+    return cdftb::generic_chebyshev_filter(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree,
+                                           stream);
+}

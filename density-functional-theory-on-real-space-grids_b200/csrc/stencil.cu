@@ -545,11 +545,11 @@ extern "C" int cdftb_cusp_apply(const cdftb_operator* op, const void* phi, int i
     return launch(a, op->accuracy, op->spacing, op->dtype, as_stream(stream));
 }
 
-extern "C" int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out,
-                                      int out_dtype, void* work, int64_t batch, const double* coefficients,
-                                      int degree, cdftb_stream_t stream) {
-    if (!op || !block || !out || !work || !coefficients || degree < 1) return CDFTB_ERR_ARGUMENT;
-    if (batch == 0) return CDFTB_OK;
+// The filter for any order on the caller's layout: each step one stencil_kernel launch. Used for
+// the orders the slab filter (filter.cu) does not take; work holds 3 * batch * N elements.
+int cdftb::generic_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out,
+                                    int out_dtype, void* work, int64_t batch, const double* coefficients, int degree,
+                                    cdftb_stream_t stream) {
     const int64_t n_points = static_cast<int64_t>(op->nx) * op->ny * op->nz;
     const int esize = op->dtype == CDFTB_F64 ? 8 : 4;
     const int dt = op->dtype;

@@ -56,6 +56,12 @@ def chebyshev_filter(hamiltonian, block: torch.Tensor, degree: int, lower: float
                              precision=precision)
 
 
+def filter_workspace(op, batch: int, device: torch.device) -> torch.Tensor:
+    """Device scratch of the fused filter (``cdftb_chebyshev_filter_work_bytes``), as bytes."""
+    nbytes = _lib.library().cdftb_chebyshev_filter_work_bytes(ctypes.byref(op), batch)
+    return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+
 def filter_with_table(hamiltonian, block: torch.Tensor, table: torch.Tensor, degree: int, *, orbitals_per_group: int,
                       potential: torch.Tensor | None = None, precision: torch.dtype | None = None) -> torch.Tensor:
     """Run the fused filter with a device coefficient table ``(groups, degree, 3)``."""
@@ -67,11 +73,11 @@ def filter_with_table(hamiltonian, block: torch.Tensor, table: torch.Tensor, deg
     if work_dtype != hamiltonian.dtype:
         raise ValueError("the filter runs in the Hamiltonian's dtype; build it with dtype=float32 for the mixed form")
     out = torch.empty_like(x)
-    work = torch.empty((3, batch, n), dtype=work_dtype, device=x.device)
     op = hamiltonian.operator(potential, orbitals_per_group=orbitals_per_group)
+    work = filter_workspace(op, batch, x.device)
     hamiltonian.note_applications(degree)
     call("cdftb_chebyshev_filter", ctypes.byref(op), ptr(x), _lib.dtype_code(x), ptr(out), _lib.dtype_code(out),
-         ptr(work), batch, ptr(table.contiguous()), degree, stream_handle(x.device))
+         ptr(work), work.numel(), batch, ptr(table.contiguous()), degree, stream_handle(x.device))
     return out
 
 

@@ -82,11 +82,20 @@ int cdftb_stencil_set_tile(int tile_y, int min_chunk, int ctas_per_sm);
  * chebyshev_filter / chebyshev_recurrence, with fused.py:391 chebyshev_update fused into each apply).
  * coefficients: device table (groups, degree, 3) of rows (c, a_k, b_k) from chefsi.py:116
  * chebyshev_coefficients, one table per potential group. block and out are in_dtype/out_dtype
- * (a double block with a float operator is cast once); work holds three blocks of the operator's
- * dtype (3 * batch * N elements). The input block is never written. */
+ * (a double block with a float operator is cast once); work is device scratch of at least
+ * cdftb_chebyshev_filter_work_bytes(op, batch) bytes, given as work_bytes. The input block is never
+ * written. Order 8 runs the slab filter (internal layout: float32 orbitals interleaved in pairs, z
+ * padded to even; TMA-staged tiles, bounded waits reported by cdftb_device_status); other orders
+ * run one stencil launch per step on the caller's layout. */
+int64_t cdftb_chebyshev_filter_work_bytes(const cdftb_operator* op, int64_t batch);
 int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
-                           void* work, int64_t batch, const double* coefficients, int degree,
+                           void* work, int64_t work_bytes, int64_t batch, const double* coefficients, int degree,
                            cdftb_stream_t stream);
+
+/* No reference counterpart: the error flags the library's kernels set on the device (bit 0: a
+ * bounded wait on a TMA barrier gave up). Synchronises the device, returns the flags in *flags and
+ * clears them; status CDFTB_ERR_TIMEOUT when any flag was set. */
+int cdftb_device_status(int* flags);
 
 /* (e1) out[g][i][j] = sum_p q[p] a[g][i][p] b[g][j][p] (src/cdft/eigen/measure.py:72-96,
  * Measure.inner/gram/cross), f64, deterministic two-pass reduction. a and b hold `groups`

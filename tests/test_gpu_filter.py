@@ -1,0 +1,129 @@
+"""The slab Chebyshev filter (order 8) against the oracle on random operators.
+
+Covers the internal layout's edge cases: odd and even nz (padding column), grids smaller than a
+tile or than a group of 8 planes, both z tiles (32 and 36 columns), x chunking, an odd number of
+float32 orbitals (a half-empty lane), several systems with their own potentials and coefficient
+tables in one call (a lane whose two orbitals belong to different systems), and degrees 1 and 2.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import eigen as oeigen
+from oracle.grid import Grid
+from oracle.operators import CuspHamiltonian
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def _random_operator(shape, seed):
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = shape
+    faces = (rng.uniform(0.5, 1.5, (nx + 8, ny, nz)), rng.uniform(0.5, 1.5, (nx, ny + 8, nz)),
+             rng.uniform(0.5, 1.5, (nx, ny, nz + 8)))
+    inv = rng.uniform(0.5, 1.5, shape).ravel()
+    q = rng.uniform(0.5, 1.5, shape).ravel()
+    return faces, inv, q
+
+
+def _pair(pkg, cuda, shape, spacing, faces, inv, q, pot, dtype=torch.float64):
+    grid_o = Grid(shape, spacing, (0.0, 0.0, 0.0))
+    ham_o = CuspHamiltonian(grid_o, SimpleNamespace(face_weights=lambda order: faces), None, bare=(pot, inv, q))
+    grid = pkg.UniformGrid(shape, spacing, (0.0, 0.0, 0.0), device=cuda)
+    dev_faces = tuple(_t(w, cuda) for w in faces)
+    bare = (_t(pot, cuda), _t(inv, cuda), pkg.Measure(grid, _t(q, cuda)))
+    ham = pkg.CuspFactoredHamiltonian(grid, SimpleNamespace(face_weights=lambda acc: dev_faces), bare=bare,
+                                      dtype=dtype)
+    return ham_o, ham
+
+
+def _device_status(pkg):
+    flags = ctypes.c_int(-1)
+    status = pkg._lib.library().cdftb_device_status(ctypes.byref(flags))
+    return status, flags.value
+
+
+SHAPES = [(9, 11, 13), (12, 17, 24), (5, 9, 40), (33, 20, 70), (21, 8, 65)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("batch", [1, 3, 4])
+def test_slab_filter_float64(pkg, cuda, shape, batch):
+    faces, inv, q = _random_operator(shape, seed=sum(shape) + batch)
+    pot = np.random.default_rng(7).standard_normal(int(np.prod(shape)))
+    ham_o, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot)
+    block = np.random.default_rng(batch).standard_normal((batch, int(np.prod(shape))))
+    for degree in (1, 2, 5):
+        want = oeigen.chebyshev_filter(ham_o, block, degree, 0.5, 3.0, -1.0)
+        got = pkg.chebyshev_filter(ham, _t(block, cuda), degree, 0.5, 3.0, -1.0).cpu().numpy()
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-12 * np.abs(want).max())
+    assert _device_status(pkg) == (0, 0)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("batch", [1, 3, 4])
+def test_slab_filter_float32(pkg, cuda, shape, batch):
+    faces, inv, q = _random_operator(shape, seed=sum(shape) + batch)
+    pot = np.random.default_rng(7).standard_normal(int(np.prod(shape)))
+    ham_o, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot, dtype=torch.float32)
+    block = np.random.default_rng(batch).standard_normal((batch, int(np.prod(shape))))
+    want = oeigen.chebyshev_filter(ham_o, block, 5, 0.5, 3.0, -1.0)
+    got = pkg.chebyshev_filter(ham, _t(block, cuda), 5, 0.5, 3.0, -1.0).cpu().numpy()
+    assert got.dtype == np.float64
+    np.testing.assert_allclose(got, want, rtol=0, atol=2e-5 * np.abs(want).max())
+    assert _device_status(pkg) == (0, 0)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_slab_filter_many_systems(pkg, cuda, dtype):
+    """Three systems x three orbitals: per-system potentials and coefficient tables in one call."""
+    from importlib import import_module
+
+    eigen = import_module(pkg.__name__ + ".eigen")
+    shape = (14, 13, 29)
+    n = int(np.prod(shape))
+    faces, inv, q = _random_operator(shape, seed=3)
+    rng = np.random.default_rng(5)
+    pots = rng.standard_normal((3, n))
+    blocks = rng.standard_normal((3, 3, n))
+    bounds = [(0.5, 3.0, -1.0), (0.2, 4.0, -0.5), (1.0, 2.5, -2.0)]
+    degree = 6
+    table = torch.tensor([eigen.chebyshev_coefficients(degree, *b) for b in bounds], dtype=torch.float64,
+                         device=cuda)
+    _, ham = _pair(pkg, cuda, shape, 0.25, faces, inv, q, pots[0], dtype=dtype)
+    got = eigen.filter_with_table(ham, _t(blocks, cuda), table, degree, orbitals_per_group=3,
+                                  potential=_t(pots, cuda)).cpu().numpy()
+    tol = 1e-12 if dtype == torch.float64 else 2e-5
+    for s in range(3):
+        ham_o, _ = _pair(pkg, cuda, shape, 0.25, faces, inv, q, pots[s])
+        want = oeigen.chebyshev_filter(ham_o, blocks[s], degree, *bounds[s])
+        np.testing.assert_allclose(got[s], want, rtol=0, atol=tol * np.abs(want).max())
+    assert _device_status(pkg) == (0, 0)
+
+
+def test_filter_work_bytes_is_checked(pkg, cuda):
+    shape = (9, 11, 13)
+    faces, inv, q = _random_operator(shape, seed=1)
+    pot = np.zeros(int(np.prod(shape)))
+    _, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot, dtype=torch.float32)
+    op = ham.operator()
+    lib = pkg._lib.library()
+    need = lib.cdftb_chebyshev_filter_work_bytes(ctypes.byref(op), 3)
+    assert need >= 3 * 2 * 9 * 11 * 14 * 8  # three blocks of two float2 lanes of (9, 11, 14), plus geometry
+    block = torch.zeros((3, int(np.prod(shape))), dtype=torch.float64, device=cuda)
+    out = torch.empty_like(block)
+    work = torch.empty(need - 8, dtype=torch.uint8, device=cuda)
+    table = torch.zeros((1, 2, 3), dtype=torch.float64, device=cuda)
+    status = lib.cdftb_chebyshev_filter(ctypes.byref(op), block.data_ptr(), 0, out.data_ptr(), 0, work.data_ptr(),
+                                        need - 8, 3, table.data_ptr(), 2, None)
+    assert status == 1  # CDFTB_ERR_ARGUMENT: the work buffer is too small

@@ -1,17 +1,19 @@
 // (c) The Coulomb-cutoff Poisson solve (src/cdft/operators/poisson.py:21-107) as five pruned
-// axis-wise transforms on the device, with the truncated kernel K(G) fused into the x pass.
+// axis-wise FFT passes on the device, with the truncated kernel K(G) fused into the x pass.
 //
-// The density occupies the first n of the N = fft_friendly(ceil(2.5 n)) points of every padded
-// axis and only the first n outputs are read back, so each pass transforms exactly the non-zero
-// lines and computes only the needed outputs:
+// The density occupies the first n of the N = fft_friendly(ceil(pad n)) points of every padded
+// axis and only the first n outputs are read back, so each pass transforms only lines that can be
+// non-zero and keeps only the outputs a later pass reads:
 //   pass 1  z, real -> half complex      rho[x][y][z]        -> A[x][y][kz]    (x < nx, y < ny)
 //   pass 2  y, forward                   A[x][y][kz]         -> B[x][ky][kz]   (x < nx)
 //   pass 3  x, forward, * K, inverse     B[x][ky][kz]        -> B[x][ky][kz]   (in place, x < nx)
 //   pass 4  y, inverse                   B[x][ky][kz]        -> A[x][y][kz]    (y < ny)
 //   pass 5  z, half complex -> real      A[x][y][kz]         -> v[x][y][z]     (z < nz), / (Nx Ny Nz)
-// Each pass stages the lines it transforms in shared memory and sums against a table of the N-th
-// roots of unity (a direct pruned DFT per line). The result is what rfftn / *K / irfftn of the
-// zero-padded box gives, up to round-off (pocketfft / cuFFT re-associate differently).
+// Every pass is one CTA per L lines: the lines are staged in shared memory as [element][line] (row
+// stride L + 1, so that both the FFT stages and the transposed loads and stores avoid bank
+// conflicts) and transformed by a mixed-radix Stockham FFT (radices 4, 2, 3, 5; each stage reads
+// one buffer and writes the other, in natural order, with per-stage twiddle tables made on the host
+// in double precision). The result is rfftn / *K / irfftn of the zero-padded box up to round-off.
 
 #include <math.h>
 
@@ -25,185 +27,224 @@ struct cplx {
     double re, im;
 };
 
+__device__ __forceinline__ cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ cplx scale(cplx a, double s) { return {a.re * s, a.im * s}; }
 __device__ __forceinline__ cplx cmul(cplx a, cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ cplx cmulc(cplx a, cplx b) { return {a.re * b.re + a.im * b.im, a.im * b.re - a.re * b.im}; }
+// i * sign * a
+__device__ __forceinline__ cplx rot(cplx a, int sign) { return sign < 0 ? cplx{a.im, -a.re} : cplx{-a.im, a.re}; }
 
-constexpr int LANES = 32;
+constexpr int MAX_STAGES = 16;
 
-// Middle-axis transform: data viewed as [outer][n][inner]; for every (outer, inner) line computes
-// out[outer][k][inner] = sum_{j < n_in} in[outer][j][inner] * root^(sign * j * k), k < n_out.
-// One CTA per (outer, 32 consecutive inner); the line segment lives in shared memory.
-__global__ void dft_middle_kernel(const cplx* __restrict__ in, int64_t in_outer_stride, int n_in, cplx* __restrict__ out,
-                                  int64_t out_outer_stride, int n_out, int64_t inner, const cplx* __restrict__ roots,
-                                  int n_fft, int sign) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx* s_in = reinterpret_cast<cplx*>(smem_raw);  // [n_in][LANES]
-    cplx* s_root = s_in + static_cast<int64_t>(n_in) * LANES;
-    const int64_t o = blockIdx.y;
-    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * LANES;
-    const int tx = threadIdx.x;
-    const int ty = threadIdx.y;
-    const int tid = ty * LANES + tx;
-    const int nthreads = LANES * blockDim.y;
-    for (int r = tid; r < n_fft; r += nthreads) s_root[r] = roots[r];
-    const cplx* src = in + o * in_outer_stride;
-    for (int idx = tid; idx < n_in * LANES; idx += nthreads) {
-        const int j = idx / LANES;
-        const int l = idx - j * LANES;
-        const int64_t ii = i0 + l;
-        s_in[idx] = (ii < inner) ? src[static_cast<int64_t>(j) * inner + ii] : cplx{0.0, 0.0};
-    }
-    __syncthreads();
-    const int64_t ii = i0 + tx;
-    if (ii >= inner) return;
-    cplx* dst = out + o * out_outer_stride;
-    for (int k = ty; k < n_out; k += blockDim.y) {
-        double re = 0.0, im = 0.0;
-        int idx = 0;  // (j * k) mod n_fft, advanced incrementally
-        for (int j = 0; j < n_in; ++j) {
-            cplx w = s_root[idx];
-            if (sign < 0) w.im = -w.im;
-            const cplx x = s_in[j * LANES + tx];
-            re += x.re * w.re - x.im * w.im;
-            im += x.re * w.im + x.im * w.re;
-            idx += k;
-            if (idx >= n_fft) idx -= n_fft;
+// One axis: N = product of radix[0..nst); stage st has stride s (product of the earlier radices),
+// m = N / (s * radix) and twiddles tw[tw_off + p * (radix - 1) + k - 1] = exp(-2 pi i p k / (N / s)).
+struct FftPlan {
+    int n;
+    int nst;
+    int radix[MAX_STAGES];
+    int stride[MAX_STAGES];
+    int m[MAX_STAGES];
+    int tw_off[MAX_STAGES];
+    const cplx* tw;
+};
+
+// Radix-R DFT with the rotation exp(sign 2 pi i / R) (sign -1 forward, +1 inverse).
+template <int R>
+__device__ __forceinline__ void dft_radix(cplx* a, int sign);
+
+template <>
+__device__ __forceinline__ void dft_radix<2>(cplx* a, int) {
+    const cplx t = a[0] - a[1];
+    a[0] = a[0] + a[1];
+    a[1] = t;
+}
+
+template <>
+__device__ __forceinline__ void dft_radix<4>(cplx* a, int sign) {
+    const cplx t0 = a[0] + a[2], t1 = a[0] - a[2], t2 = a[1] + a[3], t3 = rot(a[1] - a[3], sign);
+    a[0] = t0 + t2;
+    a[1] = t1 + t3;
+    a[2] = t0 - t2;
+    a[3] = t1 - t3;
+}
+
+template <>
+__device__ __forceinline__ void dft_radix<3>(cplx* a, int sign) {
+    constexpr double s3 = 0.86602540378443864676;  // sqrt(3) / 2
+    const cplx t = a[1] + a[2];
+    const cplx v = rot(scale(a[1] - a[2], s3), sign);
+    const cplx h = {a[0].re - 0.5 * t.re, a[0].im - 0.5 * t.im};
+    a[0] = a[0] + t;
+    a[1] = h + v;
+    a[2] = h - v;
+}
+
+template <>
+__device__ __forceinline__ void dft_radix<5>(cplx* a, int sign) {
+    constexpr double c1 = 0.30901699437494742410;   // cos(2 pi / 5)
+    constexpr double c2 = -0.80901699437494742410;  // cos(4 pi / 5)
+    constexpr double s1 = 0.95105651629515357212;   // sin(2 pi / 5)
+    constexpr double s2 = 0.58778525229247312917;   // sin(4 pi / 5)
+    const cplx t1 = a[1] + a[4], t2 = a[2] + a[3], t3 = a[1] - a[4], t4 = a[2] - a[3];
+    const cplx x1 = {a[0].re + c1 * t1.re + c2 * t2.re, a[0].im + c1 * t1.im + c2 * t2.im};
+    const cplx x2 = {a[0].re + c2 * t1.re + c1 * t2.re, a[0].im + c2 * t1.im + c1 * t2.im};
+    const cplx y1 = rot({s1 * t3.re + s2 * t4.re, s1 * t3.im + s2 * t4.im}, sign);
+    const cplx y2 = rot({s2 * t3.re - s1 * t4.re, s2 * t3.im - s1 * t4.im}, sign);
+    a[0] = a[0] + t1 + t2;
+    a[1] = x1 + y1;
+    a[2] = x2 + y2;
+    a[3] = x2 - y2;
+    a[4] = x1 - y1;
+}
+
+template <int R>
+__device__ __forceinline__ void stage_radix(const cplx* __restrict__ x, cplx* __restrict__ y, int s, int m,
+                                            const cplx* __restrict__ tw, int sign, int lp, int lane, int ty, int nty,
+                                            int nb) {
+    for (int b = ty; b < nb; b += nty) {
+        const int p = b / s;
+        const int q = b - p * s;
+        cplx a[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) a[j] = x[(q + s * (p + j * m)) * lp + lane];
+        dft_radix<R>(a, sign);
+        const cplx* w = tw + p * (R - 1);
+        y[(q + s * R * p) * lp + lane] = a[0];
+#pragma unroll
+        for (int k = 1; k < R; ++k) {
+            const cplx wk = w[k - 1];
+            y[(q + s * (R * p + k)) * lp + lane] = sign < 0 ? cmul(a[k], wk) : cmulc(a[k], wk);
         }
-        dst[static_cast<int64_t>(k) * inner + ii] = {re, im};
     }
 }
 
-// Pass 3: along x for 32 (ky, kz) lines per CTA: forward (nx -> Nx), times K, inverse (Nx -> nx),
-// written back in place.
-__global__ void dft_x_kernel_fused(cplx* __restrict__ data, int nx, int64_t inner, const double* __restrict__ kernel,
-                                   const cplx* __restrict__ roots, int n_fft) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx* s_in = reinterpret_cast<cplx*>(smem_raw);        // [nx][LANES]
-    cplx* s_mid = s_in + static_cast<int64_t>(nx) * LANES;  // [n_fft][LANES]
-    cplx* s_root = s_mid + static_cast<int64_t>(n_fft) * LANES;
-    const int64_t b = blockIdx.y;
-    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * LANES;
-    const int tx = threadIdx.x;
-    const int ty = threadIdx.y;
-    const int tid = ty * LANES + tx;
-    const int nthreads = LANES * blockDim.y;
-    cplx* col = data + b * static_cast<int64_t>(nx) * inner;
-    for (int r = tid; r < n_fft; r += nthreads) s_root[r] = roots[r];
-    for (int idx = tid; idx < nx * LANES; idx += nthreads) {
-        const int j = idx / LANES;
-        const int l = idx - j * LANES;
-        const int64_t ii = i0 + l;
-        s_in[idx] = (ii < inner) ? col[static_cast<int64_t>(j) * inner + ii] : cplx{0.0, 0.0};
-    }
-    __syncthreads();
-    const int64_t ii = i0 + tx;
-    const bool live = ii < inner;
-    for (int k = ty; k < n_fft; k += blockDim.y) {
-        double re = 0.0, im = 0.0;
-        int idx = 0;
-        for (int j = 0; j < nx; ++j) {
-            cplx w = s_root[idx];
-            w.im = -w.im;
-            const cplx x = s_in[j * LANES + tx];
-            re += x.re * w.re - x.im * w.im;
-            im += x.re * w.im + x.im * w.re;
-            idx += k;
-            if (idx >= n_fft) idx -= n_fft;
+// The FFT of the lines held in x ([N][lp]); y is scratch of the same size. Returns the buffer that
+// holds the result. Called by every thread of the CTA (it synchronises after each stage).
+__device__ cplx* fft_lines(cplx* x, cplx* y, const FftPlan& P, int sign, int lp, int lane, int ty, int nty) {
+    for (int st = 0; st < P.nst; ++st) {
+        const int R = P.radix[st];
+        const int s = P.stride[st];
+        const int m = P.m[st];
+        const cplx* tw = P.tw + P.tw_off[st];
+        const int nb = P.n / R;
+        switch (R) {
+            case 4: stage_radix<4>(x, y, s, m, tw, sign, lp, lane, ty, nty, nb); break;
+            case 2: stage_radix<2>(x, y, s, m, tw, sign, lp, lane, ty, nty, nb); break;
+            case 3: stage_radix<3>(x, y, s, m, tw, sign, lp, lane, ty, nty, nb); break;
+            default: stage_radix<5>(x, y, s, m, tw, sign, lp, lane, ty, nty, nb); break;
         }
-        const double kv = live ? kernel[static_cast<int64_t>(k) * inner + ii] : 0.0;
-        s_mid[k * LANES + tx] = {re * kv, im * kv};
+        __syncthreads();
+        cplx* t = x;
+        x = y;
+        y = t;
+    }
+    return x;
+}
+
+// Pass 1: z lines (contiguous, nz real values zero-padded to N) -> half spectrum kz < nk.
+template <int L>
+__global__ void __launch_bounds__(256) fft_z_forward_kernel(const double* __restrict__ rho, int64_t lines, int nz,
+                                                            cplx* __restrict__ out, int nk, const FftPlan P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int LP = L + 1;
+    cplx* b0 = reinterpret_cast<cplx*>(smem_raw);
+    cplx* b1 = b0 + P.n * LP;
+    const int tid = threadIdx.y * L + threadIdx.x;
+    const int nthreads = L * blockDim.y;
+    const int64_t l0 = int64_t(blockIdx.x) * L;
+    for (int idx = tid; idx < L * P.n; idx += nthreads) {
+        const int line = idx / P.n;
+        const int z = idx - line * P.n;
+        const double v = (z < nz && l0 + line < lines) ? rho[(l0 + line) * nz + z] : 0.0;
+        b0[z * LP + line] = {v, 0.0};
     }
     __syncthreads();
+    const cplx* r = fft_lines(b0, b1, P, -1, LP, threadIdx.x, threadIdx.y, blockDim.y);
+    for (int idx = tid; idx < L * nk; idx += nthreads) {
+        const int line = idx / nk;
+        const int k = idx - line * nk;
+        if (l0 + line < lines) out[(l0 + line) * nk + k] = r[k * LP + line];
+    }
+}
+
+// Passes 2 and 4: middle-axis lines of data viewed as [outer][n][inner], inner contiguous; reads
+// n_in elements per line (zero beyond), transforms with length P.n, writes n_out elements.
+template <int L>
+__global__ void __launch_bounds__(256) fft_middle_kernel(const cplx* __restrict__ in, int64_t in_outer_stride, int n_in,
+                                                         cplx* __restrict__ out, int64_t out_outer_stride, int n_out,
+                                                         int64_t inner, const FftPlan P, int sign) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int LP = L + 1;
+    cplx* b0 = reinterpret_cast<cplx*>(smem_raw);
+    cplx* b1 = b0 + P.n * LP;
+    const int64_t o = blockIdx.x;
+    const int64_t c = int64_t(blockIdx.y) * L + threadIdx.x;
+    const bool live = c < inner;
+    const cplx* src = in + o * in_outer_stride + c;
+    for (int j = threadIdx.y; j < P.n; j += blockDim.y)
+        b0[j * LP + threadIdx.x] = (j < n_in && live) ? src[int64_t(j) * inner] : cplx{0.0, 0.0};
+    __syncthreads();
+    const cplx* r = fft_lines(b0, b1, P, sign, LP, threadIdx.x, threadIdx.y, blockDim.y);
     if (!live) return;
-    for (int x = ty; x < nx; x += blockDim.y) {
-        double re = 0.0, im = 0.0;
-        int idx = 0;
-        for (int k = 0; k < n_fft; ++k) {
-            const cplx w = s_root[idx];
-            const cplx v = s_mid[k * LANES + tx];
-            re += v.re * w.re - v.im * w.im;
-            im += v.re * w.im + v.im * w.re;
-            idx += x;
-            if (idx >= n_fft) idx -= n_fft;
-        }
-        col[static_cast<int64_t>(x) * inner + ii] = {re, im};
-    }
+    cplx* dst = out + o * out_outer_stride + c;
+    for (int j = threadIdx.y; j < n_out; j += blockDim.y) dst[int64_t(j) * inner] = r[j * LP + threadIdx.x];
 }
 
-// Pass 1: z lines (contiguous, length nz, zero-padded to N) -> half spectrum kz <= N/2.
-// One CTA per LANES consecutive (x, y) lines; lines staged transposed [z][line].
-__global__ void dft_z_r2c_kernel(const double* __restrict__ rho, int64_t lines, int nz, cplx* __restrict__ out, int nk,
-                                 const cplx* __restrict__ roots, int n_fft) {
+// Pass 3: x lines of one system ([nx][inner], inner = N1 * nk contiguous): forward FFT of the nx
+// non-zero values, times K[kx][ky][kz], inverse FFT, the first nx values written back in place.
+template <int L>
+__global__ void __launch_bounds__(256) fft_x_fused_kernel(cplx* __restrict__ data, int nx, int64_t inner,
+                                                          const double* __restrict__ kernel, const FftPlan P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* s_line = reinterpret_cast<double*>(smem_raw);  // [nz][LANES]
-    cplx* s_root = reinterpret_cast<cplx*>(s_line + static_cast<int64_t>(nz) * LANES);
-    const int64_t l0 = static_cast<int64_t>(blockIdx.x) * LANES;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * LANES + tx;
-    const int nthreads = LANES * blockDim.y;
-    for (int r = tid; r < n_fft; r += nthreads) s_root[r] = roots[r];
-    for (int idx = tid; idx < nz * LANES; idx += nthreads) {
-        const int l = idx / nz;
-        const int z = idx - l * nz;
-        const int64_t line = l0 + l;
-        s_line[z * LANES + l] = (line < lines) ? rho[line * nz + z] : 0.0;
+    constexpr int LP = L + 1;
+    cplx* b0 = reinterpret_cast<cplx*>(smem_raw);
+    cplx* b1 = b0 + P.n * LP;
+    const int64_t c = int64_t(blockIdx.x) * L + threadIdx.x;
+    const bool live = c < inner;
+    cplx* col = data + int64_t(blockIdx.y) * nx * inner + c;
+    for (int j = threadIdx.y; j < P.n; j += blockDim.y)
+        b0[j * LP + threadIdx.x] = (j < nx && live) ? col[int64_t(j) * inner] : cplx{0.0, 0.0};
+    __syncthreads();
+    cplx* r = fft_lines(b0, b1, P, -1, LP, threadIdx.x, threadIdx.y, blockDim.y);
+    for (int j = threadIdx.y; j < P.n; j += blockDim.y) {
+        const double kv = live ? kernel[int64_t(j) * inner + c] : 0.0;
+        r[j * LP + threadIdx.x] = scale(r[j * LP + threadIdx.x], kv);
     }
     __syncthreads();
-    const int64_t line = l0 + tx;
-    if (line >= lines) return;
-    for (int k = ty; k < nk; k += blockDim.y) {
-        double re = 0.0, im = 0.0;
-        int idx = 0;
-        for (int z = 0; z < nz; ++z) {
-            const cplx w = s_root[idx];
-            const double x = s_line[z * LANES + tx];
-            re += x * w.re;
-            im -= x * w.im;
-            idx += k;
-            if (idx >= n_fft) idx -= n_fft;
-        }
-        out[line * nk + k] = {re, im};
-    }
+    const cplx* v = fft_lines(r, r == b0 ? b1 : b0, P, +1, LP, threadIdx.x, threadIdx.y, blockDim.y);
+    if (!live) return;
+    for (int j = threadIdx.y; j < nx; j += blockDim.y) col[int64_t(j) * inner] = v[j * LP + threadIdx.x];
 }
 
-// Pass 5: half spectrum -> real z lines, z < nz, with the 1/(Nx Ny Nz) normalisation of irfftn.
-// out[z] = A0.re + (-1)^z A_{N/2}.re + 2 sum_{0<k<N/2} Re(A_k w^{kz}) for even N.
-__global__ void dft_z_c2r_kernel(const cplx* __restrict__ in, int64_t lines, int nk, double* __restrict__ v, int nz,
-                                 const cplx* __restrict__ roots, int n_fft, double scale) {
+// Pass 5: half spectrum -> real z lines (z < nz), with the 1/(Nx Ny Nz) of irfftn. The full
+// spectrum is the Hermitian extension X[N-k] = conj(X[k]); the real part of its inverse is irfft
+// (the imaginary parts of the k = 0 and Nyquist terms drop out, as in irfft).
+template <int L>
+__global__ void __launch_bounds__(256) fft_z_inverse_kernel(const cplx* __restrict__ in, int64_t lines, int nk,
+                                                            double* __restrict__ v, int nz, const FftPlan P,
+                                                            double norm) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx* s_line = reinterpret_cast<cplx*>(smem_raw);  // [nk][LANES]
-    cplx* s_root = s_line + static_cast<int64_t>(nk) * LANES;
-    const int64_t l0 = static_cast<int64_t>(blockIdx.x) * LANES;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * LANES + tx;
-    const int nthreads = LANES * blockDim.y;
-    for (int r = tid; r < n_fft; r += nthreads) s_root[r] = roots[r];
-    for (int idx = tid; idx < nk * LANES; idx += nthreads) {
-        const int l = idx / nk;
-        const int k = idx - l * nk;
-        const int64_t line = l0 + l;
-        s_line[k * LANES + l] = (line < lines) ? in[line * nk + k] : cplx{0.0, 0.0};
+    constexpr int LP = L + 1;
+    cplx* b0 = reinterpret_cast<cplx*>(smem_raw);
+    cplx* b1 = b0 + P.n * LP;
+    const int tid = threadIdx.y * L + threadIdx.x;
+    const int nthreads = L * blockDim.y;
+    const int64_t l0 = int64_t(blockIdx.x) * L;
+    const int N = P.n;
+    for (int idx = tid; idx < L * nk; idx += nthreads) {
+        const int line = idx / nk;
+        const int k = idx - line * nk;
+        const cplx a = (l0 + line < lines) ? in[(l0 + line) * nk + k] : cplx{0.0, 0.0};
+        b0[k * LP + line] = a;
+        if (k > 0 && N - k >= nk) b0[(N - k) * LP + line] = {a.re, -a.im};
     }
     __syncthreads();
-    const int64_t line = l0 + tx;
-    if (line >= lines) return;
-    const bool even = (n_fft % 2) == 0;
-    const int k_last = even ? n_fft / 2 : -1;  // the Nyquist term (real part only)
-    for (int z = ty; z < nz; z += blockDim.y) {
-        double acc = s_line[tx].re;  // k = 0, real part only
-        int idx = z;                 // (k * z) mod n_fft for k = 1
-        if (idx >= n_fft) idx -= n_fft;
-        double sum = 0.0;
-        for (int k = 1; k < nk; ++k) {
-            const cplx a = s_line[k * LANES + tx];
-            const cplx w = s_root[idx];
-            if (k == k_last)
-                acc += a.re * w.re;  // (-1)^z, imaginary part ignored
-            else
-                sum += a.re * w.re - a.im * w.im;
-            idx += z;
-            if (idx >= n_fft) idx -= n_fft;
-        }
-        v[line * nz + z] = (acc + 2.0 * sum) * scale;
+    const cplx* r = fft_lines(b0, b1, P, +1, LP, threadIdx.x, threadIdx.y, blockDim.y);
+    for (int idx = tid; idx < L * nz; idx += nthreads) {
+        const int line = idx / nz;
+        const int z = idx - line * nz;
+        if (l0 + line < lines) v[(l0 + line) * nz + z] = r[z * LP + line].re * norm;
     }
 }
 
@@ -236,15 +277,32 @@ __global__ void kernel_table_kernel(double* __restrict__ out, int n0, int n1, in
 }
 
 constexpr int kPoissonSmem = 200 * 1024;
+constexpr int kThreads = 256;
+
+// Lines per CTA for transforms of length n: 16 while two [n][17] complex buffers fit, else 8.
+int lines_for(int n) { return size_t(2) * n * 17 * sizeof(cplx) <= size_t(kPoissonSmem) ? 16 : 8; }
+
+size_t smem_for(int n, int L) { return size_t(2) * n * (L + 1) * sizeof(cplx); }
+
+template <int L>
+int configure_lines() {
+    int st = check(cudaFuncSetAttribute(fft_z_forward_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kPoissonSmem));
+    if (st == CDFTB_OK)
+        st = check(cudaFuncSetAttribute(fft_middle_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kPoissonSmem));
+    if (st == CDFTB_OK)
+        st = check(cudaFuncSetAttribute(fft_x_fused_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kPoissonSmem));
+    if (st == CDFTB_OK)
+        st = check(cudaFuncSetAttribute(fft_z_inverse_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kPoissonSmem));
+    return st;
+}
 
 int configure_poisson_kernels() {
-    int st = check(cudaFuncSetAttribute(dft_x_kernel_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, kPoissonSmem));
-    if (st == CDFTB_OK)
-        st = check(cudaFuncSetAttribute(dft_middle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPoissonSmem));
-    if (st == CDFTB_OK)
-        st = check(cudaFuncSetAttribute(dft_z_r2c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPoissonSmem));
-    if (st == CDFTB_OK)
-        st = check(cudaFuncSetAttribute(dft_z_c2r_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPoissonSmem));
+    int st = configure_lines<16>();
+    if (st == CDFTB_OK) st = configure_lines<8>();
     return st;
 }
 
@@ -257,13 +315,67 @@ int fft_friendly(int n) {
     }
 }
 
+// Stage list and twiddle table (host, double) of a length-n transform; false if n is not 2,3,5-smooth
+// or has too many stages.
+bool make_fft_plan(int n, FftPlan* plan, cplx** device_tw) {
+    FftPlan P{};
+    P.n = n;
+    int rem = n;
+    int radices[MAX_STAGES];
+    int count = 0;
+    for (int r : {4, 2, 3, 5}) {
+        while (rem % r == 0 && count < MAX_STAGES) {
+            radices[count++] = r;
+            rem /= r;
+        }
+    }
+    if (rem != 1) return false;
+    P.nst = count;
+    int total = 0;
+    int stride = 1;
+    for (int st = 0; st < count; ++st) {
+        const int r = radices[st];
+        const int len = n / stride;
+        P.radix[st] = r;
+        P.stride[st] = stride;
+        P.m[st] = len / r;
+        P.tw_off[st] = total;
+        total += P.m[st] * (r - 1);
+        stride *= r;
+    }
+    cplx* host = new cplx[total > 0 ? total : 1];
+    for (int st = 0; st < count; ++st) {
+        const int r = P.radix[st];
+        const int len = n / P.stride[st];
+        for (int p = 0; p < P.m[st]; ++p)
+            for (int k = 1; k < r; ++k) {
+                // exp(-2 pi i p k / len), the angle reduced exactly in integers first
+                const long long num = static_cast<long long>(p) * k % len;
+                const double t = -2.0 * 3.14159265358979323846 * static_cast<double>(num) / static_cast<double>(len);
+                host[P.tw_off[st] + p * (r - 1) + k - 1] = {cos(t), sin(t)};
+            }
+    }
+    cplx* dev = nullptr;
+    bool ok = cudaMalloc(&dev, sizeof(cplx) * (total > 0 ? total : 1)) == cudaSuccess &&
+              cudaMemcpy(dev, host, sizeof(cplx) * (total > 0 ? total : 1), cudaMemcpyHostToDevice) == cudaSuccess;
+    delete[] host;
+    if (!ok) {
+        cudaFree(dev);
+        return false;
+    }
+    P.tw = dev;
+    *plan = P;
+    *device_tw = dev;
+    return true;
+}
+
 }  // namespace
 
 }  // namespace cdftb
 
 using namespace cdftb;
 
-// A plan: padded shape, the kernel table, roots of unity per axis, and the two transform buffers.
+// A plan: padded shape, the kernel table, the FFT plan of each axis, and the two transform buffers.
 struct cdftb_poisson_plan {
     int n[3];
     int pad[3];
@@ -271,11 +383,20 @@ struct cdftb_poisson_plan {
     double spacing;
     double radius;
     double* kernel;  // [pad0][pad1][nk]
-    cplx* roots[3];  // N-th roots of unity per axis
-    cplx* a;         // [batch][n0][n1][nk]
-    cplx* b;         // [batch][n0][pad1][nk]
+    FftPlan fft[3];
+    cplx* tw[3];
+    cplx* a;  // [batch][n0][n1][nk]
+    cplx* b;  // [batch][n0][pad1][nk]
     int max_batch;
 };
+
+static void free_plan(cdftb_poisson_plan* p) {
+    cudaFree(p->kernel);
+    for (int d = 0; d < 3; ++d) cudaFree(p->tw[d]);
+    cudaFree(p->a);
+    cudaFree(p->b);
+    delete p;
+}
 
 extern "C" int cdftb_poisson_plan_create(int nx, int ny, int nz, double spacing, double pad_factor, int max_batch,
                                          void** plan_out, int* padded_shape_out, double* cutoff_radius_out) {
@@ -292,6 +413,11 @@ extern "C" int cdftb_poisson_plan_create(int nx, int ny, int nz, double spacing,
     for (int d = 0; d < 3; ++d) r = fmin(r, p->pad[d] * spacing);
     p->radius = 0.5 * r;
     p->max_batch = max_batch;
+    for (int d = 0; d < 3; ++d)
+        if (smem_for(p->pad[d], lines_for(p->pad[d])) > size_t(kPoissonSmem)) {
+            delete p;
+            return CDFTB_ERR_CAPACITY;
+        }
     const int64_t nkern = static_cast<int64_t>(p->pad[0]) * p->pad[1] * p->nk;
     int st = configure_poisson_kernels();
     if (st != CDFTB_OK) {
@@ -299,18 +425,8 @@ extern "C" int cdftb_poisson_plan_create(int nx, int ny, int nz, double spacing,
         return st;
     }
     st = check(cudaMalloc(&p->kernel, nkern * sizeof(double)));
-    for (int d = 0; d < 3 && st == CDFTB_OK; ++d) {
-        const int N = p->pad[d];
-        cplx* host = new cplx[N];
-        for (int j = 0; j < N; ++j) {
-            // exp(+2 pi i j / N); the sign is applied per pass
-            const double t = 2.0 * 3.14159265358979323846 * static_cast<double>(j) / static_cast<double>(N);
-            host[j] = {cos(t), sin(t)};
-        }
-        st = check(cudaMalloc(&p->roots[d], N * sizeof(cplx)));
-        if (st == CDFTB_OK) st = check(cudaMemcpy(p->roots[d], host, N * sizeof(cplx), cudaMemcpyHostToDevice));
-        delete[] host;
-    }
+    for (int d = 0; d < 3 && st == CDFTB_OK; ++d)
+        if (!make_fft_plan(p->pad[d], &p->fft[d], &p->tw[d])) st = CDFTB_ERR_LAUNCH;
     if (st == CDFTB_OK)
         st = check(cudaMalloc(&p->a, static_cast<int64_t>(max_batch) * nx * ny * p->nk * sizeof(cplx)));
     if (st == CDFTB_OK)
@@ -322,11 +438,7 @@ extern "C" int cdftb_poisson_plan_create(int nx, int ny, int nz, double spacing,
         if (st == CDFTB_OK) st = check(cudaDeviceSynchronize());
     }
     if (st != CDFTB_OK) {
-        cudaFree(p->kernel);
-        for (int d = 0; d < 3; ++d) cudaFree(p->roots[d]);
-        cudaFree(p->a);
-        cudaFree(p->b);
-        delete p;
+        free_plan(p);
         return st;
     }
     if (padded_shape_out)
@@ -339,11 +451,7 @@ extern "C" int cdftb_poisson_plan_create(int nx, int ny, int nz, double spacing,
 extern "C" int cdftb_poisson_plan_destroy(void* plan) {
     auto* p = static_cast<cdftb_poisson_plan*>(plan);
     if (!p) return CDFTB_OK;
-    cudaFree(p->kernel);
-    for (int d = 0; d < 3; ++d) cudaFree(p->roots[d]);
-    cudaFree(p->a);
-    cudaFree(p->b);
-    delete p;
+    free_plan(p);
     return CDFTB_OK;
 }
 
@@ -354,58 +462,60 @@ extern "C" int cdftb_poisson_kernel_table(void* plan, const double** table_out) 
     return CDFTB_OK;
 }
 
+namespace {
+
+template <int L>
+int run_passes(cdftb_poisson_plan* p, const double* density, double* potential, int batch, cudaStream_t s, int which) {
+    const int nx = p->n[0], ny = p->n[1], nz = p->n[2];
+    const int N0 = p->pad[0], N1 = p->pad[1], N2 = p->pad[2], nk = p->nk;
+    const int64_t lines = static_cast<int64_t>(batch) * nx * ny;
+    const dim3 blk(L, kThreads / L);
+    switch (which) {
+        case 1:
+            fft_z_forward_kernel<L><<<static_cast<unsigned>(ceil_div(lines, L)), blk, smem_for(N2, L), s>>>(
+                density, lines, nz, p->a, nk, p->fft[2]);
+            break;
+        case 2: {
+            dim3 grid(static_cast<unsigned>(batch * nx), static_cast<unsigned>(ceil_div(nk, L)));
+            fft_middle_kernel<L><<<grid, blk, smem_for(N1, L), s>>>(p->a, static_cast<int64_t>(ny) * nk, ny, p->b,
+                                                                   static_cast<int64_t>(N1) * nk, N1, nk, p->fft[1], -1);
+            break;
+        }
+        case 3: {
+            const int64_t inner = static_cast<int64_t>(N1) * nk;
+            dim3 grid(static_cast<unsigned>(ceil_div(inner, L)), static_cast<unsigned>(batch));
+            fft_x_fused_kernel<L><<<grid, blk, smem_for(N0, L), s>>>(p->b, nx, inner, p->kernel, p->fft[0]);
+            break;
+        }
+        case 4: {
+            dim3 grid(static_cast<unsigned>(batch * nx), static_cast<unsigned>(ceil_div(nk, L)));
+            fft_middle_kernel<L><<<grid, blk, smem_for(N1, L), s>>>(p->b, static_cast<int64_t>(N1) * nk, N1, p->a,
+                                                                   static_cast<int64_t>(ny) * nk, ny, nk, p->fft[1], +1);
+            break;
+        }
+        default: {
+            const double norm = 1.0 / (static_cast<double>(N0) * N1 * N2);
+            fft_z_inverse_kernel<L><<<static_cast<unsigned>(ceil_div(lines, L)), blk, smem_for(N2, L), s>>>(
+                p->a, lines, nk, potential, nz, p->fft[2], norm);
+            break;
+        }
+    }
+    return check_launch();
+}
+
+}  // namespace
+
 extern "C" int cdftb_poisson_solve(void* plan, const double* density, double* potential, int batch,
                                    cdftb_stream_t stream) {
     auto* p = static_cast<cdftb_poisson_plan*>(plan);
     if (!p || !density || !potential || batch < 1 || batch > p->max_batch) return CDFTB_ERR_ARGUMENT;
+    if (static_cast<int64_t>(batch) * p->n[0] > 0x7fffffff) return CDFTB_ERR_CAPACITY;
     cudaStream_t s = as_stream(stream);
-    const int nx = p->n[0], ny = p->n[1], nz = p->n[2];
-    const int N0 = p->pad[0], N1 = p->pad[1], N2 = p->pad[2], nk = p->nk;
-    const int64_t lines = static_cast<int64_t>(batch) * nx * ny;
-    const dim3 blk(LANES, 8);
-    // pass 1
-    {
-        const size_t sm = static_cast<size_t>(nz) * LANES * sizeof(double) + N2 * sizeof(cplx);
-        dft_z_r2c_kernel<<<static_cast<unsigned>(ceil_div(lines, LANES)), blk, sm, s>>>(density, lines, nz, p->a, nk,
-                                                                                        p->roots[2], N2);
-        int st = check_launch();
-        if (st != CDFTB_OK) return st;
-    }
-    // pass 2: [b*nx][ny][nk] -> [b*nx][N1][nk]
-    {
-        const size_t sm = static_cast<size_t>(ny) * LANES * sizeof(cplx) + N1 * sizeof(cplx);
-        dim3 grid(static_cast<unsigned>(ceil_div(nk, LANES)), static_cast<unsigned>(batch * nx));
-        dft_middle_kernel<<<grid, blk, sm, s>>>(p->a, static_cast<int64_t>(ny) * nk, ny, p->b,
-                                                static_cast<int64_t>(N1) * nk, N1, nk, p->roots[1], N1, -1);
-        int st = check_launch();
-        if (st != CDFTB_OK) return st;
-    }
-    // pass 3: per batch, [nx][N1*nk] columns
-    {
-        const size_t sm = (static_cast<size_t>(nx) * LANES + static_cast<size_t>(N0) * LANES + N0) * sizeof(cplx);
-        if (sm > kPoissonSmem) return CDFTB_ERR_CAPACITY;
-        const int64_t inner = static_cast<int64_t>(N1) * nk;
-        dim3 grid(static_cast<unsigned>(ceil_div(inner, LANES)), static_cast<unsigned>(batch));
-        dft_x_kernel_fused<<<grid, blk, sm, s>>>(p->b, nx, inner, p->kernel, p->roots[0], N0);
-        int st = check_launch();
-        if (st != CDFTB_OK) return st;
-    }
-    // pass 4: [b*nx][N1][nk] -> [b*nx][ny][nk]
-    {
-        const size_t sm = static_cast<size_t>(N1) * LANES * sizeof(cplx) + N1 * sizeof(cplx);
-        dim3 grid(static_cast<unsigned>(ceil_div(nk, LANES)), static_cast<unsigned>(batch * nx));
-        dft_middle_kernel<<<grid, blk, sm, s>>>(p->b, static_cast<int64_t>(N1) * nk, N1, p->a,
-                                                static_cast<int64_t>(ny) * nk, ny, nk, p->roots[1], N1, +1);
-        int st = check_launch();
-        if (st != CDFTB_OK) return st;
-    }
-    // pass 5
-    {
-        const size_t sm = static_cast<size_t>(nk) * LANES * sizeof(cplx) + N2 * sizeof(cplx);
-        const double scale = 1.0 / (static_cast<double>(N0) * N1 * N2);
-        dft_z_c2r_kernel<<<static_cast<unsigned>(ceil_div(lines, LANES)), blk, sm, s>>>(p->a, lines, nk, potential, nz,
-                                                                                        p->roots[2], N2, scale);
-        int st = check_launch();
+    const int axis_of_pass[6] = {0, 2, 1, 0, 1, 2};
+    for (int pass = 1; pass <= 5; ++pass) {
+        const int n = p->pad[axis_of_pass[pass]];
+        const int st = lines_for(n) == 16 ? run_passes<16>(p, density, potential, batch, s, pass)
+                                          : run_passes<8>(p, density, potential, batch, s, pass);
         if (st != CDFTB_OK) return st;
     }
     return CDFTB_OK;

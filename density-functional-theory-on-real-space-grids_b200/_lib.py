@@ -42,7 +42,9 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_launch_count": (ctypes.c_ulonglong, []),
     "cdftb_weighted_divergence_f64": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p, c_void_p,
                                               c_void_p, c_double, c_int, c_void_p]),
-    "cdftb_cusp_apply": (c_int, [ctypes.POINTER(Operator), c_void_p, c_int, c_void_p, c_int, c_int64, c_int, c_void_p]),
+    "cdftb_cusp_apply_work_bytes": (c_int64, [ctypes.POINTER(Operator), c_int64]),
+    "cdftb_cusp_apply": (c_int, [ctypes.POINTER(Operator), c_void_p, c_int, c_void_p, c_int, c_int64, c_int, c_void_p,
+                                 c_int64, c_void_p]),
     "cdftb_chebyshev_filter_work_bytes": (c_int64, [ctypes.POINTER(Operator), c_int64]),
     "cdftb_chebyshev_filter": (c_int, [ctypes.POINTER(Operator), c_void_p, c_int, c_void_p, c_int, c_void_p, c_int64,
                                        c_int64, c_void_p, c_int, c_void_p]),
@@ -79,8 +81,20 @@ SIGNATURES: dict[str, tuple] = {
                                       c_void_p]),
     "cdftb_quadrature_interpolate_f64": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p, c_int,
                                                  c_int64, c_void_p, c_int64, c_void_p]),
-    "cdftb_quadrature_lift_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_int,
-                                          c_int64, c_void_p, c_int64, c_void_p]),
+    "cdftb_lift_plan_values_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p,
+                                           c_void_p]),
+    "cdftb_quadrature_lift_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                          c_void_p, c_int, c_int64, c_void_p, c_int64, c_void_p]),
+    "cdftb_quadrature_many_scratch_bytes": (c_int64, [c_int64, c_int64]),
+    "cdftb_quadrature_interpolate_many_f64": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p, c_int,
+                                                      c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p]),
+    "cdftb_lift_segments_capacity": (c_int64, [c_int64, c_int64]),
+    "cdftb_lift_segments_scratch_bytes": (c_int64, [c_int64]),
+    "cdftb_lift_plan_segments": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int64, c_void_p, c_int64,
+                                         c_void_p]),
+    "cdftb_quadrature_lift_many_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int,
+                                               c_int, c_int64, c_void_p, c_int, c_int64, c_void_p, c_int64, c_void_p,
+                                               c_int64, c_void_p]),
     "cdftb_cusp_coefficients_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "cdftb_hartree_split_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int64, c_int, c_void_p,
                                         c_void_p, c_void_p]),

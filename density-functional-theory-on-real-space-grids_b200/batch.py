@@ -28,7 +28,7 @@ from . import _lib
 from ._lib import F32, F64, call, ptr, stream_handle
 from .eigen import BOUND_REUSE_RITZ_FRACTION, EigenConfig, chebyshev_coefficients, filter_workspace
 from .geometry import CuspGeometry, gradient, row_sums
-from .operators import cast, measure_cross, rowwise_inner
+from .operators import apply_workspace, cast, measure_cross, rowwise_inner
 from .poisson import CoulombCutoffPoisson
 from .rng import SeededStream
 from .scf import (FILTER_STEPS_PER_ITERATION, BoundReusePolicy, LinearMixer, MixingConfig, PulayMixer, SCFConfig,
@@ -86,8 +86,9 @@ class BatchedHamiltonian:
         k = x.shape[1]
         out = torch.empty_like(x)
         op = self._op(k)
+        work = apply_workspace(op, x.shape[0] * k, x.device)
         call("cdftb_cusp_apply", ctypes.byref(op), ptr(x), _lib.dtype_code(x), ptr(out), _lib.dtype_code(out),
-             x.shape[0] * k, 1 if kinetic_only else 0, stream_handle(x.device))
+             x.shape[0] * k, 1 if kinetic_only else 0, ptr(work), work.numel(), stream_handle(x.device))
         if not kinetic_only:
             self.applications += 1
         return out
@@ -430,9 +431,7 @@ class BatchedKohnShamStep:
         call("cdftb_hartree_split_f64", ptr(n_grid), ptr(self.f2), ptr(g.step.cusp_grid), ptr(coef), na, n, b,
              ptr(rho), ptr(n_smooth), stream)
         self.poisson.solve_batch(n_smooth, out=fields[1])
-        node = torch.empty((2, b, m), **f)
-        call("cdftb_quadrature_interpolate_f64", ptr(q.base), ptr(q.w1d), m, *grid.shape, ptr(fields), 2 * b, n,
-             ptr(node), m, stream)
+        node = q._interp_raw(fields.reshape(2 * b, n), 2 * b).reshape(2, b, m)
         lift_in = torch.empty((b, 2, m), **f)
         e_w = torch.empty((b, m), **f)
         call("cdftb_potentials_node_lda_f64", ptr(node), m, ptr(q.weights), ptr(q.f2), ptr(g.step.v1s_node),

@@ -71,6 +71,8 @@ StaggeredTaps staggered_taps(int accuracy);
 int generic_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
                              void* work, int64_t batch, const double* coefficients, int degree, cdftb_stream_t stream);
 int64_t slab_filter_work_bytes(const cdftb_operator* op, int64_t batch);
+int generic_cusp_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* out, int out_dtype,
+                       int64_t batch, int kinetic_only, cdftb_stream_t stream);
 bool slab_filter_applies(const cdftb_operator* op);
 int slab_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
                           void* work, int64_t batch, const double* coefficients, int degree, cudaStream_t stream);

@@ -186,6 +186,53 @@ __global__ void lanczos_kernel(int mode, double* __restrict__ w, const double* _
     }
 }
 
+// The same two kernels for a block width known at compile time (the common m <= 8): the orbital
+// values of a point stay in registers instead of a runtime-indexed array.
+template <int M>
+__global__ void trsm_lower_fixed_kernel(const double* __restrict__ lower, const double* __restrict__ in,
+                                        int64_t in_stride, void* out, int out_dtype, int64_t out_stride, int64_t n) {
+    __shared__ double l[M * M];
+    const int g = blockIdx.y;
+    for (int i = threadIdx.x; i < M * M; i += blockDim.x) l[i] = lower[static_cast<int64_t>(g) * M * M + i];
+    __syncthreads();
+    const double* src = in + g * in_stride;
+    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double x[M];
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            double v = src[i * n + p];
+#pragma unroll
+            for (int k = 0; k < i; ++k) v -= l[i * M + k] * x[k];
+            x[i] = v / l[i * M + i];
+            store_as<double>(out, out_dtype, g * out_stride + i * n + p, x[i]);
+        }
+    }
+}
+
+template <int M>
+__global__ void rotate_fixed_kernel(const double* __restrict__ r, const double* __restrict__ in, int64_t in_stride,
+                                    void* out, int out_dtype, int64_t out_stride, int64_t n) {
+    __shared__ double rs[M * M];
+    const int g = blockIdx.y;
+    for (int i = threadIdx.x; i < M * M; i += blockDim.x) rs[i] = r[static_cast<int64_t>(g) * M * M + i];
+    __syncthreads();
+    const double* src = in + g * in_stride;
+    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double x[M];
+#pragma unroll
+        for (int j = 0; j < M; ++j) x[j] = src[j * n + p];
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            double v = 0.0;
+#pragma unroll
+            for (int j = 0; j < M; ++j) v = fma(rs[i * M + j], x[j], v);
+            store_as<double>(out, out_dtype, g * out_stride + i * n + p, v);
+        }
+    }
+}
+
 inline unsigned point_blocks(int64_t n) {
     const int64_t b = ceil_div(n, 256);
     return static_cast<unsigned>(b < 148 * 8 ? b : 148 * 8);
@@ -209,8 +256,18 @@ extern "C" int cdftb_block_trsm_lower_f64(const double* lower, const double* in,
                                           cdftb_stream_t stream) {
     if (!lower || !in || !out || m <= 0 || m > MMAX || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
     dim3 grid(point_blocks(n), groups);
-    trsm_lower_kernel<<<grid, 256, 0, as_stream(stream)>>>(lower, in, in_group_stride, out, out_dtype, out_group_stride, m, n,
-                                                           groups);
+    cudaStream_t s = as_stream(stream);
+    switch (m) {
+#define CDFTB_TRSM(M)                                                                                             \
+    case M:                                                                                                       \
+        trsm_lower_fixed_kernel<M><<<grid, 256, 0, s>>>(lower, in, in_group_stride, out, out_dtype, out_group_stride, \
+                                                        n);                                                       \
+        return check_launch();
+        CDFTB_TRSM(1) CDFTB_TRSM(2) CDFTB_TRSM(3) CDFTB_TRSM(4) CDFTB_TRSM(5) CDFTB_TRSM(6) CDFTB_TRSM(7) CDFTB_TRSM(8)
+#undef CDFTB_TRSM
+        default: break;
+    }
+    trsm_lower_kernel<<<grid, 256, 0, s>>>(lower, in, in_group_stride, out, out_dtype, out_group_stride, m, n, groups);
     return check_launch();
 }
 
@@ -228,7 +285,19 @@ extern "C" int cdftb_block_rotate_f64(const double* r, const double* in, int64_t
         groups > 65535)
         return CDFTB_ERR_ARGUMENT;
     dim3 grid(point_blocks(n), groups);
-    rotate_kernel<<<grid, 256, 0, as_stream(stream)>>>(r, in, in_group_stride, out, out_dtype, out_group_stride, m_out, m_in, n);
+    cudaStream_t s = as_stream(stream);
+    if (m_out == m_in) {
+        switch (m_in) {
+#define CDFTB_ROT(M)                                                                                                 \
+    case M:                                                                                                          \
+        rotate_fixed_kernel<M><<<grid, 256, 0, s>>>(r, in, in_group_stride, out, out_dtype, out_group_stride, n); \
+        return check_launch();
+            CDFTB_ROT(1) CDFTB_ROT(2) CDFTB_ROT(3) CDFTB_ROT(4) CDFTB_ROT(5) CDFTB_ROT(6) CDFTB_ROT(7) CDFTB_ROT(8)
+#undef CDFTB_ROT
+            default: break;
+        }
+    }
+    rotate_kernel<<<grid, 256, 0, s>>>(r, in, in_group_stride, out, out_dtype, out_group_stride, m_out, m_in, n);
     return check_launch();
 }
 

@@ -152,6 +152,8 @@ struct FilterArgs {
     int orb_per_group;
     int shared_potential;  // one potential for every orbital
     unsigned token;        // this launch's abort token (never 0)
+    int apply_only;        // out = A phi (no recurrence; coef unused)
+    int kinetic_only;      // with apply_only: out = 0.5 (h^3/omega) div phi (no potential)
     const double* coef;
     int degree;
     int step;
@@ -427,8 +429,8 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
     const int64_t plane_n = int64_t(ny) * nz;
     const int own = ty * TZ + tz;  // index in the (TY, TZ) boxes
 
-    E cc, ca, cb;
-    {
+    E cc = Lane::zero(), ca = Lane::zero(), cb = Lane::zero();
+    if (!a.apply_only) {
         const int64_t c0 = o0 / a.orb_per_group;  // one coefficient table per orbital group
         const int64_t c1 = o1 / a.orb_per_group;
         const double* r0 = a.coef + (c0 * a.degree + a.step) * 3;
@@ -491,16 +493,25 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
                     const E phi = phq[(g + 1) & 7];
                     const S inv = reinterpret_cast<const S*>(slot + SH::O_INV)[own];
                     const E kin = Lane::mul(Lane::mul(div, Lane::splat(S(0.5))), Lane::splat(inv));
-                    E potv;
-                    if constexpr (Lane::ORBITALS == 2)
-                        potv = make_float2(reinterpret_cast<const S*>(slot + SH::O_POT0)[own],
-                                           reinterpret_cast<const S*>(slot + SH::O_POT1)[own]);
-                    else
-                        potv = reinterpret_cast<const S*>(slot + SH::O_POT0)[own];
-                    const E applied = Lane::fma(phi, potv, kin);
-                    res = Lane::mul(Lane::fma(Lane::neg(cc), phi, applied), ca);
-                    if (has_prev)
-                        res = Lane::fma(Lane::neg(cb), reinterpret_cast<const E*>(slot + SH::O_PREV)[own], res);
+                    if (a.kinetic_only) {
+                        res = kin;
+                    } else {
+                        E potv;
+                        if constexpr (Lane::ORBITALS == 2)
+                            potv = make_float2(reinterpret_cast<const S*>(slot + SH::O_POT0)[own],
+                                               reinterpret_cast<const S*>(slot + SH::O_POT1)[own]);
+                        else
+                            potv = reinterpret_cast<const S*>(slot + SH::O_POT0)[own];
+                        const E applied = Lane::fma(phi, potv, kin);
+                        if (a.apply_only) {
+                            res = applied;
+                        } else {
+                            res = Lane::mul(Lane::fma(Lane::neg(cc), phi, applied), ca);
+                            if (has_prev)
+                                res = Lane::fma(Lane::neg(cb), reinterpret_cast<const E*>(slot + SH::O_PREV)[own],
+                                                res);
+                        }
+                    }
                 } else {
                     res = Lane::zero();  // the padding column stays zero
                 }
@@ -711,88 +722,116 @@ int pad_rows(const void* src, int64_t rows, int cols, int cols_pad, S* dst, cuda
     return check_launch();
 }
 
+// Copies the geometry into the padded rows TMA reads (at geo, element type S) and encodes the maps
+// of the geometry; kinetic_only zeroes the potential rows instead of copying them.
 template <typename Lane>
-int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype, void* work,
-                int64_t batch, const double* coefficients, int degree, cudaStream_t stream) {
+int prepare_geometry(const cdftb_operator* op, int64_t batch, void* geo_base, int tz, bool kinetic_only,
+                     FilterMaps* maps, cudaStream_t stream) {
     using S = typename Lane::S;
     const int nx = op->nx, ny = op->ny, nz = op->nz;
-    const int nzp = padded_z(nz);
-    const int64_t lanes = lanes_of(op, batch);
-    const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
-    char* w = static_cast<char*>(work);
-    void* buf[3] = {w, w + lanes * lane_bytes, w + 2 * lanes * lane_bytes};
     const GeoPack gp = geo_pack(op, batch);
-    S* geo = reinterpret_cast<S*>(w + 3 * lanes * lane_bytes);
-    S* w0p = geo;
+    S* w0p = static_cast<S*>(geo_base);
     S* w1p = w0p + gp.n_w0;
     S* w2p = w1p + gp.n_w1;
     S* invp = w2p + gp.n_w2;
     S* potp = invp + gp.n_inv;
     const int64_t nsys = systems_of(op, batch);
     int st;
-    {
-        const int64_t total = lanes * int64_t(nx) * ny * nzp;
-        const unsigned blocks = static_cast<unsigned>(std::min<int64_t>(ceil_div(total, 256), 148 * 16));
-        pack_lanes_kernel<Lane><<<blocks, 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
-                                                            static_cast<typename Lane::E*>(buf[2]));
-        if ((st = check_launch()) != CDFTB_OK) return st;
-    }
     if ((st = pad_rows<S>(op->face_weights[0], int64_t(nx + 8) * ny, nz, gp.nzg, w0p, stream)) != CDFTB_OK) return st;
     if ((st = pad_rows<S>(op->face_weights[1], int64_t(nx) * (ny + 8), nz, gp.nzg, w1p, stream)) != CDFTB_OK) return st;
     if ((st = pad_rows<S>(op->face_weights[2], int64_t(nx) * ny, nz + 8, gp.nz8g, w2p, stream)) != CDFTB_OK) return st;
     if ((st = pad_rows<S>(op->inverse_weight, int64_t(nx) * ny, nz, gp.nzg, invp, stream)) != CDFTB_OK) return st;
-    for (int64_t g = 0; g < nsys; ++g) {
-        const void* src = static_cast<const S*>(op->potential) + g * op->potential_stride;
-        if ((st = pad_rows<S>(src, int64_t(nx) * ny, nz, gp.nzg, potp + g * int64_t(nx) * ny * gp.nzg, stream)) !=
-            CDFTB_OK)
-            return st;
+    if (kinetic_only || !op->potential) {
+        if ((st = check(cudaMemsetAsync(potp, 0, gp.n_pot * sizeof(S), stream))) != CDFTB_OK) return st;
+    } else if (op->potential_stride == 0 || op->potential_stride == int64_t(nx) * ny * nz) {
+        // every system's row block at once (rows of consecutive systems are consecutive)
+        if ((st = pad_rows<S>(op->potential, nsys * nx * ny, nz, gp.nzg, potp, stream)) != CDFTB_OK) return st;
+    } else {
+        for (int64_t g = 0; g < nsys; ++g) {
+            const void* src = static_cast<const S*>(op->potential) + g * op->potential_stride;
+            if ((st = pad_rows<S>(src, int64_t(nx) * ny, nz, gp.nzg, potp + g * int64_t(nx) * ny * gp.nzg, stream)) !=
+                CDFTB_OK)
+                return st;
+        }
     }
-
-    const int tz = choose_tz(nzp);
     const CUtensorMapDataType gt = Lane::GEO_TYPE;
     const int sb = sizeof(S);
-    FilterMaps maps[3];
-    for (int b = 0; b < 3; ++b) {
-        const int64_t lane_dims[4] = {nzp, ny, nx, lanes};
-        const unsigned phi_box[4] = {unsigned(tz + 18), unsigned(NROW), 1, 1};
-        const unsigned prev_box[4] = {unsigned(tz), unsigned(TY), 1, 1};
-        if ((st = encode_map(&maps[b].phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf[b], lane_dims, phi_box)) !=
-            CDFTB_OK)
-            return st;
-        if ((st = encode_map(&maps[b].prev, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf[b], lane_dims, prev_box)) !=
-            CDFTB_OK)
-            return st;
-    }
-    FilterMaps geo_maps{};
-    {
-        const unsigned tile_box[3] = {unsigned(tz), unsigned(TY), 1};
-        const int64_t d_w0[3] = {gp.nzg, ny, nx + 8};
-        const int64_t d_w1[3] = {gp.nzg, ny + 8, nx};
-        const unsigned b_w1[3] = {unsigned(tz), unsigned(TY + 7), 1};
-        const int64_t d_w2[3] = {gp.nz8g, ny, nx};
-        const unsigned b_w2[3] = {unsigned(tz + 8), unsigned(TY), 1};
-        const int64_t d_inv[3] = {gp.nzg, ny, nx};
-        const int64_t d_pot[4] = {gp.nzg, ny, nx, nsys};
-        const unsigned b_pot[4] = {unsigned(tz), unsigned(TY), 1, 1};
-        if ((st = encode_map(&geo_maps.w0, gt, sb, 3, w0p, d_w0, tile_box)) != CDFTB_OK) return st;
-        if ((st = encode_map(&geo_maps.w1, gt, sb, 3, w1p, d_w1, b_w1)) != CDFTB_OK) return st;
-        if ((st = encode_map(&geo_maps.w2, gt, sb, 3, w2p, d_w2, b_w2)) != CDFTB_OK) return st;
-        if ((st = encode_map(&geo_maps.inv, gt, sb, 3, invp, d_inv, tile_box)) != CDFTB_OK) return st;
-        if ((st = encode_map(&geo_maps.pot, gt, sb, 4, potp, d_pot, b_pot)) != CDFTB_OK) return st;
-    }
-    StaggeredTaps taps = staggered_taps(8);
+    const unsigned tile_box[3] = {unsigned(tz), unsigned(TY), 1};
+    const int64_t d_w0[3] = {gp.nzg, ny, nx + 8};
+    const int64_t d_w1[3] = {gp.nzg, ny + 8, nx};
+    const unsigned b_w1[3] = {unsigned(tz), unsigned(TY + 7), 1};
+    const int64_t d_w2[3] = {gp.nz8g, ny, nx};
+    const unsigned b_w2[3] = {unsigned(tz + 8), unsigned(TY), 1};
+    const int64_t d_inv[3] = {gp.nzg, ny, nx};
+    const int64_t d_pot[4] = {gp.nzg, ny, nx, nsys};
+    const unsigned b_pot[4] = {unsigned(tz), unsigned(TY), 1, 1};
+    if ((st = encode_map(&maps->w0, gt, sb, 3, w0p, d_w0, tile_box)) != CDFTB_OK) return st;
+    if ((st = encode_map(&maps->w1, gt, sb, 3, w1p, d_w1, b_w1)) != CDFTB_OK) return st;
+    if ((st = encode_map(&maps->w2, gt, sb, 3, w2p, d_w2, b_w2)) != CDFTB_OK) return st;
+    if ((st = encode_map(&maps->inv, gt, sb, 3, invp, d_inv, tile_box)) != CDFTB_OK) return st;
+    return encode_map(&maps->pot, gt, sb, 4, potp, d_pot, b_pot);
+}
+
+template <typename Lane>
+int pack_block(const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz, int nzp, int64_t lanes,
+               void* dst, cudaStream_t stream) {
+    const int64_t total = lanes * int64_t(nx) * ny * nzp;
+    const unsigned blocks = static_cast<unsigned>(std::min<int64_t>(ceil_div(total, 256), 148 * 16));
+    pack_lanes_kernel<Lane><<<blocks, 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
+                                                        static_cast<typename Lane::E*>(dst));
+    return check_launch();
+}
+
+int encode_lane_maps(void* buf, int nzp, int ny, int nx, int64_t lanes, int tz, CUtensorMap* phi, CUtensorMap* prev) {
+    const int64_t lane_dims[4] = {nzp, ny, nx, lanes};
+    const unsigned phi_box[4] = {unsigned(tz + 18), unsigned(NROW), 1, 1};
+    const unsigned prev_box[4] = {unsigned(tz), unsigned(TY), 1, 1};
+    int st = encode_map(phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, phi_box);
+    if (st == CDFTB_OK) st = encode_map(prev, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, prev_box);
+    return st;
+}
+
+FilterArgs base_args(const cdftb_operator* op, int64_t batch) {
     FilterArgs a{};
-    a.nx = nx;
-    a.ny = ny;
-    a.nz = nz;
-    a.nzp = nzp;
+    a.nx = op->nx;
+    a.ny = op->ny;
+    a.nz = op->nz;
+    a.nzp = padded_z(op->nz);
     a.batch = batch;
     a.orb_per_group = op->orbitals_per_group;
     a.shared_potential = op->potential_stride == 0;
-    a.coef = coefficients;
-    a.degree = degree;
+    const StaggeredTaps taps = staggered_taps(8);
     const double scale = 1.0 / op->spacing;  // taps c_k * (1/h), divergence.py:112, 121
     for (int j = 0; j < 8; ++j) a.taps[j] = taps.c[j] * scale;
+    return a;
+}
+
+template <typename Lane>
+int launch_any_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lanes, cudaStream_t stream) {
+    return tz == 36 ? launch_slab<Lane, 36>(m, a, lanes, stream) : launch_slab<Lane, 32>(m, a, lanes, stream);
+}
+
+template <typename Lane>
+int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype, void* work,
+                int64_t batch, const double* coefficients, int degree, cudaStream_t stream) {
+    const int nx = op->nx, ny = op->ny, nz = op->nz;
+    const int nzp = padded_z(nz);
+    const int64_t lanes = lanes_of(op, batch);
+    const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
+    char* w = static_cast<char*>(work);
+    void* buf[3] = {w, w + lanes * lane_bytes, w + 2 * lanes * lane_bytes};
+    const int tz = choose_tz(nzp);
+    int st = pack_block<Lane>(block, in_dtype, batch, nx, ny, nz, nzp, lanes, buf[2], stream);
+    if (st != CDFTB_OK) return st;
+    FilterMaps geo_maps{};
+    if ((st = prepare_geometry<Lane>(op, batch, w + 3 * lanes * lane_bytes, tz, false, &geo_maps, stream)) != CDFTB_OK)
+        return st;
+    FilterMaps maps[3];
+    for (int b = 0; b < 3; ++b)
+        if ((st = encode_lane_maps(buf[b], nzp, ny, nx, lanes, tz, &maps[b].phi, &maps[b].prev)) != CDFTB_OK) return st;
+    FilterArgs a = base_args(op, batch);
+    a.coef = coefficients;
+    a.degree = degree;
     // Y_1 -> buf0, Y_2 -> buf1, then Y_{k+1} overwrites Y_{k-1} in place (a point's previous value
     // is read only by the CTA that writes that point); the packed block is buf2.
     int y = 2, prev = -1;
@@ -806,12 +845,37 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
         FilterMaps m = geo_maps;
         m.phi = maps[y].phi;
         m.prev = maps[prev >= 0 ? prev : y].prev;
-        st = tz == 36 ? launch_slab<Lane, 36>(m, a, lanes, stream) : launch_slab<Lane, 32>(m, a, lanes, stream);
-        if (st != CDFTB_OK) return st;
+        if ((st = launch_any_tz<Lane>(tz, m, a, lanes, stream)) != CDFTB_OK) return st;
         prev = y;
         y = dst;
     }
     return CDFTB_OK;
+}
+
+template <typename Lane>
+int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* out, int out_dtype, void* work,
+               int64_t batch, int kinetic_only, cudaStream_t stream) {
+    const int nx = op->nx, ny = op->ny, nz = op->nz;
+    const int nzp = padded_z(nz);
+    const int64_t lanes = lanes_of(op, batch);
+    const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
+    char* w = static_cast<char*>(work);
+    const int tz = choose_tz(nzp);
+    int st = pack_block<Lane>(phi, in_dtype, batch, nx, ny, nz, nzp, lanes, w, stream);
+    if (st != CDFTB_OK) return st;
+    FilterMaps m{};
+    if ((st = prepare_geometry<Lane>(op, batch, w + lanes * lane_bytes, tz, kinetic_only != 0, &m, stream)) !=
+        CDFTB_OK)
+        return st;
+    if ((st = encode_lane_maps(w, nzp, ny, nx, lanes, tz, &m.phi, &m.prev)) != CDFTB_OK) return st;
+    FilterArgs a = base_args(op, batch);
+    a.apply_only = 1;
+    a.kinetic_only = kinetic_only != 0;
+    a.degree = 1;
+    a.final_out = 1;
+    a.out = out;
+    a.out_dtype = out_dtype;
+    return launch_any_tz<Lane>(tz, m, a, lanes, stream);
 }
 
 }  // namespace
@@ -824,6 +888,11 @@ int64_t slab_filter_work_bytes(const cdftb_operator* op, int64_t batch) {
 bool slab_filter_applies(const cdftb_operator* op) {
     return op->accuracy == 8 && (op->dtype == CDFTB_F32 || op->dtype == CDFTB_F64) && op->nx > 0 && op->ny > 0 &&
            op->nz > 0;
+}
+
+int64_t slab_apply_work_bytes(const cdftb_operator* op, int64_t batch) {
+    const int64_t sb = op->dtype == CDFTB_F32 ? 4 : 8;
+    return lanes_of(op, batch) * int64_t(op->nx) * op->ny * padded_z(op->nz) * 8 + geo_pack(op, batch).total() * sb;
 }
 
 int slab_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
@@ -875,4 +944,28 @@ extern "C" int cdftb_chebyshev_filter(const cdftb_operator* op, const void* bloc
                                             cdftb::as_stream(stream));
     return cdftb::generic_chebyshev_filter(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree,
                                            stream);
+}
+
+extern "C" int64_t cdftb_cusp_apply_work_bytes(const cdftb_operator* op, int64_t batch) {
+    if (!op || batch <= 0 || op->nx <= 0 || op->ny <= 0 || op->nz <= 0) return 0;
+    return cdftb::slab_filter_applies(op) ? cdftb::slab_apply_work_bytes(op, batch) : 0;
+}
+
+extern "C" int cdftb_cusp_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* out, int out_dtype,
+                                int64_t batch, int kinetic_only, void* work, int64_t work_bytes,
+                                cdftb_stream_t stream) {
+    if (!op || !phi || !out || batch < 0) return CDFTB_ERR_ARGUMENT;
+    if (batch == 0) return CDFTB_OK;
+    const bool slab = work && cdftb::slab_filter_applies(op) && work_bytes >= cdftb_cusp_apply_work_bytes(op, batch) &&
+                      reinterpret_cast<uintptr_t>(work) % 16 == 0 && op->spacing > 0.0 && op->face_weights[0] &&
+                      op->face_weights[1] && op->face_weights[2] && op->inverse_weight &&
+                      (kinetic_only || (op->potential && op->orbitals_per_group > 0)) &&
+                      (in_dtype == CDFTB_F64 || in_dtype == CDFTB_F32) &&
+                      (out_dtype == CDFTB_F64 || out_dtype == CDFTB_F32);
+    if (!slab)
+        return cdftb::generic_cusp_apply(op, phi, in_dtype, out, out_dtype, batch, kinetic_only, stream);
+    cudaStream_t s = cdftb::as_stream(stream);
+    if (op->dtype == CDFTB_F32)
+        return cdftb::slab_apply<cdftb::LaneF2>(op, phi, in_dtype, out, out_dtype, work, batch, kinetic_only, s);
+    return cdftb::slab_apply<cdftb::LaneD>(op, phi, in_dtype, out, out_dtype, work, batch, kinetic_only, s);
 }

@@ -108,8 +108,9 @@ __global__ void interpolate_kernel(const int* __restrict__ base, const double* _
 
 // out[f][j] = sum_{entries e of row j} x[f][node_e] * (wx wy wz)(node_e, j), one warp per grid point.
 __global__ void lift_kernel(const int* __restrict__ base, const double* __restrict__ w1d,
-                            const long long* __restrict__ row_ptr, const int* __restrict__ col, int64_t n_points, int ny,
-                            int nz, const double* __restrict__ x, int nf, int64_t x_stride, double* __restrict__ out,
+                            const long long* __restrict__ row_ptr, const int* __restrict__ col,
+                            const double* __restrict__ values, int64_t n_points, int ny, int nz,
+                            const double* __restrict__ x, int nf, int64_t x_stride, double* __restrict__ out,
                             int64_t out_stride) {
     const int64_t row = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -126,11 +127,16 @@ __global__ void lift_kernel(const int* __restrict__ base, const double* __restri
         const int jz = static_cast<int>(row % nz);
         for (long long e = e0 + lane; e < e1; e += 32) {
             const int node = col[e];
-            const int a = jx - (base[node * 3 + 0] - HALFD);
-            const int b = jy - (base[node * 3 + 1] - HALFD);
-            const int c = jz - (base[node * 3 + 2] - HALFD);
-            const double* w = w1d + static_cast<int64_t>(node) * 24;
-            const double v = (w[a] * w[8 + b]) * w[16 + c];
+            double v;
+            if (values) {
+                v = values[e];
+            } else {
+                const int a = jx - (base[node * 3 + 0] - HALFD);
+                const int b = jy - (base[node * 3 + 1] - HALFD);
+                const int c = jz - (base[node * 3 + 2] - HALFD);
+                const double* w = w1d + static_cast<int64_t>(node) * 24;
+                v = (w[a] * w[8 + b]) * w[16 + c];
+            }
             for (int f = 0; f < nf; ++f) acc[f] += x[f * x_stride + node] * v;
         }
     }
@@ -239,13 +245,298 @@ extern "C" int cdftb_quadrature_interpolate_f64(const int* base, const double* w
 }
 
 extern "C" int cdftb_quadrature_lift_f64(const int* base, const double* w1d, const long long* row_ptr, const int* col,
-                                         int nx, int ny, int nz, const double* node_values, int nf, int64_t x_stride,
-                                         double* out, int64_t out_stride, cdftb_stream_t stream) {
+                                         const double* values, int nx, int ny, int nz, const double* node_values,
+                                         int nf, int64_t x_stride, double* out, int64_t out_stride,
+                                         cdftb_stream_t stream) {
     const int64_t n_points = static_cast<int64_t>(nx) * ny * nz;
     if (nf < 1 || nf > 5 * 65535 || !base || !w1d || !row_ptr || !col || !node_values || !out || n_points <= 0)
         return CDFTB_ERR_ARGUMENT;
     dim3 grid(blocks_for(n_points * 32, 256), static_cast<unsigned>(ceil_div(nf, 5)));
-    lift_kernel<<<grid, 256, 0, as_stream(stream)>>>(base, w1d, row_ptr, col, n_points, ny, nz, node_values, nf, x_stride,
-                                                     out, out_stride);
+    lift_kernel<<<grid, 256, 0, as_stream(stream)>>>(base, w1d, row_ptr, col, values, n_points, ny, nz, node_values, nf,
+                                                     x_stride, out, out_stride);
     return check_launch();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Many fields at once (the batched systems): L and L^T for up to 32 fields per pass with one lane
+// per field. The fields are first copied into point-major rows of 32 (scratch), so that the value of
+// every field at one grid point (or node) is one coalesced 256-byte row; a warp then walks one node's
+// 512 stencil points (interpolate) or one grid point's CSR row (lift) once for all fields, instead
+// of once per 5 fields. Results pass through a shared tile so that the field-major stores coalesce.
+
+namespace cdftb {
+namespace {
+
+constexpr int MANY = 32;
+constexpr int kLiftSegment = 256;  // CSR entries per warp task of the many-field lift
+
+// src[f * stride + i] (f < nf, i < n) -> dst[i * 32 + f], zero for f >= nf.
+__global__ void fields_to_rows_kernel(const double* __restrict__ src, int nf, int64_t stride, int64_t n,
+                                      double* __restrict__ dst) {
+    __shared__ double tile[MANY][MANY + 1];
+    const int64_t i0 = int64_t(blockIdx.x) * MANY;
+    for (int f = threadIdx.y; f < MANY; f += blockDim.y) {
+        const int64_t i = i0 + threadIdx.x;
+        tile[f][threadIdx.x] = (f < nf && i < n) ? src[f * stride + i] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < MANY; r += blockDim.y) {
+        const int64_t i = i0 + r;
+        if (i < n) dst[i * MANY + threadIdx.x] = tile[threadIdx.x][r];
+    }
+}
+
+// A CTA of 8 warps handles 32 consecutive outputs (nodes or grid points), 4 per warp; tile[j][f].
+__device__ __forceinline__ void store_tile(double (*tile)[MANY + 1], int64_t j0, int64_t count, int nf,
+                                           double* __restrict__ out, int64_t out_stride) {
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (int f = threadIdx.x >> 5; f < nf; f += blockDim.x >> 5)
+        if (j0 + lane < count) out[f * out_stride + j0 + lane] = tile[lane][f];
+}
+
+__global__ void __launch_bounds__(256) interpolate_many_kernel(const int* __restrict__ base,
+                                                               const double* __restrict__ w1d, int64_t m, int ny,
+                                                               int nz, const double* __restrict__ rows, int nf,
+                                                               double* __restrict__ out, int64_t out_stride) {
+    __shared__ double tile[MANY][MANY + 1];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int64_t j0 = int64_t(blockIdx.x) * MANY;
+    for (int r = warp; r < MANY; r += 8) {
+        const int64_t node = j0 + r;
+        if (node >= m) break;
+        const int bx = base[node * 3 + 0] - HALFD, by = base[node * 3 + 1] - HALFD, bz = base[node * 3 + 2] - HALFD;
+        const double* w = w1d + node * 24;
+        const double wl = w[lane < 24 ? lane : 0];  // the 24 1-D weights, one per lane, then shuffled
+        double acc = 0.0;
+        for (int a = 0; a < KTAP; ++a) {
+            const double wa = __shfl_sync(0xffffffffu, wl, a);
+            for (int b = 0; b < KTAP; ++b) {
+                const double wab = wa * __shfl_sync(0xffffffffu, wl, 8 + b);
+                const double* row = rows + ((int64_t(bx + a) * ny + (by + b)) * nz + bz) * MANY + lane;
+#pragma unroll
+                for (int c = 0; c < KTAP; ++c) {
+                    const double v = wab * __shfl_sync(0xffffffffu, wl, 16 + c);
+                    acc += v * row[c * MANY];
+                }
+            }
+        }
+        tile[r][lane] = acc;
+    }
+    store_tile(tile, j0, m, nf, out, out_stride);
+}
+
+int fields_to_rows(const double* src, int nf, int64_t stride, int64_t n, double* dst, cudaStream_t s) {
+    fields_to_rows_kernel<<<static_cast<unsigned>(ceil_div(n, MANY)), dim3(MANY, 8), 0, s>>>(src, nf, stride, n, dst);
+    return check_launch();
+}
+
+}  // namespace
+}  // namespace cdftb
+
+extern "C" int64_t cdftb_lift_segments_capacity(int64_t m, int64_t n_points) {
+    if (m < 0 || n_points < 0) return 0;
+    return m * 512 / cdftb::kLiftSegment + n_points + 1;
+}
+
+extern "C" int64_t cdftb_quadrature_many_scratch_bytes(int64_t m, int64_t n_points) {
+    if (m < 0 || n_points < 0) return 0;
+    const int64_t lift = m + cdftb_lift_segments_capacity(m, n_points);  // node rows + segment partials
+    return (lift > n_points ? lift : n_points) * cdftb::MANY * 8;
+}
+
+extern "C" int cdftb_quadrature_interpolate_many_f64(const int* base, const double* w1d, int64_t m, int nx, int ny,
+                                                     int nz, const double* fields, int nf, int64_t field_stride,
+                                                     double* out, int64_t out_stride, void* scratch,
+                                                     int64_t scratch_bytes, cdftb_stream_t stream) {
+    const int64_t n_points = int64_t(nx) * ny * nz;
+    if (m < 0 || nf < 1 || n_points <= 0 || (m > 0 && (!base || !w1d || !fields || !out || !scratch)))
+        return CDFTB_ERR_ARGUMENT;
+    if (scratch_bytes < n_points * cdftb::MANY * 8) return CDFTB_ERR_ARGUMENT;
+    if (m == 0) return CDFTB_OK;
+    cudaStream_t s = as_stream(stream);
+    double* rows = static_cast<double*>(scratch);
+    for (int f0 = 0; f0 < nf; f0 += cdftb::MANY) {
+        const int count = nf - f0 < cdftb::MANY ? nf - f0 : cdftb::MANY;
+        int st = cdftb::fields_to_rows(fields + f0 * field_stride, count, field_stride, n_points, rows, s);
+        if (st != CDFTB_OK) return st;
+        cdftb::interpolate_many_kernel<<<static_cast<unsigned>(ceil_div(m, cdftb::MANY)), 256, 0, s>>>(
+            base, w1d, m, ny, nz, rows, count, out + f0 * out_stride, out_stride);
+        st = check_launch();
+        if (st != CDFTB_OK) return st;
+    }
+    return CDFTB_OK;
+}
+
+// The weight of every CSR entry of L^T (the same product as the lift kernels form on the fly).
+namespace cdftb {
+namespace {
+__global__ void lift_values_kernel(const int* __restrict__ base, const double* __restrict__ w1d,
+                                   const long long* __restrict__ row_ptr, const int* __restrict__ col, int64_t n_points,
+                                   int ny, int nz, double* __restrict__ values) {
+    const int64_t row = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n_points) return;
+    const int jx = static_cast<int>(row / (static_cast<int64_t>(ny) * nz));
+    const int jy = static_cast<int>((row / nz) % ny);
+    const int jz = static_cast<int>(row % nz);
+    for (long long e = row_ptr[row] + lane; e < row_ptr[row + 1]; e += 32) {
+        const int node = col[e];
+        const int a = jx - (base[node * 3 + 0] - HALFD);
+        const int b = jy - (base[node * 3 + 1] - HALFD);
+        const int c = jz - (base[node * 3 + 2] - HALFD);
+        const double* w = w1d + static_cast<int64_t>(node) * 24;
+        values[e] = (w[a] * w[8 + b]) * w[16 + c];
+    }
+}
+}  // namespace
+}  // namespace cdftb
+
+extern "C" int cdftb_lift_plan_values_f64(const int* base, const double* w1d, const long long* row_ptr, const int* col,
+                                          int nx, int ny, int nz, double* values, cdftb_stream_t stream) {
+    const int64_t n_points = static_cast<int64_t>(nx) * ny * nz;
+    if (!base || !w1d || !row_ptr || !col || !values || n_points <= 0) return CDFTB_ERR_ARGUMENT;
+    cdftb::lift_values_kernel<<<blocks_for(n_points * 32, 256), 256, 0, as_stream(stream)>>>(base, w1d, row_ptr, col,
+                                                                                             n_points, ny, nz, values);
+    return check_launch();
+}
+
+// ---------------------------------------------------------------------------------------------
+// L^T for many fields with the CSR rows cut into segments of at most kLiftSegment entries. The rows
+// are very uneven (thousands of entries next to a nucleus, none far away), so one warp per segment
+// rather than per row keeps every SM busy; each segment leaves a 32-field partial and a second pass
+// adds the partials of a row in segment order (deterministic).
+
+namespace cdftb {
+namespace {
+
+__global__ void segment_counts_kernel(const long long* __restrict__ row_ptr, int64_t n_points, int* __restrict__ counts) {
+    const int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (r < n_points) {
+        const long long len = row_ptr[r + 1] - row_ptr[r];
+        counts[r] = static_cast<int>((len + kLiftSegment - 1) / kLiftSegment);
+    } else if (r == n_points) {
+        counts[r] = 0;
+    }
+}
+
+__global__ void segment_rows_kernel(const int* __restrict__ seg_ptr, int64_t n_points, int* __restrict__ seg_row) {
+    const int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (r >= n_points) return;
+    for (int sgi = seg_ptr[r]; sgi < seg_ptr[r + 1]; ++sgi) seg_row[sgi] = static_cast<int>(r);
+}
+
+__global__ void __launch_bounds__(256) lift_segments_kernel(const long long* __restrict__ row_ptr,
+                                                            const int* __restrict__ col,
+                                                            const double* __restrict__ values,
+                                                            const int* __restrict__ seg_ptr,
+                                                            const int* __restrict__ seg_row, int64_t n_points,
+                                                            const double* __restrict__ rows,
+                                                            double* __restrict__ partial) {
+    const int64_t sgi = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (sgi >= seg_ptr[n_points]) return;
+    const int r = seg_row[sgi];
+    const long long eb0 = row_ptr[r] + (sgi - seg_ptr[r]) * int64_t(kLiftSegment);
+    const long long ee = min(row_ptr[r + 1], eb0 + kLiftSegment);
+    double acc = 0.0;
+    for (long long eb = eb0; eb < ee; eb += 32) {
+        int node_l = 0;
+        double v_l = 0.0;
+        if (eb + lane < ee) {
+            node_l = col[eb + lane];
+            v_l = values[eb + lane];
+        }
+        const int count = (ee - eb) < 32 ? static_cast<int>(ee - eb) : 32;
+        int k = 0;
+        for (; k + 8 <= count; k += 8) {
+            double g[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) g[u] = rows[int64_t(__shfl_sync(0xffffffffu, node_l, k + u)) * MANY + lane];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc += g[u] * __shfl_sync(0xffffffffu, v_l, k + u);
+        }
+        for (; k < count; ++k)
+            acc += rows[int64_t(__shfl_sync(0xffffffffu, node_l, k)) * MANY + lane] * __shfl_sync(0xffffffffu, v_l, k);
+    }
+    partial[sgi * MANY + lane] = acc;
+}
+
+__global__ void __launch_bounds__(256) lift_segments_sum_kernel(const int* __restrict__ seg_ptr, int64_t n_points,
+                                                                const double* __restrict__ partial, int nf,
+                                                                double* __restrict__ out, int64_t out_stride) {
+    __shared__ double tile[MANY][MANY + 1];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int64_t j0 = int64_t(blockIdx.x) * MANY;
+    for (int r = warp; r < MANY; r += 8) {
+        const int64_t row = j0 + r;
+        if (row >= n_points) break;
+        double acc = 0.0;
+        for (int sgi = seg_ptr[row]; sgi < seg_ptr[row + 1]; ++sgi) acc += partial[int64_t(sgi) * MANY + lane];
+        tile[r][lane] = acc;
+    }
+    store_tile(tile, j0, n_points, nf, out, out_stride);
+}
+
+}  // namespace
+}  // namespace cdftb
+
+extern "C" int64_t cdftb_lift_segments_scratch_bytes(int64_t n_points) {
+    if (n_points <= 0) return 0;
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, static_cast<int*>(nullptr), static_cast<int*>(nullptr),
+                                  static_cast<int>(n_points + 1));
+    return static_cast<int64_t>(((n_points + 1) * 4 + 255) / 256 * 256 + scan_bytes);
+}
+
+extern "C" int cdftb_lift_plan_segments(const long long* row_ptr, int nx, int ny, int nz, int* seg_ptr, int* seg_row,
+                                        int64_t capacity, void* scratch, int64_t scratch_bytes,
+                                        cdftb_stream_t stream) {
+    const int64_t n_points = int64_t(nx) * ny * nz;
+    if (!row_ptr || !seg_ptr || !seg_row || !scratch || n_points <= 0 || n_points >= (1ll << 31) - 1)
+        return CDFTB_ERR_ARGUMENT;
+    if (scratch_bytes < cdftb_lift_segments_scratch_bytes(n_points)) return CDFTB_ERR_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    int* counts = static_cast<int*>(scratch);
+    char* temp = static_cast<char*>(scratch) + ((n_points + 1) * 4 + 255) / 256 * 256;
+    size_t scan_bytes = static_cast<size_t>(scratch_bytes) - (temp - static_cast<char*>(scratch));
+    cdftb::segment_counts_kernel<<<blocks_for(n_points + 1, 256), 256, 0, s>>>(row_ptr, n_points, counts);
+    int st = check_launch();
+    if (st != CDFTB_OK) return st;
+    if ((st = check(cub::DeviceScan::ExclusiveSum(temp, scan_bytes, counts, seg_ptr, static_cast<int>(n_points + 1),
+                                                  s))) != CDFTB_OK)
+        return st;
+    // capacity bounds the segment count by construction: sum ceil(len/S) <= nnz/S + rows
+    (void)capacity;
+    cdftb::segment_rows_kernel<<<blocks_for(n_points, 256), 256, 0, s>>>(seg_ptr, n_points, seg_row);
+    return check_launch();
+}
+
+extern "C" int cdftb_quadrature_lift_many_f64(const long long* row_ptr, const int* col, const double* values,
+                                              const int* seg_ptr, const int* seg_row, int64_t seg_capacity, int nx,
+                                              int ny, int nz, int64_t m, const double* node_values, int nf,
+                                              int64_t x_stride, double* out, int64_t out_stride, void* scratch,
+                                              int64_t scratch_bytes, cdftb_stream_t stream) {
+    const int64_t n_points = int64_t(nx) * ny * nz;
+    if (m <= 0 || nf < 1 || n_points <= 0 || !row_ptr || !col || !values || !seg_ptr || !seg_row || !node_values ||
+        !out || !scratch || seg_capacity < cdftb_lift_segments_capacity(m, n_points))
+        return CDFTB_ERR_ARGUMENT;
+    if (scratch_bytes < (m + seg_capacity) * cdftb::MANY * 8) return CDFTB_ERR_ARGUMENT;
+    cudaStream_t s = as_stream(stream);
+    double* rows = static_cast<double*>(scratch);
+    double* partial = rows + m * cdftb::MANY;
+    for (int f0 = 0; f0 < nf; f0 += cdftb::MANY) {
+        const int count = nf - f0 < cdftb::MANY ? nf - f0 : cdftb::MANY;
+        int st = cdftb::fields_to_rows(node_values + f0 * x_stride, count, x_stride, m, rows, s);
+        if (st != CDFTB_OK) return st;
+        cdftb::lift_segments_kernel<<<blocks_for(seg_capacity * 32, 256), 256, 0, s>>>(row_ptr, col, values, seg_ptr,
+                                                                                       seg_row, n_points, rows, partial);
+        if ((st = check_launch()) != CDFTB_OK) return st;
+        cdftb::lift_segments_sum_kernel<<<static_cast<unsigned>(ceil_div(n_points, cdftb::MANY)), 256, 0, s>>>(
+            seg_ptr, n_points, partial, count, out + f0 * out_stride, out_stride);
+        if ((st = check_launch()) != CDFTB_OK) return st;
+    }
+    return CDFTB_OK;
 }

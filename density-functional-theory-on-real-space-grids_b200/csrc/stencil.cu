@@ -532,8 +532,9 @@ extern "C" int cdftb_weighted_divergence_f64(const double* box, double* out, int
     return launch(a, accuracy, spacing, CDFTB_F64, as_stream(stream));
 }
 
-extern "C" int cdftb_cusp_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* out, int out_dtype,
-                                int64_t batch, int kinetic_only, cdftb_stream_t stream) {
+// The apply for any order on the caller's layout: one stencil_kernel launch.
+int cdftb::generic_cusp_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* out, int out_dtype,
+                              int64_t batch, int kinetic_only, cdftb_stream_t stream) {
     if (!op) return CDFTB_ERR_ARGUMENT;
     StencilArgs a = args_from_operator(op);
     a.in = phi;

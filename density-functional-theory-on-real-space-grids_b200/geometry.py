@@ -286,6 +286,19 @@ class CuspQuadrature:
         call("cdftb_lift_plan_build", ptr(self.base), m, *grid.shape, ptr(self.row_ptr), ptr(self.col), ptr(scratch),
              scratch.numel(), stream)
         del scratch
+        # the weight of every entry of L^T, formed once (the lifts then stream (col, value) pairs)
+        self.lift_values = torch.empty(m * 512, dtype=torch.float64, device=dev)
+        call("cdftb_lift_plan_values_f64", ptr(self.base), ptr(self.w1d), ptr(self.row_ptr), ptr(self.col),
+             *grid.shape, ptr(self.lift_values), stream)
+        # the rows of L^T cut into segments of at most 256 entries (the many-field lift's work units)
+        lib = _lib.library()
+        self.seg_capacity = lib.cdftb_lift_segments_capacity(m, n)
+        self.seg_ptr = torch.empty(n + 1, dtype=torch.int32, device=dev)
+        self.seg_row = torch.empty(self.seg_capacity, dtype=torch.int32, device=dev)
+        seg_scratch = torch.empty(lib.cdftb_lift_segments_scratch_bytes(n), dtype=torch.uint8, device=dev)
+        call("cdftb_lift_plan_segments", ptr(self.row_ptr), *grid.shape, ptr(self.seg_ptr), ptr(self.seg_row),
+             self.seg_capacity, ptr(seg_scratch), seg_scratch.numel(), stream)
+        del seg_scratch
         # far factor, plain and lumped far mass weights
         self.far = torch.empty(n, **f)
         self.far_weights = torch.empty(n, **f)
@@ -332,9 +345,22 @@ class CuspQuadrature:
         return out
 
     # --- interpolation and its transpose (quadrature.py:613-650) ---
+    #: From this many fields on, L and L^T run one pass per 32 fields (the batched systems).
+    MANY_FIELDS = 8
+
+    def _many_scratch(self, device) -> torch.Tensor:
+        nbytes = _lib.library().cdftb_quadrature_many_scratch_bytes(self.n_nodes, self.grid.n_points)
+        return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
     def _interp_raw(self, fields: torch.Tensor, nf: int) -> torch.Tensor:
         n = self.grid.n_points
         out = torch.empty((nf, self.n_nodes), dtype=torch.float64, device=fields.device)
+        if nf >= self.MANY_FIELDS:
+            scratch = self._many_scratch(fields.device)
+            call("cdftb_quadrature_interpolate_many_f64", ptr(self.base), ptr(self.w1d), self.n_nodes,
+                 *self.grid.shape, ptr(fields), nf, n, ptr(out), self.n_nodes, ptr(scratch), scratch.numel(),
+                 stream_handle(fields.device))
+            return out
         call("cdftb_quadrature_interpolate_f64", ptr(self.base), ptr(self.w1d), self.n_nodes, *self.grid.shape,
              ptr(fields), nf, n, ptr(out), self.n_nodes, stream_handle(fields.device))
         return out
@@ -342,8 +368,14 @@ class CuspQuadrature:
     def _lift_raw(self, x: torch.Tensor, nf: int) -> torch.Tensor:
         n = self.grid.n_points
         out = torch.empty((nf, n), dtype=torch.float64, device=x.device)
+        if nf >= self.MANY_FIELDS:
+            scratch = self._many_scratch(x.device)
+            call("cdftb_quadrature_lift_many_f64", ptr(self.row_ptr), ptr(self.col), ptr(self.lift_values),
+                 ptr(self.seg_ptr), ptr(self.seg_row), self.seg_capacity, *self.grid.shape, self.n_nodes, ptr(x), nf,
+                 self.n_nodes, ptr(out), n, ptr(scratch), scratch.numel(), stream_handle(x.device))
+            return out
         call("cdftb_quadrature_lift_f64", ptr(self.base), ptr(self.w1d), ptr(self.row_ptr), ptr(self.col),
-             *self.grid.shape, ptr(x), nf, self.n_nodes, ptr(out), n, stream_handle(x.device))
+             ptr(self.lift_values), *self.grid.shape, ptr(x), nf, self.n_nodes, ptr(out), n, stream_handle(x.device))
         return out
 
     def interpolate(self, field: torch.Tensor) -> torch.Tensor:

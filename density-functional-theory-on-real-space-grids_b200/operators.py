@@ -22,6 +22,12 @@ def _scratch(nbytes: int, device) -> torch.Tensor:
     return torch.empty(max(int(nbytes), 8), dtype=torch.uint8, device=device)
 
 
+def apply_workspace(op, batch: int, device: torch.device) -> torch.Tensor:
+    """Device scratch of the one-launch apply (``cdftb_cusp_apply_work_bytes``), as bytes."""
+    nbytes = _lib.library().cdftb_cusp_apply_work_bytes(ctypes.byref(op), batch)
+    return torch.empty(max(nbytes, 16), dtype=torch.uint8, device=device)
+
+
 def measure_cross(a: torch.Tensor, b: torch.Tensor, q: torch.Tensor | None, groups: int = 1) -> torch.Tensor:
     """``out[g] = (a[g] * q) @ b[g].T`` for ``groups`` stacked blocks (float64, deterministic)."""
     n = a.shape[-1]
@@ -191,8 +197,9 @@ class CuspFactoredHamiltonian:
         batch = x.numel() // self.grid.n_points
         out = torch.empty_like(x)
         op = self.operator(potential)
+        work = apply_workspace(op, batch, x.device)
         call("cdftb_cusp_apply", ctypes.byref(op), ptr(x), _lib.dtype_code(x), ptr(out), _lib.dtype_code(out), batch,
-             1 if kinetic_only else 0, stream_handle(phi.device))
+             1 if kinetic_only else 0, ptr(work), work.numel(), stream_handle(phi.device))
         return out
 
     def apply(self, phi: torch.Tensor) -> torch.Tensor:

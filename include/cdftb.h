@@ -68,10 +68,14 @@ int cdftb_weighted_divergence_f64(const double* box, double* out, int64_t batch,
                                   int accuracy, cdftb_stream_t stream);
 
 /* (a2) out = A phi for a batch of orbitals (src/cdft/operators/hamiltonian.py:251-318,
- * apply / apply_with_potential / kinetic_apply). phi must be in the operator's dtype; out may be
- * double or float (out_dtype). kinetic_only = 1 drops the V phi term (hamiltonian.py:303). */
+ * apply / apply_with_potential / kinetic_apply). out may be double or float (out_dtype).
+ * kinetic_only = 1 drops the V phi term (hamiltonian.py:303). With device scratch of at least
+ * cdftb_cusp_apply_work_bytes(op, batch) bytes (work, work_bytes; non-zero only for order 8) the
+ * apply runs as one launch of the slab kernel (phi in either dtype); with work NULL it runs the
+ * generic stencil on the caller's layout (phi must then be in the operator's dtype). */
+int64_t cdftb_cusp_apply_work_bytes(const cdftb_operator* op, int64_t batch);
 int cdftb_cusp_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* out, int out_dtype,
-                     int64_t batch, int kinetic_only, cdftb_stream_t stream);
+                     int64_t batch, int kinetic_only, void* work, int64_t work_bytes, cdftb_stream_t stream);
 
 /* Slab tile of the apply/filter kernels, process-wide: tile_y rows (4, 8 or 16) of 32 z columns per
  * CTA, x chunks no shorter than min_chunk planes, about ctas_per_sm CTAs per SM. Chosen by the
@@ -202,10 +206,33 @@ int cdftb_lift_plan_build(const int* base, int64_t m, int nx, int ny, int nz, lo
 int cdftb_quadrature_interpolate_f64(const int* base, const double* w1d, int64_t m, int nx, int ny, int nz,
                                      const double* fields, int nf, int64_t field_stride, double* out,
                                      int64_t out_stride, cdftb_stream_t stream);
-/* out[f] = L^T x_f for nf node vectors (quadrature.py:628-638 lift). */
-int cdftb_quadrature_lift_f64(const int* base, const double* w1d, const long long* row_ptr, const int* col, int nx,
-                              int ny, int nz, const double* node_values, int nf, int64_t x_stride, double* out,
-                              int64_t out_stride, cdftb_stream_t stream);
+/* values[e] = the weight of CSR entry e of L^T (row_ptr[nx*ny*nz] entries), for the lifts below. */
+int cdftb_lift_plan_values_f64(const int* base, const double* w1d, const long long* row_ptr, const int* col, int nx,
+                               int ny, int nz, double* values, cdftb_stream_t stream);
+/* out[f] = L^T x_f for nf node vectors (quadrature.py:628-638 lift). values: the entry weights of
+ * cdftb_lift_plan_values_f64, or NULL to form them from base and w1d on the fly. */
+int cdftb_quadrature_lift_f64(const int* base, const double* w1d, const long long* row_ptr, const int* col,
+                              const double* values, int nx, int ny, int nz, const double* node_values, int nf,
+                              int64_t x_stride, double* out, int64_t out_stride, cdftb_stream_t stream);
+/* The same two products for many fields (the systems of a batch): up to 32 fields per pass, one
+ * lane per field, after copying the fields into point-major rows of 32 in caller scratch of
+ * cdftb_quadrature_many_scratch_bytes(m, n_points) bytes. The lift walks the CSR rows in segments
+ * of at most 256 entries (cdftb_lift_plan_segments: seg_ptr[n_points + 1], seg_row[capacity],
+ * capacity = cdftb_lift_segments_capacity(m, n_points)) and needs the entry weights (values).
+ * Results equal the one-field entry points up to the order of the sums (~1e-16 relative). */
+int64_t cdftb_quadrature_many_scratch_bytes(int64_t m, int64_t n_points);
+int64_t cdftb_lift_segments_capacity(int64_t m, int64_t n_points);
+int64_t cdftb_lift_segments_scratch_bytes(int64_t n_points);
+int cdftb_lift_plan_segments(const long long* row_ptr, int nx, int ny, int nz, int* seg_ptr, int* seg_row,
+                             int64_t capacity, void* scratch, int64_t scratch_bytes, cdftb_stream_t stream);
+int cdftb_quadrature_interpolate_many_f64(const int* base, const double* w1d, int64_t m, int nx, int ny, int nz,
+                                          const double* fields, int nf, int64_t field_stride, double* out,
+                                          int64_t out_stride, void* scratch, int64_t scratch_bytes,
+                                          cdftb_stream_t stream);
+int cdftb_quadrature_lift_many_f64(const long long* row_ptr, const int* col, const double* values, const int* seg_ptr,
+                                   const int* seg_row, int64_t seg_capacity, int nx, int ny, int nz, int64_t m,
+                                   const double* node_values, int nf, int64_t x_stride, double* out,
+                                   int64_t out_stride, void* scratch, int64_t scratch_bytes, cdftb_stream_t stream);
 
 /* ---- (c2, s1) the Kohn-Sham potentials (src/cdft/scf/step.py:224-313) ---- */
 

@@ -199,3 +199,23 @@ def test_config2_he65_lda_scf(pkg, cuda, golden_values):
     assert out.converged
     assert abs(out.energies["total"] - ref["total"]) < 1e-10
     assert out.scf_iterations == ref["iterations"]
+
+
+@pytest.mark.parametrize("nf", [8, 13, 40])
+def test_interpolate_and_lift_many_fields(pkg, he25, cuda, nf):
+    """The 32-fields-per-pass L and L^T (batched systems) against the one-field path."""
+    _, geo, (grid_o, _, quad_o) = he25
+    quad = geo.quadrature
+    g = torch.Generator().manual_seed(nf)
+    fields = torch.randn((nf, geo.grid.n_points), dtype=torch.float64, generator=g).to(cuda)
+    nodes = torch.randn((nf, quad.n_nodes), dtype=torch.float64, generator=g).to(cuda)
+    many_i = quad._interp_raw(fields.contiguous(), nf)
+    many_l = quad._lift_raw(nodes.contiguous(), nf)
+    for f in (0, nf // 2, nf - 1):
+        one_i = quad._interp_raw(fields[f:f + 1].contiguous(), 1)[0]
+        one_l = quad._lift_raw(nodes[f:f + 1].contiguous(), 1)[0]
+        torch.testing.assert_close(many_i[f], one_i, rtol=0, atol=1e-13 * float(one_i.abs().max()))
+        torch.testing.assert_close(many_l[f], one_l, rtol=0, atol=1e-13 * float(one_l.abs().max()))
+    # and the oracle, for one field
+    want = quad_o.interpolate(_np(fields[0]))
+    np.testing.assert_allclose(_np(many_i[0]), want, rtol=0, atol=1e-12 * np.abs(want).max())

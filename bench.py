@@ -269,6 +269,27 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def replica_seeds(rank: int, batch: int) -> list[int]:
+    """Seeds of the independent systems one replica solves: disjoint across ranks."""
+    return [rank * batch + k for k in range(batch)]
+
+
+def max_over_ranks(seconds: float, dist, device) -> float:
+    """The slowest rank's time (all-reduce MAX); the local time without a process group."""
+    if dist is None:
+        return seconds
+    import torch
+
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, batch: int, steps: int, seconds: float) -> float:
+    """Solves per second of the whole job: every rank solves `batch` systems per step."""
+    return world * batch * steps / seconds
+
+
 def main() -> None:
     args = _args()
     if args.impl == "reference":
@@ -317,7 +338,7 @@ def main() -> None:
             return [out.energies["total"]], out.density, out.scf_iterations, out.applications
     else:
         # independent systems: the same atom from different seeded random starts (seed = rank * batch + b)
-        seeds = [rank * batch + k for k in range(batch)]
+        seeds = replica_seeds(rank, batch)
         step = pkg.batch.BatchedKohnShamStep(geometry, "lda_vwn", system.n_electrons, batch, seeds=seeds,
                                              filter_precision=precision)
         n0 = step.initial_density()
@@ -355,12 +376,8 @@ def main() -> None:
     if dist is not None:
         dist.barrier()
     clocks = sampler.stop()
-    seconds = total_ms / 1e3
-    if dist is not None:
-        t = torch.tensor([seconds], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        seconds = float(t.item())
-    value = world * batch * args.steps / seconds
+    seconds = max_over_ranks(total_ms / 1e3, dist, dev)
+    value = whole_job_rate(world, batch, args.steps, seconds)
     error = max(abs(e - golden["total"]) for e in energies)
 
     # --- end to end through the public API with host buffers ---
@@ -378,12 +395,8 @@ def main() -> None:
         end.record(stream)
         end.synchronize()
         e2e_ms += start.elapsed_time(end)
-    e2e_s = e2e_ms / 1e3
-    if dist is not None:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * batch * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(e2e_ms / 1e3, dist, dev)
+    e2e_value = whole_job_rate(world, batch, e2e_steps, e2e_s)
     bytes_in = host_in.numel() * host_in.element_size()
     bytes_out = host_out.numel() * host_out.element_size() + 8 * 12 * batch
 

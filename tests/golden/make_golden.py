@@ -62,6 +62,8 @@ def numerics(spacing, box, degree=20, mixing=None, residual_tol=1e-8):
 
 
 LINEAR = MixingConfig(scheme=MixingScheme.LINEAR, alpha=0.3)
+# config 4's scan is R = 0.8 + k * 5.2 / 47, k = 0..47; these are five of its members
+SCAN_SAMPLES = tuple(0.8 + k * 5.2 / 47 for k in (0, 11, 23, 35, 47))
 PROBE_SEED = 1234
 
 
@@ -79,6 +81,8 @@ def checks(t: torch.Tensor) -> list[float]:
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--with-65", action="store_true")
+    parser.add_argument("--with-config3", action="store_true", help="H2 PBE at 81 x 81 x 91 (tens of minutes)")
+    parser.add_argument("--with-scan", action="store_true", help="five members of the H2+ bond scan")
     args = parser.parse_args()
     arrays: dict[str, np.ndarray] = {}
     values: dict[str, object] = {}
@@ -227,6 +231,15 @@ def main() -> None:
     timed("h2_pbe_h04", lambda: solve_self_consistent(h2, numerics(0.4, (10.0, 10.0, 11.2), degree=16), derive_grid=False))
     if args.with_65:
         timed("he65_lda_linear", lambda: solve_self_consistent(scenario, numerics(0.25, (16.0, 16.0, 16.0), mixing=LINEAR), derive_grid=False))
+    if args.with_config3:
+        # config 3: H2 (R = 1.4) PBE, box 16 x 16 x 18, h = 0.20 -> 81 x 81 x 91, degree 16, unanchored lattice
+        timed("h2_pbe_h020", lambda: solve_self_consistent(h2, numerics(0.20, (16.0, 16.0, 18.0), degree=16),
+                                                          derive_grid=False))
+    if args.with_scan:
+        # config 4 samples: bare H2+ at R in [0.8, 6.0], box (12, 12, R + 12), h = 0.25
+        for bond in SCAN_SAMPLES:
+            timed(f"h2plus_scan_R{bond:.4f}", lambda b=bond: solve_noninteracting(
+                h2_plus(b), numerics(0.25, (12.0, 12.0, b + 12.0)), derive_grid=False))
 
     np.savez_compressed(OUT / "reference_fixtures.npz", **arrays)
     old = {}

@@ -43,6 +43,13 @@ class UniformGrid:
     def volume_element(self) -> float:
         return self.spacing ** 3
 
+    def points(self) -> torch.Tensor:
+        """Cartesian coordinates of every grid point, ``(N, 3)`` float64 in C order (grid.py points)."""
+        axes = [torch.arange(n, dtype=torch.float64, device=self.device) * self.spacing + o
+                for n, o in zip(self.shape, self.origin)]
+        x, y, z = torch.meshgrid(*axes, indexing="ij")
+        return torch.stack([x.reshape(-1), y.reshape(-1), z.reshape(-1)], dim=1)
+
     def scatter_to_box(self, field: torch.Tensor) -> torch.Tensor:
         return field.reshape(*field.shape[:-1], *self.shape)
 

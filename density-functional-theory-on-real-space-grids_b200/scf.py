@@ -77,7 +77,11 @@ class KohnShamStep:
 
     def __init__(self, geometry: CuspGeometry, functional: str, n_electrons: float, eigen: EigenConfig | None = None,
                  *, seed: int = 0, pad_factor: float = 2.5, filter_precision: torch.dtype = torch.float64,
-                 n_states: int | None = None) -> None:
+                 n_states: int | None = None, external_potential: torch.Tensor | None = None) -> None:
+        # external_potential: an extra diagonal term of the operator (an external perturbation in the
+        # form quadrature.effective_potential gives it). It enters the Hamiltonian and so the band
+        # energy, but not the Hartree/XC double counting, so the total energy gains Q[n dv].
+        self.external = None if external_potential is None else external_potential.to(torch.float64).contiguous()
         self.geometry = geometry
         self.grid = geometry.grid
         self.factor = geometry.factor
@@ -212,8 +216,9 @@ class KohnShamStep:
                           xc_energy=xc_energy, xc_double_counting=xc_dc, hartree_coefficients=coef)
 
     def hamiltonian(self, potentials: Potentials, *, dtype: torch.dtype = torch.float64) -> CuspFactoredHamiltonian:
-        return CuspFactoredHamiltonian(self.grid, self.factor, extra_potential=potentials.effective,
-                                       quadrature=self.quadrature, dtype=dtype)
+        extra = potentials.effective if self.external is None else potentials.effective + self.external
+        return CuspFactoredHamiltonian(self.grid, self.factor, extra_potential=extra, quadrature=self.quadrature,
+                                       dtype=dtype)
 
     #: A float-filtered full diagonalisation switches to the float64 filter below this residual.
     FLOAT_FILTER_SWITCH_RESIDUAL = 1.0e-4
@@ -615,10 +620,16 @@ def solve_self_consistent(step: KohnShamStep, mixing: MixingConfig | None = None
 
 
 def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: int = 0,
-                         eigen: EigenConfig | None = None) -> dict:
-    """(``src/cdft/scf/noninteracting.py:118-330``) for the cusp-factorised path, ``ritz_stop=True``."""
+                         eigen: EigenConfig | None = None, external_potential: torch.Tensor | None = None) -> dict:
+    """(``src/cdft/scf/noninteracting.py:118-330``) for the cusp-factorised path, ``ritz_stop=True``.
+
+    ``external_potential`` adds a diagonal term to the operator (an external perturbation in the
+    form quadrature.effective_potential gives it). The result also holds the occupied orbitals and
+    their occupations (``"orbitals"``, ``"occupations"``), normalised in the measure.
+    """
     grid = geometry.grid
-    ham = CuspFactoredHamiltonian(grid, geometry.factor, quadrature=geometry.quadrature)
+    ham = CuspFactoredHamiltonian(grid, geometry.factor, extra_potential=external_potential,
+                                  quadrature=geometry.quadrature)
     n_states = max(1, int(-(-float(n_electrons) // 2.0)))
     generator = SeededStream(seed, grid.device)
     solver = ChebyshevFilteredSubspace(grid, eigen or EigenConfig(), ritz_stop=True)
@@ -632,4 +643,4 @@ def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: in
     external = band - kinetic
     return {"total": kinetic + external + ion_ion, "kinetic": kinetic, "eigenvalues": vals[2:],
             "iterations": result.n_iterations, "converged": result.converged, "applications": float(ham.apply_count),
-            "stop_reason": solver.stop_reason}
+            "stop_reason": solver.stop_reason, "orbitals": result.eigenvectors, "occupations": occ[0]}

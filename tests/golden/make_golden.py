@@ -83,6 +83,7 @@ def main() -> None:
     parser.add_argument("--with-65", action="store_true")
     parser.add_argument("--with-config3", action="store_true", help="H2 PBE at 81 x 81 x 91 (tens of minutes)")
     parser.add_argument("--with-scan", action="store_true", help="five members of the H2+ bond scan")
+    parser.add_argument("--with-adjoint", action="store_true", help="Hellmann-Feynman and nuclear-gradient references")
     args = parser.parse_args()
     arrays: dict[str, np.ndarray] = {}
     values: dict[str, object] = {}
@@ -231,6 +232,38 @@ def main() -> None:
     timed("h2_pbe_h04", lambda: solve_self_consistent(h2, numerics(0.4, (10.0, 10.0, 11.2), degree=16), derive_grid=False))
     if args.with_65:
         timed("he65_lda_linear", lambda: solve_self_consistent(scenario, numerics(0.25, (16.0, 16.0, 16.0), mixing=LINEAR), derive_grid=False))
+    if args.with_adjoint:
+        # Hellmann--Feynman gradient of the He 25^3 energy with respect to eight seeded Gaussians
+        # g_k = exp(-|r - c_k|^2 / (2 w_k^2)) (the seeding of adjoint.seeded_gaussians), from the
+        # reference's converged density through its own quadrature (effective_potential,
+        # quadrature.py:747-753): dE/d alpha_k = sum_grid dv_k * mass_weights * n / f^2.
+        rng = np.random.default_rng(2024)
+        centres = rng.uniform(-3.0, 3.0, size=(8, 3))
+        widths = rng.uniform(0.5, 1.5, size=8)
+        art = solve_self_consistent(scenario, num, derive_grid=False)
+        density = art.result.density.reshape(-1).to(torch.float64)
+        c = torch.tensor(centres, dtype=torch.float64)
+        w = torch.tensor(widths, dtype=torch.float64)
+
+        def gauss(points):
+            d2 = ((points[None, :, :] - c[:, None, :]) ** 2).sum(dim=-1)
+            return torch.exp(-d2 / (2.0 * w[:, None] ** 2))
+
+        g_node, g_grid = gauss(quad.points), gauss(grid.points())
+        rho = density / factor.weight
+        hf = [float((quad.effective_potential(g_node[k], g_grid[k]) * quad.mass_weights * rho).sum()) for k in range(8)]
+        values["he25_external_gradient"] = {"centres": centres.tolist(), "widths": widths.tolist(),
+                                            "hellmann_feynman": hf, "total": art.result.energies.total}
+        print("he25_external_gradient", hf, flush=True)
+        # H2+ (R = 2, h = 0.4): the bond-length derivative by central differences (1e-4 bohr)
+        energies = {}
+        for sign in (+1, -1):
+            art = solve_noninteracting(h2_plus(2.0 + sign * 1e-4), numerics(0.4, (10.0, 10.0, 12.0)),
+                                       derive_grid=False)
+            energies[sign] = art.result.energies.total
+        values["h2plus_R2_h04_bond_derivative"] = {"plus": energies[1], "minus": energies[-1],
+                                                   "derivative": (energies[1] - energies[-1]) / 2e-4}
+        print("h2plus bond derivative", values["h2plus_R2_h04_bond_derivative"], flush=True)
     if args.with_config3:
         # config 3: H2 (R = 1.4) PBE, box 16 x 16 x 18, h = 0.20 -> 81 x 81 x 91, degree 16, unanchored lattice
         timed("h2_pbe_h020", lambda: solve_self_consistent(h2, numerics(0.20, (16.0, 16.0, 18.0), degree=16),

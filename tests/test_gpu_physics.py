@@ -219,3 +219,18 @@ def test_interpolate_and_lift_many_fields(pkg, he25, cuda, nf):
     # and the oracle, for one field
     want = quad_o.interpolate(_np(fields[0]))
     np.testing.assert_allclose(_np(many_i[0]), want, rtol=0, atol=1e-12 * np.abs(want).max())
+
+
+SCAN_SAMPLES = tuple(0.8 + k * 5.2 / 47 for k in (0, 11, 23, 35, 47))
+
+
+@pytest.mark.parametrize("bond", SCAN_SAMPLES)
+def test_h2plus_scan_members(pkg, cuda, golden_values, bond):
+    """Config 4: members of the bare H2+ bond scan (box 12 x 12 x (R + 12), h = 0.25, unanchored)."""
+    ref = golden_values.get(f"h2plus_scan_R{bond:.4f}")
+    if ref is None:
+        pytest.skip("no scan fixture (make_golden.py --with-scan)")
+    system = oscf.h2_plus(bond, spacing=0.25, transverse=12.0)
+    out = pkg.solve_noninteracting(_geometry(pkg, system, cuda), n_electrons=1.0)
+    assert abs(out["total"] - ref["total"]) < 1e-11
+    assert out["iterations"] == ref["iterations"]

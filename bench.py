@@ -118,7 +118,7 @@ def _peaks():
 
 def _profile_traffic(kernel_tag: str):
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if present."""
-    path = ROOT / "profiles" / "stencil_filter_he65.txt"
+    path = ROOT / "profiles" / "slab_filter_he65.txt"
     if not path.exists():
         return None
     for line in path.read_text().splitlines():
@@ -184,7 +184,11 @@ def batched_filter_roofline(pkg, dev, grid, bham, m: int, precision, reps: int =
 
 
 def run_kernel_only(args) -> None:
-    """The fused Chebyshev step alone on a He grid (profiling entry: small, bounded)."""
+    """The fused Chebyshev step alone on a He grid (profiling entry: small, bounded).
+
+    With ``--batch B`` (B > 1) the step runs over B systems of 5 orbitals with their own potentials
+    (the bare potential, repeated), as in the batched solve.
+    """
     import torch
 
     import __graft_entry__
@@ -195,14 +199,23 @@ def run_kernel_only(args) -> None:
     grid = pkg.UniformGrid.box((16.0, 16.0, 16.0), spacing, (0.0, 0.0, 0.0), device=dev)
     geometry = pkg.build_cusp_geometry(grid, (2.0,), ((0.0, 0.0, 0.0),))
     precision = torch.float32 if args.form == "mixed" else torch.float64
-    ham = pkg.CuspFactoredHamiltonian(grid, geometry.factor, quadrature=geometry.quadrature, dtype=precision)
-    per_launch_s, algorithmic = filter_step_roofline(pkg, dev, grid, ham, args.orbitals, precision, reps=args.steps)
+    batch = args.batch or 1
+    if batch > 1:
+        bare = geometry.quadrature.bare_operator_terms()[0]
+        bham = pkg.batch.BatchedHamiltonian(grid, geometry.factor, geometry.quadrature,
+                                            bare[None, :].repeat(batch, 1).contiguous(), dtype=precision)
+        per_launch_s, algorithmic = batched_filter_roofline(pkg, dev, grid, bham, args.orbitals, precision,
+                                                            reps=args.steps)
+    else:
+        ham = pkg.CuspFactoredHamiltonian(grid, geometry.factor, quadrature=geometry.quadrature, dtype=precision)
+        per_launch_s, algorithmic = filter_step_roofline(pkg, dev, grid, ham, args.orbitals, precision,
+                                                         reps=args.steps)
     peak, kind = _peaks()
     achieved = algorithmic / per_launch_s / 1e9
-    print(json.dumps({"kernel": "stencil_kernel (one Chebyshev step)", "grid": grid.shape, "orbitals": args.orbitals,
-                      "form": args.form, "us_per_launch": per_launch_s * 1e6, "algorithmic_bytes": algorithmic,
-                      "achieved_gbs": achieved, "peak_gbs": peak, "peak_kind": kind, "frac": achieved / peak}),
-          flush=True)
+    print(json.dumps({"kernel": "slab_filter_kernel (one Chebyshev step)", "grid": grid.shape, "systems": batch,
+                      "orbitals": args.orbitals, "form": args.form, "us_per_launch": per_launch_s * 1e6,
+                      "algorithmic_bytes": algorithmic, "achieved_gbs": achieved, "peak_gbs": peak,
+                      "peak_kind": kind, "frac": achieved / peak}), flush=True)
 
 
 def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str]:
@@ -424,8 +437,8 @@ def main() -> None:
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_in, "d2h_bytes_per_step": bytes_out},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": _profile_traffic(tag),
-                     "kernel": f"stencil_kernel<{tag}> (one Chebyshev step, {batch} systems x 5 orbitals)",
+                     "traffic": _profile_traffic(f"{tag},batch={batch}"),
+                     "kernel": f"slab_filter_kernel<{tag}> (one Chebyshev step, {batch} systems x 5 orbitals)",
                      "algorithmic_bytes_per_launch": algorithmic, "us_per_launch": per_launch_s * 1e6,
                      "peak_kind": peak_kind},
         "clocks": clocks,

@@ -49,6 +49,8 @@ def _args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--kernel-only", action="store_true",
                    help="time only the fused Chebyshev step on a He grid of --edge points (for profiling)")
+    p.add_argument("--breakdown", action="store_true",
+                   help="device time per kernel of one solve (torch.profiler, no replay) instead of the bench line")
     p.add_argument("--edge", type=int, default=65)
     p.add_argument("--orbitals", type=int, default=5)
     return p.parse_args()
@@ -282,6 +284,25 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def _breakdown(solve, n0) -> None:
+    """Print the device time of every kernel of one solve (torch.profiler's CUDA activity)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    t = time.perf_counter()
+    solve(n0)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t
+    with profile(activities=[ProfilerActivity.CPU, ProfilerActivity.CUDA]) as prof:
+        solve(n0)
+        torch.cuda.synchronize()
+    rows = [k for k in prof.key_averages() if k.self_device_time_total > 0]
+    busy = sum(k.self_device_time_total for k in rows) / 1e3
+    print(f"wall {wall * 1e3:.0f} ms per step, GPU busy {busy:.1f} ms")
+    for k in sorted(rows, key=lambda r: -r.self_device_time_total)[:30]:
+        print(f"{k.self_device_time_total / 1e3:9.2f} ms  {k.count:7d}  {k.key[:110]}")
+
+
 def replica_seeds(rank: int, batch: int) -> list[int]:
     """Seeds of the independent systems one replica solves: disjoint across ranks."""
     return [rank * batch + k for k in range(batch)]
@@ -363,6 +384,9 @@ def main() -> None:
     for _ in range(max(0, args.warmup)):
         solve(n0)
     torch.cuda.synchronize()
+    if args.breakdown:
+        _breakdown(solve, n0)
+        return
 
     # --- device-timed steps, inputs resident in HBM ---
     sampler = ClockSampler(local)

@@ -28,6 +28,7 @@ from . import _lib
 from ._lib import F32, F64, call, ptr, stream_handle
 from .eigen import BOUND_REUSE_RITZ_FRACTION, EigenConfig, chebyshev_coefficients, filter_workspace
 from .geometry import CuspGeometry, gradient, row_sums
+from .grid import UniformGrid
 from .operators import apply_workspace, cast, measure_cross, rowwise_inner
 from .poisson import CoulombCutoffPoisson
 from .rng import SeededStream
@@ -133,6 +134,16 @@ class _RitzBuffers:
 _RB = _RitzBuffers()
 
 
+def _row_inner(a: torch.Tensor, b: torch.Tensor, q: torch.Tensor) -> torch.Tensor:
+    """``sum_p q a b`` per row of ``(B, k, N)`` blocks; ``q`` shared ``(N,)`` or per system ``(B, N)``."""
+    bsz, k, n = a.shape
+    if q.dim() == 1:
+        return rowwise_inner(a.reshape(bsz * k, n), b.reshape(bsz * k, n), q).reshape(bsz, k)
+    if k == 1:
+        return measure_cross(a, b, q, bsz).reshape(bsz, 1)
+    return measure_cross(a, b, q, bsz).diagonal(dim1=1, dim2=2).contiguous()
+
+
 def batched_rayleigh_ritz(h: BatchedHamiltonian, block: torch.Tensor):
     """Rayleigh--Ritz for every system (``src/cdft/eigen/rayleigh_ritz.py:51-115``), one call per step.
 
@@ -162,7 +173,7 @@ def batched_rayleigh_ritz(h: BatchedHamiltonian, block: torch.Tensor):
     evals = rb.evals.clone()
     res = torch.empty_like(flat)
     call("cdftb_block_residual_f64", ptr(rot_applied), ptr(vectors), ptr(evals), ptr(res), m, n, b, m * n, stream)
-    norms = rowwise_inner(res.reshape(b * m, n), res.reshape(b * m, n), q).reshape(b, m).clamp_min(0.0).sqrt()
+    norms = _row_inner(res, res, q).clamp_min(0.0).sqrt()
     return evals, vectors, norms, orth, rb.info.clone()
 
 
@@ -173,6 +184,10 @@ def batched_lanczos(h: BatchedHamiltonian, starts: torch.Tensor, steps: int, saf
     dev = starts.device
     stream = stream_handle(dev)
     v = starts.to(torch.float64).clone().contiguous()
+
+    def rowwise_inner(x, y, q):
+        return _row_inner(x.reshape(b, 1, n), y.reshape(b, 1, n), q).reshape(b)
+
     nrm = rowwise_inner(v, v, q).clamp_min(0.0).contiguous()
     call("cdftb_lanczos_update_f64", 2, ptr(v), None, None, ptr(nrm), None, n, b, stream)
     v_prev = torch.zeros_like(v)
@@ -227,6 +242,13 @@ class _EigenState:
     iterations: int = 0
     stop_reason: str = "iteration limit"
     float_filter: bool = False
+    stable: int = 0
+
+
+def _stable(state, drift: float, tol: float) -> bool:
+    """Count consecutive iterations whose Ritz drift is below ``tol``; true at the second."""
+    state.stable = state.stable + 1 if drift < tol else 0
+    return state.stable >= 2
 
 
 def _fraction(value, low, high):
@@ -236,8 +258,11 @@ def _fraction(value, low, high):
 
 def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_states: int, config: EigenConfig,
                    initial: torch.Tensor | None, streams: list[SeededStream], bounds: list, max_iterations: int,
-                   switch_residual: float | None):
-    """CheFSI for every system of ``h`` (``src/cdft/eigen/chefsi.py:442-585``, ``ritz_stop=False``).
+                   switch_residual: float | None, ritz_stop: bool = False):
+    """CheFSI for every system of ``h`` (``src/cdft/eigen/chefsi.py:442-585``).
+
+    ``ritz_stop`` adds the weak-form stop of the bare-nucleus path: Ritz values stable (drift below
+    a tenth of ``cross_check_tol``) on two iterations in a row.
 
     ``bounds[b]`` is ``None`` (run Lanczos) or ``(lower, upper, shift)``. Returns per-system
     eigenvalues ``(B, n_states)``, eigenvectors ``(B, n_states, N)``, residuals ``(B, n_states)``,
@@ -345,6 +370,10 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
             if host[0, j] < config.residual_tol:
                 st.converged = True
                 st.stop_reason = "residual below residual_tol"
+                done.append(s)
+            elif ritz_stop and _stable(st, host[1, j], 0.1 * config.cross_check_tol):
+                st.converged = True
+                st.stop_reason = "Ritz values stable on the weak-form path"
                 done.append(s)
             else:
                 still.append(s)
@@ -706,3 +735,178 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
                           scf_iterations=[st.iterations for st in systems],
                           converged=[st.converged and final_converged[s] for s, st in enumerate(systems)],
                           applications=float(apps), density=n_out, measurements=measurements)
+
+
+# ------------------------------------------------------------------------------------------------
+# Systems on their own grids in one launch (e.g. a bond-length scan, whose boxes grow with R)
+
+
+class EmbeddedStream:
+    """A system's seeded draws in its own shape, embedded in the common box (zeros elsewhere)."""
+
+    def __init__(self, stream: SeededStream, embed) -> None:
+        self.stream = stream
+        self.embed = embed
+        self.n = None
+
+    def randn(self, shape):
+        size = (shape,) if isinstance(shape, int) else tuple(shape)
+        own = self.stream.randn((*size[:-1], self.n))
+        return self.embed(own)
+
+
+class MultiGeometryHamiltonian:
+    """``A`` on B systems with their own grids (same spacing and order), blocks ``(B, k, N)``.
+
+    Every system is embedded at the low corner of a common box ``max(shape_s)``: its face weights,
+    h^3/omega, bare potential and measure are copied in, and are zero outside it. Zero h^3/omega and
+    potential keep every point outside a system at zero through the apply and the filter, zero face
+    weights couple nothing across its boundary (its own Dirichlet zeros lie there), and a zero measure
+    leaves the Rayleigh--Ritz products those of the system alone. The kernels read the per-system
+    geometry through ``cdftb_operator.per_system_geometry`` (one launch for all systems).
+    """
+
+    def __init__(self, geometries, dtype=torch.float64, potentials=None) -> None:
+        if potentials is None:
+            spacings = {round(float(g.grid.spacing), 14) for g in geometries}
+            if len(spacings) != 1 or any(g.grid.fd_order != 8 for g in geometries):
+                raise ValueError("the systems must share the grid spacing and the order-8 stencil")
+            self.geometries = list(geometries)
+            self.shapes = [tuple(g.grid.shape) for g in geometries]
+            common = tuple(max(s[d] for s in self.shapes) for d in range(3))
+            first = geometries[0].grid
+            self.grid = UniformGrid(common, first.spacing, (0.0, 0.0, 0.0), device=first.device, fd_order=8)
+            b = len(geometries)
+            n = self.grid.n_points
+            nx, ny, nz = common
+            f = dict(dtype=torch.float64, device=first.device)
+            self._w = [torch.zeros((b, nx + 8, ny, nz), **f), torch.zeros((b, nx, ny + 8, nz), **f),
+                       torch.zeros((b, nx, ny, nz + 8), **f)]
+            self._inv64 = torch.zeros((b, n), **f)
+            self.potentials = torch.zeros((b, n), **f)
+            self.q = torch.zeros((b, n), **f)
+            for s, g in enumerate(geometries):
+                sx, sy, sz = self.shapes[s]
+                faces = g.factor.face_weights(8)
+                self._w[0][s, :sx + 8, :sy, :sz] = faces[0]
+                self._w[1][s, :sx, :sy + 8, :sz] = faces[1]
+                self._w[2][s, :sx, :sy, :sz + 8] = faces[2]
+                pot, inv, measure = g.quadrature.bare_operator_terms()
+                self.embed_into(self._inv64[s], s, inv)
+                self.embed_into(self.potentials[s], s, pot)
+                self.embed_into(self.q[s], s, measure.quadrature)
+        else:
+            raise ValueError("use subset() to select systems")
+        self.dtype = dtype
+        self._cast()
+        self.applications = 0
+
+    def _cast(self) -> None:
+        if self.dtype == torch.float64:
+            self._faces = tuple(w.contiguous() for w in self._w)
+            self._inv = self._inv64.contiguous()
+            self._pot = self.potentials.contiguous()
+        else:
+            self._faces = tuple(cast(w.contiguous(), self.dtype) for w in self._w)
+            self._inv = cast(self._inv64.contiguous(), self.dtype)
+            self._pot = cast(self.potentials.contiguous(), self.dtype)
+
+    def as_dtype(self, dtype) -> "MultiGeometryHamiltonian":
+        other = MultiGeometryHamiltonian.__new__(MultiGeometryHamiltonian)
+        other.__dict__.update(self.__dict__)
+        other.dtype = dtype
+        other._cast()
+        other.applications = 0
+        return other
+
+    # -- embedding of fields between a system's grid and the common box
+    def embed_into(self, dst: torch.Tensor, s: int, field: torch.Tensor) -> None:
+        sx, sy, sz = self.shapes[s]
+        dst.reshape(self.grid.shape)[:sx, :sy, :sz] = field.reshape(sx, sy, sz)
+
+    def embed(self, s: int, field: torch.Tensor) -> torch.Tensor:
+        """``(..., N_s)`` on system s's grid -> ``(..., N)`` in the common box."""
+        lead = field.shape[:-1]
+        out = torch.zeros((*lead, self.grid.n_points), dtype=field.dtype, device=field.device)
+        sx, sy, sz = self.shapes[s]
+        out.reshape(*lead, *self.grid.shape)[..., :sx, :sy, :sz] = field.reshape(*lead, sx, sy, sz)
+        return out
+
+    def extract(self, s: int, field: torch.Tensor) -> torch.Tensor:
+        """``(..., N)`` in the common box -> ``(..., N_s)`` on system s's grid."""
+        lead = field.shape[:-1]
+        sx, sy, sz = self.shapes[s]
+        return field.reshape(*lead, *self.grid.shape)[..., :sx, :sy, :sz].reshape(*lead, sx * sy * sz).contiguous()
+
+    @property
+    def batch(self) -> int:
+        return self.potentials.shape[0]
+
+    def _op(self, k: int) -> _lib.Operator:
+        op = _lib.Operator()
+        op.nx, op.ny, op.nz = self.grid.shape
+        op.accuracy = 8
+        op.spacing = self.grid.spacing
+        op.dtype = F64 if self.dtype == torch.float64 else F32
+        op.face_weights = (ctypes.c_void_p * 3)(*(w.data_ptr() for w in self._faces))
+        op.inverse_weight = self._inv.data_ptr()
+        op.potential = self._pot.data_ptr()
+        op.potential_stride = self.grid.n_points
+        op.orbitals_per_group = int(k)
+        op.quadrature = self.q.data_ptr()
+        op.per_system_geometry = 1
+        return op
+
+    apply = BatchedHamiltonian.apply
+    filter = BatchedHamiltonian.filter
+
+    def subset(self, index: list[int]) -> "MultiGeometryHamiltonian":
+        sub = MultiGeometryHamiltonian.__new__(MultiGeometryHamiltonian)
+        sub.__dict__.update(self.__dict__)
+        idx = torch.tensor(index, dtype=torch.long, device=self.potentials.device)
+        sub._w = [w.index_select(0, idx).contiguous() for w in self._w]
+        sub._inv64 = self._inv64.index_select(0, idx).contiguous()
+        sub.potentials = self.potentials.index_select(0, idx).contiguous()
+        sub.q = self.q.index_select(0, idx).contiguous()
+        sub.shapes = [self.shapes[i] for i in index]
+        sub.geometries = [self.geometries[i] for i in index]
+        sub._cast()
+        sub.applications = 0
+        return sub
+
+
+def solve_noninteracting_batch(geometries, n_electrons: float, *, seeds=None, eigen: EigenConfig | None = None,
+                               filter_precision: torch.dtype = torch.float64) -> list[dict]:
+    """``solve_noninteracting`` (``src/cdft/scf/noninteracting.py:118-330``) for B systems at once.
+
+    The systems may have different grids (same spacing): one filter launch, one Rayleigh--Ritz
+    step and one Lanczos enclosure per CheFSI iteration serve all of them. Each system draws its
+    seeded random block in its own shape, as the single-system solve does. Returns one result dict
+    per system (``total``, ``eigenvalues``, ``iterations``, ``converged``, ``stop_reason``).
+    """
+    from .scf import aufbau_occupations, nuclear_repulsion
+
+    config = eigen or EigenConfig()
+    b = len(geometries)
+    seeds = list(seeds) if seeds is not None else [0] * b
+    h = MultiGeometryHamiltonian(geometries)
+    h32 = h.as_dtype(torch.float32) if filter_precision == torch.float32 else None
+    n_states = max(1, int(-(-float(n_electrons) // 2.0)))
+    dev = h.grid.device
+    streams = []
+    for s in range(b):
+        stream = EmbeddedStream(SeededStream(seeds[s], dev), lambda x, s=s: h.embed(s, x))
+        stream.n = geometries[s].grid.n_points
+        streams.append(stream)
+    evals, vectors, residual, states = batched_chefsi(
+        h, h32, n_states, config, None, streams, [None] * b, config.max_iterations,
+        BatchedKohnShamStep.FLOAT_FILTER_SWITCH_RESIDUAL if h32 is not None else None, ritz_stop=True)
+    occ = aufbau_occupations(n_states, float(n_electrons))[0]
+    values = evals.cpu().numpy()
+    out = []
+    for s, g in enumerate(geometries):
+        band = float((occ * values[s]).sum())
+        out.append({"total": band + nuclear_repulsion(g.charges, g.positions), "eigenvalues": values[s].tolist(),
+                    "iterations": states[s].iterations, "converged": states[s].converged,
+                    "stop_reason": states[s].stop_reason, "orbitals": h.extract(s, vectors[s])})
+    return out

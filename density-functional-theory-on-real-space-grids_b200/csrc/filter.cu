@@ -153,6 +153,8 @@ struct FilterArgs {
     int shared_potential;  // one potential for every orbital
     unsigned token;        // this launch's abort token (never 0)
     int apply_only;        // out = A phi (no recurrence; coef unused)
+    int per_system_geometry;  // face weights and h^3/omega per orbital group (systems on their own grids)
+    int lanes_per_group;      // > 0: lanes aligned to orbital groups (lane l holds group l / lanes_per_group)
     int kinetic_only;      // with apply_only: out = 0.5 (h^3/omega) div phi (no potential)
     const double* coef;
     int degree;
@@ -250,6 +252,23 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// The orbital held by half h of lane l, or -1 for an empty half. Lanes run over the orbitals in order
+// (lane l: orbitals ORBITALS l + h) or, aligned to orbital groups, over each group separately, so that
+// no lane mixes two groups (lane l: group l / lpg, orbitals ORBITALS (l mod lpg) + h of that group).
+template <int ORBITALS>
+__host__ __device__ __forceinline__ int64_t lane_orbital(int64_t l, int h, int64_t batch, int opg, int lpg) {
+    int64_t o;
+    if (lpg > 0) {
+        const int64_t g = l / lpg;
+        const int64_t j = ORBITALS * (l - g * lpg) + h;
+        if (j >= opg) return -1;
+        o = g * opg + j;
+    } else {
+        o = ORBITALS * l + h;
+    }
+    return o < batch ? o : -1;
+}
+
 template <typename Lane, int TZ>
 __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
     slab_filter_kernel(const __grid_constant__ FilterMaps maps, const FilterArgs a) {
@@ -275,10 +294,15 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
     const int npl = xe - xa + 1 + 2 * HALO;  // planes marched
     const bool has_prev = a.has_prev != 0;
 
-    const int64_t o0 = int64_t(lane) * Lane::ORBITALS;
-    const int64_t o1 = (Lane::ORBITALS == 2) ? min(o0 + 1, a.batch - 1) : o0;
+    // the lane's orbitals (an empty second half borrows the first's group for its lookups)
+    const int64_t o0 = lane_orbital<Lane::ORBITALS>(lane, 0, a.batch, a.orb_per_group, a.lanes_per_group);
+    const int64_t o1s = (Lane::ORBITALS == 2)
+                            ? lane_orbital<Lane::ORBITALS>(lane, 1, a.batch, a.orb_per_group, a.lanes_per_group)
+                            : -1;
+    const int64_t o1 = o1s >= 0 ? o1s : o0;
     const int g0 = a.shared_potential ? 0 : static_cast<int>(o0 / a.orb_per_group);
     const int g1 = a.shared_potential ? 0 : static_cast<int>(o1 / a.orb_per_group);
+    const int gg = a.per_system_geometry ? static_cast<int>(o0 / a.orb_per_group) : 0;
 
     if (t == 0) {
         for (int s = 0; s < R; ++s) {
@@ -313,10 +337,10 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
             mbar_expect_tx(full, tx);
             tma_load_4d(slot + SH::O_PHI, &maps.phi, z0 - 8, y0 - HALO, q, lane, full);
             if (has_prev) tma_load_4d(slot + SH::O_PREV, &maps.prev, z0, y0, q - HALO, lane, full);
-            tma_load_3d(slot + SH::O_W0, &maps.w0, z0, y0, q, full);  // x face q-4 is stored at index q
-            tma_load_3d(slot + SH::O_W1, &maps.w1, z0, y0, q, full);  // y faces y0-4 .. y0+10
-            tma_load_3d(slot + SH::O_W2, &maps.w2, z0, y0, q, full);  // z faces z0-4 .. z0+TZ+3
-            tma_load_3d(slot + SH::O_INV, &maps.inv, z0, y0, q - HALO, full);
+            tma_load_4d(slot + SH::O_W0, &maps.w0, z0, y0, q, gg, full);  // x face q-4 is stored at index q
+            tma_load_4d(slot + SH::O_W1, &maps.w1, z0, y0, q, gg, full);  // y faces y0-4 .. y0+10
+            tma_load_4d(slot + SH::O_W2, &maps.w2, z0, y0, q, gg, full);  // z faces z0-4 .. z0+TZ+3
+            tma_load_4d(slot + SH::O_INV, &maps.inv, z0, y0, q - HALO, gg, full);
             tma_load_4d(slot + SH::O_POT0, &maps.pot, z0, y0, q - HALO, g0, full);
             tma_load_4d(slot + SH::O_POT1, &maps.pot, z0, y0, q - HALO, g1, full);
             issued = n + 1;
@@ -518,9 +542,8 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
                 if (a.final_out) {
                     if (own_in) {
                         if constexpr (Lane::ORBITALS == 2) {
-                            store_as<float>(a.out, a.out_dtype, o0 * (plane_n * nx) + pt, res.x);
-                            if (o0 + 1 < a.batch)
-                                store_as<float>(a.out, a.out_dtype, (o0 + 1) * (plane_n * nx) + pt, res.y);
+                            if (o0 >= 0) store_as<float>(a.out, a.out_dtype, o0 * (plane_n * nx) + pt, res.x);
+                            if (o1s >= 0) store_as<float>(a.out, a.out_dtype, o1s * (plane_n * nx) + pt, res.y);
                         } else {
                             store_as<double>(a.out, a.out_dtype, o0 * (plane_n * nx) + pt, res);
                         }
@@ -543,7 +566,7 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
 // Internal layout from a caller block: lanes of (nx, ny, nzp), padding and missing orbitals zero.
 template <typename Lane>
 __global__ void pack_lanes_kernel(const void* __restrict__ in, int in_dtype, int64_t batch, int nx, int ny, int nz,
-                                  int nzp, int64_t lanes, typename Lane::E* __restrict__ out) {
+                                  int nzp, int64_t lanes, int opg, int lpg, typename Lane::E* __restrict__ out) {
     using E = typename Lane::E;
     const int64_t per_lane = int64_t(nx) * ny * nzp;
     const int64_t total = lanes * per_lane;
@@ -558,9 +581,10 @@ __global__ void pack_lanes_kernel(const void* __restrict__ in, int in_dtype, int
         if (zp < nz) {
             const int64_t pt = xy * nz + zp;
             if constexpr (Lane::ORBITALS == 2) {
-                const int64_t o = 2 * l;
-                v.x = load_as<float>(in, in_dtype, o * n_points + pt);
-                v.y = (o + 1 < batch) ? load_as<float>(in, in_dtype, (o + 1) * n_points + pt) : 0.f;
+                const int64_t a0 = lane_orbital<2>(l, 0, batch, opg, lpg);
+                const int64_t a1 = lane_orbital<2>(l, 1, batch, opg, lpg);
+                v.x = a0 >= 0 ? load_as<float>(in, in_dtype, a0 * n_points + pt) : 0.f;
+                v.y = a1 >= 0 ? load_as<float>(in, in_dtype, a1 * n_points + pt) : 0.f;
             } else {
                 v = load_as<double>(in, in_dtype, l * n_points + pt);
             }
@@ -617,7 +641,16 @@ int encode_map(CUtensorMap* map, CUtensorMapDataType type, int esize, int rank, 
     return r == CUDA_SUCCESS ? CDFTB_OK : CDFTB_ERR_ARGUMENT;
 }
 
-int64_t lanes_of(const cdftb_operator* op, int64_t batch) { return op->dtype == CDFTB_F32 ? (batch + 1) / 2 : batch; }
+// Lanes per orbital group when lanes are aligned to groups (float32 lanes with per-system geometry), else 0.
+int aligned_lanes_per_group(const cdftb_operator* op) {
+    return (op->per_system_geometry && op->dtype == CDFTB_F32) ? (op->orbitals_per_group + 1) / 2 : 0;
+}
+
+int64_t lanes_of(const cdftb_operator* op, int64_t batch) {
+    if (op->dtype != CDFTB_F32) return batch;
+    const int lpg = aligned_lanes_per_group(op);
+    return lpg > 0 ? ceil_div(batch, op->orbitals_per_group) * lpg : (batch + 1) / 2;
+}
 
 int padded_z(int nz) { return nz + (nz & 1); }
 
@@ -625,6 +658,11 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 int64_t systems_of(const cdftb_operator* op, int64_t batch) {
     return op->potential_stride == 0 ? 1 : ceil_div(batch, op->orbitals_per_group);
+}
+
+// Geometry copies: one, or one per orbital group.
+int64_t geometry_systems(const cdftb_operator* op, int64_t batch) {
+    return op->per_system_geometry ? ceil_div(batch, op->orbitals_per_group) : 1;
 }
 
 // Element counts of the padded geometry copies: w0, w1, w2, inv, potentials.
@@ -640,10 +678,11 @@ GeoPack geo_pack(const cdftb_operator* op, int64_t batch) {
     g.nzg = static_cast<int>(round_up(op->nz, per16));
     g.nz8g = static_cast<int>(round_up(op->nz + 8, per16));
     const int64_t nx = op->nx, ny = op->ny;
-    g.n_w0 = round_up((nx + 8) * ny * g.nzg, per16);
-    g.n_w1 = round_up(nx * (ny + 8) * g.nzg, per16);
-    g.n_w2 = round_up(nx * ny * g.nz8g, per16);
-    g.n_inv = round_up(nx * ny * g.nzg, per16);
+    const int64_t ng = geometry_systems(op, batch);
+    g.n_w0 = round_up(ng * (nx + 8) * ny * g.nzg, per16);
+    g.n_w1 = round_up(ng * nx * (ny + 8) * g.nzg, per16);
+    g.n_w2 = round_up(ng * nx * ny * g.nz8g, per16);
+    g.n_inv = round_up(ng * nx * ny * g.nzg, per16);
     g.n_pot = systems_of(op, batch) * nx * ny * g.nzg;
     return g;
 }
@@ -736,11 +775,12 @@ int prepare_geometry(const cdftb_operator* op, int64_t batch, void* geo_base, in
     S* invp = w2p + gp.n_w2;
     S* potp = invp + gp.n_inv;
     const int64_t nsys = systems_of(op, batch);
+    const int64_t ng = geometry_systems(op, batch);  // per-system arrays follow each other in memory
     int st;
-    if ((st = pad_rows<S>(op->face_weights[0], int64_t(nx + 8) * ny, nz, gp.nzg, w0p, stream)) != CDFTB_OK) return st;
-    if ((st = pad_rows<S>(op->face_weights[1], int64_t(nx) * (ny + 8), nz, gp.nzg, w1p, stream)) != CDFTB_OK) return st;
-    if ((st = pad_rows<S>(op->face_weights[2], int64_t(nx) * ny, nz + 8, gp.nz8g, w2p, stream)) != CDFTB_OK) return st;
-    if ((st = pad_rows<S>(op->inverse_weight, int64_t(nx) * ny, nz, gp.nzg, invp, stream)) != CDFTB_OK) return st;
+    if ((st = pad_rows<S>(op->face_weights[0], ng * (nx + 8) * ny, nz, gp.nzg, w0p, stream)) != CDFTB_OK) return st;
+    if ((st = pad_rows<S>(op->face_weights[1], ng * nx * (ny + 8), nz, gp.nzg, w1p, stream)) != CDFTB_OK) return st;
+    if ((st = pad_rows<S>(op->face_weights[2], ng * nx * ny, nz + 8, gp.nz8g, w2p, stream)) != CDFTB_OK) return st;
+    if ((st = pad_rows<S>(op->inverse_weight, ng * nx * ny, nz, gp.nzg, invp, stream)) != CDFTB_OK) return st;
     if (kinetic_only || !op->potential) {
         if ((st = check(cudaMemsetAsync(potp, 0, gp.n_pot * sizeof(S), stream))) != CDFTB_OK) return st;
     } else if (op->potential_stride == 0 || op->potential_stride == int64_t(nx) * ny * nz) {
@@ -756,28 +796,29 @@ int prepare_geometry(const cdftb_operator* op, int64_t batch, void* geo_base, in
     }
     const CUtensorMapDataType gt = Lane::GEO_TYPE;
     const int sb = sizeof(S);
-    const unsigned tile_box[3] = {unsigned(tz), unsigned(TY), 1};
-    const int64_t d_w0[3] = {gp.nzg, ny, nx + 8};
-    const int64_t d_w1[3] = {gp.nzg, ny + 8, nx};
-    const unsigned b_w1[3] = {unsigned(tz), unsigned(TY + 7), 1};
-    const int64_t d_w2[3] = {gp.nz8g, ny, nx};
-    const unsigned b_w2[3] = {unsigned(tz + 8), unsigned(TY), 1};
-    const int64_t d_inv[3] = {gp.nzg, ny, nx};
+    const unsigned tile_box[4] = {unsigned(tz), unsigned(TY), 1, 1};
+    const int64_t d_w0[4] = {gp.nzg, ny, nx + 8, ng};
+    const int64_t d_w1[4] = {gp.nzg, ny + 8, nx, ng};
+    const unsigned b_w1[4] = {unsigned(tz), unsigned(TY + 7), 1, 1};
+    const int64_t d_w2[4] = {gp.nz8g, ny, nx, ng};
+    const unsigned b_w2[4] = {unsigned(tz + 8), unsigned(TY), 1, 1};
+    const int64_t d_inv[4] = {gp.nzg, ny, nx, ng};
     const int64_t d_pot[4] = {gp.nzg, ny, nx, nsys};
     const unsigned b_pot[4] = {unsigned(tz), unsigned(TY), 1, 1};
-    if ((st = encode_map(&maps->w0, gt, sb, 3, w0p, d_w0, tile_box)) != CDFTB_OK) return st;
-    if ((st = encode_map(&maps->w1, gt, sb, 3, w1p, d_w1, b_w1)) != CDFTB_OK) return st;
-    if ((st = encode_map(&maps->w2, gt, sb, 3, w2p, d_w2, b_w2)) != CDFTB_OK) return st;
-    if ((st = encode_map(&maps->inv, gt, sb, 3, invp, d_inv, tile_box)) != CDFTB_OK) return st;
+    if ((st = encode_map(&maps->w0, gt, sb, 4, w0p, d_w0, tile_box)) != CDFTB_OK) return st;
+    if ((st = encode_map(&maps->w1, gt, sb, 4, w1p, d_w1, b_w1)) != CDFTB_OK) return st;
+    if ((st = encode_map(&maps->w2, gt, sb, 4, w2p, d_w2, b_w2)) != CDFTB_OK) return st;
+    if ((st = encode_map(&maps->inv, gt, sb, 4, invp, d_inv, tile_box)) != CDFTB_OK) return st;
     return encode_map(&maps->pot, gt, sb, 4, potp, d_pot, b_pot);
 }
 
 template <typename Lane>
-int pack_block(const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz, int nzp, int64_t lanes,
-               void* dst, cudaStream_t stream) {
+int pack_block(const cdftb_operator* op, const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz,
+               int nzp, int64_t lanes, void* dst, cudaStream_t stream) {
     const int64_t total = lanes * int64_t(nx) * ny * nzp;
     const unsigned blocks = static_cast<unsigned>(std::min<int64_t>(ceil_div(total, 256), 148 * 16));
     pack_lanes_kernel<Lane><<<blocks, 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
+                                                        op->orbitals_per_group, aligned_lanes_per_group(op),
                                                         static_cast<typename Lane::E*>(dst));
     return check_launch();
 }
@@ -800,6 +841,8 @@ FilterArgs base_args(const cdftb_operator* op, int64_t batch) {
     a.batch = batch;
     a.orb_per_group = op->orbitals_per_group;
     a.shared_potential = op->potential_stride == 0;
+    a.per_system_geometry = op->per_system_geometry != 0;
+    a.lanes_per_group = aligned_lanes_per_group(op);
     const StaggeredTaps taps = staggered_taps(8);
     const double scale = 1.0 / op->spacing;  // taps c_k * (1/h), divergence.py:112, 121
     for (int j = 0; j < 8; ++j) a.taps[j] = taps.c[j] * scale;
@@ -821,7 +864,7 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
     char* w = static_cast<char*>(work);
     void* buf[3] = {w, w + lanes * lane_bytes, w + 2 * lanes * lane_bytes};
     const int tz = choose_tz(nzp);
-    int st = pack_block<Lane>(block, in_dtype, batch, nx, ny, nz, nzp, lanes, buf[2], stream);
+    int st = pack_block<Lane>(op, block, in_dtype, batch, nx, ny, nz, nzp, lanes, buf[2], stream);
     if (st != CDFTB_OK) return st;
     FilterMaps geo_maps{};
     if ((st = prepare_geometry<Lane>(op, batch, w + 3 * lanes * lane_bytes, tz, false, &geo_maps, stream)) != CDFTB_OK)
@@ -861,7 +904,7 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
     const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
     char* w = static_cast<char*>(work);
     const int tz = choose_tz(nzp);
-    int st = pack_block<Lane>(phi, in_dtype, batch, nx, ny, nz, nzp, lanes, w, stream);
+    int st = pack_block<Lane>(op, phi, in_dtype, batch, nx, ny, nz, nzp, lanes, w, stream);
     if (st != CDFTB_OK) return st;
     FilterMaps m{};
     if ((st = prepare_geometry<Lane>(op, batch, w + lanes * lane_bytes, tz, kinetic_only != 0, &m, stream)) !=
@@ -942,6 +985,7 @@ extern "C" int cdftb_chebyshev_filter(const cdftb_operator* op, const void* bloc
     if (cdftb::slab_filter_applies(op))
         return cdftb::slab_chebyshev_filter(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree,
                                             cdftb::as_stream(stream));
+    if (op->per_system_geometry) return CDFTB_ERR_ARGUMENT;  // the generic stencil shares one geometry
     return cdftb::generic_chebyshev_filter(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree,
                                            stream);
 }
@@ -962,8 +1006,10 @@ extern "C" int cdftb_cusp_apply(const cdftb_operator* op, const void* phi, int i
                       (kinetic_only || (op->potential && op->orbitals_per_group > 0)) &&
                       (in_dtype == CDFTB_F64 || in_dtype == CDFTB_F32) &&
                       (out_dtype == CDFTB_F64 || out_dtype == CDFTB_F32);
-    if (!slab)
+    if (!slab) {
+        if (op->per_system_geometry) return CDFTB_ERR_ARGUMENT;  // the generic stencil shares one geometry
         return cdftb::generic_cusp_apply(op, phi, in_dtype, out, out_dtype, batch, kinetic_only, stream);
+    }
     cudaStream_t s = cdftb::as_stream(stream);
     if (op->dtype == CDFTB_F32)
         return cdftb::slab_apply<cdftb::LaneF2>(op, phi, in_dtype, out, out_dtype, work, batch, kinetic_only, s);

@@ -41,8 +41,9 @@ CrossShape cross_shape(int ma, int mb, int64_t n, int groups) {
 template <int TI, int TJ>
 __global__ void __launch_bounds__(RT) cross_partial_kernel(const double* __restrict__ a, int ma, int64_t sa,
                                                             const double* __restrict__ b, int mb, int64_t sb,
-                                                            const double* __restrict__ q, int64_t n, int tiles_j,
-                                                            int64_t chunk, int chunks, double* __restrict__ partial) {
+                                                            const double* __restrict__ q, int64_t q_stride, int64_t n,
+                                                            int tiles_j, int64_t chunk, int chunks,
+                                                            double* __restrict__ partial) {
     const int c = blockIdx.x;
     const int tile = blockIdx.y;
     const int g = blockIdx.z;
@@ -52,13 +53,14 @@ __global__ void __launch_bounds__(RT) cross_partial_kernel(const double* __restr
     const int64_t p1 = (p0 + chunk < n) ? p0 + chunk : n;
     const double* ag = a + g * sa;
     const double* bg = b + g * sb;
+    const double* qg = q ? q + g * q_stride : nullptr;
     double acc[TI][TJ];
 #pragma unroll
     for (int i = 0; i < TI; ++i)
 #pragma unroll
         for (int j = 0; j < TJ; ++j) acc[i][j] = 0.0;
     for (int64_t p = p0 + threadIdx.x; p < p1; p += RT) {
-        const double w = q ? q[p] : 1.0;
+        const double w = qg ? qg[p] : 1.0;
         double av[TI], bv[TJ];
 #pragma unroll
         for (int i = 0; i < TI; ++i) av[i] = (i0 + i < ma) ? ag[(i0 + i) * n + p] * w : 0.0;
@@ -123,26 +125,27 @@ extern "C" int64_t cdftb_measure_cross_scratch_bytes(int ma, int mb, int64_t n, 
     return static_cast<int64_t>(groups) * s.tiles_i * s.tiles_j * s.chunks * s.ti * s.tj * 8;
 }
 
-extern "C" int cdftb_measure_cross_f64(const double* a, int ma, int64_t group_stride_a, const double* b, int mb,
-                                       int64_t group_stride_b, const double* q, int64_t n, int groups, double* out,
-                                       void* scratch, int64_t scratch_bytes, cdftb_stream_t stream) {
+namespace cdftb {
+namespace {
+int launch_cross(const double* a, int ma, int64_t group_stride_a, const double* b, int mb, int64_t group_stride_b,
+                 const double* q, int64_t q_group_stride, int64_t n, int groups, double* out, void* scratch,
+                 int64_t scratch_bytes, cudaStream_t st) {
     if (!a || !b || !out || ma <= 0 || mb <= 0 || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
     CrossShape s = cross_shape(ma, mb, n, groups);
     const int64_t need = cdftb_measure_cross_scratch_bytes(ma, mb, n, groups);
     if (!scratch || scratch_bytes < need) return CDFTB_ERR_ARGUMENT;
-    cudaStream_t st = as_stream(stream);
     double* partial = static_cast<double*>(scratch);
     const int tiles = s.tiles_i * s.tiles_j;
     dim3 grid(s.chunks, tiles, groups);
     if (s.ti == 1)
-        cross_partial_kernel<1, 1><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, n, s.tiles_j,
-                                                        s.chunk, s.chunks, partial);
+        cross_partial_kernel<1, 1><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, q_group_stride,
+                                                        n, s.tiles_j, s.chunk, s.chunks, partial);
     else if (s.ti == 6)
-        cross_partial_kernel<6, 6><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, n, s.tiles_j,
-                                                        s.chunk, s.chunks, partial);
+        cross_partial_kernel<6, 6><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, q_group_stride,
+                                                        n, s.tiles_j, s.chunk, s.chunks, partial);
     else
-        cross_partial_kernel<4, 4><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, n, s.tiles_j,
-                                                        s.chunk, s.chunks, partial);
+        cross_partial_kernel<4, 4><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, q_group_stride,
+                                                        n, s.tiles_j, s.chunk, s.chunks, partial);
     int rc = check_launch();
     if (rc != CDFTB_OK) return rc;
     const int64_t total = static_cast<int64_t>(groups) * ma * mb;
@@ -150,6 +153,24 @@ extern "C" int cdftb_measure_cross_f64(const double* a, int ma, int64_t group_st
                                                                                          s.tiles_j, tiles, s.chunks,
                                                                                          groups, out);
     return check_launch();
+}
+}  // namespace
+}  // namespace cdftb
+
+extern "C" int cdftb_measure_cross_f64(const double* a, int ma, int64_t group_stride_a, const double* b, int mb,
+                                       int64_t group_stride_b, const double* q, int64_t n, int groups, double* out,
+                                       void* scratch, int64_t scratch_bytes, cdftb_stream_t stream) {
+    return launch_cross(a, ma, group_stride_a, b, mb, group_stride_b, q, 0, n, groups, out, scratch, scratch_bytes,
+                        as_stream(stream));
+}
+
+extern "C" int cdftb_measure_cross_grouped_f64(const double* a, int ma, int64_t group_stride_a, const double* b, int mb,
+                                               int64_t group_stride_b, const double* q, int64_t q_group_stride,
+                                               int64_t n, int groups, double* out, void* scratch,
+                                               int64_t scratch_bytes, cdftb_stream_t stream) {
+    if (!q || q_group_stride < 0) return CDFTB_ERR_ARGUMENT;
+    return launch_cross(a, ma, group_stride_a, b, mb, group_stride_b, q, q_group_stride, n, groups, out, scratch,
+                        scratch_bytes, as_stream(stream));
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -29,7 +29,10 @@ def apply_workspace(op, batch: int, device: torch.device) -> torch.Tensor:
 
 
 def measure_cross(a: torch.Tensor, b: torch.Tensor, q: torch.Tensor | None, groups: int = 1) -> torch.Tensor:
-    """``out[g] = (a[g] * q) @ b[g].T`` for ``groups`` stacked blocks (float64, deterministic)."""
+    """``out[g] = (a[g] * q) @ b[g].T`` for ``groups`` stacked blocks (float64, deterministic).
+
+    ``q`` is one measure ``(N,)`` for every group, or one per group ``(groups, N)``.
+    """
     n = a.shape[-1]
     a2 = a.reshape(groups, -1, n)
     b2 = b.reshape(groups, -1, n)
@@ -41,6 +44,13 @@ def measure_cross(a: torch.Tensor, b: torch.Tensor, q: torch.Tensor | None, grou
     out = torch.empty((groups, ma, mb), dtype=torch.float64, device=a.device)
     nbytes = _lib.library().cdftb_measure_cross_scratch_bytes(ma, mb, n, groups)
     scratch = _scratch(nbytes, a.device)
+    if q is not None and q.dim() == 2:
+        if q.shape != (groups, n):
+            raise ValueError(f"a per-group measure must be ({groups}, {n}), got {tuple(q.shape)}")
+        qc = q.contiguous()
+        call("cdftb_measure_cross_grouped_f64", ptr(a2), ma, a2.stride(0), ptr(b2), mb, b2.stride(0), ptr(qc),
+             qc.stride(0), n, groups, ptr(out), ptr(scratch), scratch.numel(), stream_handle(a.device))
+        return out
     call("cdftb_measure_cross_f64", ptr(a2), ma, a2.stride(0), ptr(b2), mb, b2.stride(0), ptr(q), n, groups, ptr(out),
          ptr(scratch), scratch.numel(), stream_handle(a.device))
     return out

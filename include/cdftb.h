@@ -46,6 +46,9 @@ unsigned long long cdftb_launch_count(void);
  * group, groups `potential_stride` elements apart; orbital b uses group b / orbitals_per_group).
  * `dtype` says whether the weight and potential arrays are double or float. The measure
  * `quadrature` (omega, N, always double) is used by the reductions.
+ * per_system_geometry = 1: face_weights[d] and inverse_weight hold one array per orbital group,
+ * back to back (systems on their own grids, embedded in a common box with zero weights, zero
+ * h^3/omega and zero potential outside each system); only the order-8 slab paths take it.
  */
 typedef struct cdftb_operator {
     int nx, ny, nz;
@@ -58,6 +61,7 @@ typedef struct cdftb_operator {
     int64_t potential_stride;
     int orbitals_per_group;
     const double* quadrature;
+    int per_system_geometry;
 } cdftb_operator;
 
 /* (a1) out = sum_d D_d^T [w_d D_d box], f64, batched.
@@ -108,6 +112,12 @@ int64_t cdftb_measure_cross_scratch_bytes(int ma, int mb, int64_t n, int groups)
 int cdftb_measure_cross_f64(const double* a, int ma, int64_t group_stride_a, const double* b, int mb,
                             int64_t group_stride_b, const double* q, int64_t n, int groups, double* out,
                             void* scratch, int64_t scratch_bytes, cdftb_stream_t stream);
+/* The same with one measure per group (q + g * q_group_stride): systems on their own grids in one
+ * call (src/cdft/eigen/measure.py:72-96 per system). */
+int cdftb_measure_cross_grouped_f64(const double* a, int ma, int64_t group_stride_a, const double* b, int mb,
+                                    int64_t group_stride_b, const double* q, int64_t q_group_stride, int64_t n,
+                                    int groups, double* out, void* scratch, int64_t scratch_bytes,
+                                    cdftb_stream_t stream);
 
 /* No reference counterpart: cdftb_measure_cross_f64 for callers that cannot allocate device
  * memory. Same arguments and results (bit-identical), but the partials go to a fixed device array

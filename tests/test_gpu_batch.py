@@ -49,3 +49,61 @@ def test_batch_mixed_precision(pkg, he25_geometry, golden_values):
         assert abs(e["total"] - ref["total"]) < 1e-8
         assert abs(ev[0] - ref["eigenvalues"][0]) < 1e-6
     assert out.measurements["filter_precision"] == "float32"
+
+
+# ------------------------------------------------------------------ systems on their own grids
+
+
+def _scan_geometry(pkg, cuda, bond, spacing=0.25, transverse=12.0):
+    system = oscf.h2_plus(bond, spacing=spacing, transverse=transverse)
+    grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=cuda)
+    return pkg.build_cusp_geometry(grid, system.charges, system.positions)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_multi_grid_filter_matches_single_grids(pkg, cuda, dtype):
+    """One launch over systems of different nz equals the per-system filters."""
+    geos = [_scan_geometry(pkg, cuda, bond, spacing=0.4, transverse=10.0) for bond in (0.8, 2.6, 4.1)]
+    assert len({g.grid.shape for g in geos}) == 3
+    h = pkg.batch.MultiGeometryHamiltonian(geos)
+    if dtype == torch.float32:
+        h = h.as_dtype(torch.float32)
+    k = 5
+    degree = 7
+    bounds = [(0.4, 30.0, -1.5), (0.3, 28.0, -1.2), (0.5, 32.0, -1.0)]
+    rows = [pkg.chebyshev_coefficients(degree, *bb) for bb in bounds]
+    table = torch.tensor(rows, dtype=torch.float64, device=cuda)
+    gen = torch.Generator().manual_seed(4)
+    blocks = [torch.randn((k, g.grid.n_points), dtype=torch.float64, generator=gen).to(cuda) for g in geos]
+    big = torch.stack([h.embed(s, blocks[s]) for s in range(3)])
+    got = h.filter(big, table, degree)
+    tol = 1e-12 if dtype == torch.float64 else 2e-5
+    for s, g in enumerate(geos):
+        single = pkg.CuspFactoredHamiltonian(g.grid, g.factor, quadrature=g.quadrature, dtype=dtype)
+        want = pkg.chebyshev_filter(single, blocks[s], degree, *bounds[s])
+        sub = h.extract(s, got[s])
+        torch.testing.assert_close(sub, want, rtol=0, atol=tol * float(want.abs().max()))
+        outside = got[s].reshape(-1, *h.grid.shape)
+        sx, sy, sz = g.grid.shape
+        assert float(outside[:, sx:].abs().max() if sx < h.grid.shape[0] else 0.0) == 0.0
+        assert float(outside[:, :, :, sz:].abs().max() if sz < h.grid.shape[2] else 0.0) == 0.0
+
+
+SCAN = tuple(0.8 + k * 5.2 / 47 for k in (0, 11, 23, 35, 47))
+
+
+@pytest.mark.parametrize("precision", [torch.float64, torch.float32])
+def test_batched_scan_matches_the_reference(pkg, cuda, golden_values, precision):
+    """Config 4: five members of the H2+ scan (grids 49x49x52 .. 73) in one batched solve."""
+    refs = [golden_values.get(f"h2plus_scan_R{bond:.4f}") for bond in SCAN]
+    if any(r is None for r in refs):
+        pytest.skip("no scan fixtures (make_golden.py --with-scan)")
+    geos = [_scan_geometry(pkg, cuda, bond) for bond in SCAN]
+    out = pkg.batch.solve_noninteracting_batch(geos, 1.0, filter_precision=precision)
+    for res, ref in zip(out, refs):
+        assert res["converged"]
+        if precision == torch.float64:
+            assert abs(res["total"] - ref["total"]) < 1e-11
+            assert res["iterations"] == ref["iterations"]
+        else:
+            assert abs(res["total"] - ref["total"]) < 1e-9

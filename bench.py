@@ -51,6 +51,8 @@ def _args():
                    help="time only the fused Chebyshev step on a He grid of --edge points (for profiling)")
     p.add_argument("--breakdown", action="store_true",
                    help="device time per kernel of one solve (torch.profiler, no replay) instead of the bench line")
+    p.add_argument("--workload", choices=("he-lda", "h2plus-scan"), default="he-lda",
+                   help="he-lda: the headline He-LDA 65^3 solve; h2plus-scan: the 48-system bond scan")
     p.add_argument("--edge", type=int, default=65)
     p.add_argument("--orbitals", type=int, default=5)
     return p.parse_args()
@@ -220,6 +222,57 @@ def run_kernel_only(args) -> None:
                       "peak_kind": kind, "frac": achieved / peak}), flush=True)
 
 
+def run_scan(args) -> None:
+    """The bare H2+ bond scan: 48 systems, R = 0.8 + k 5.2 / 47, box (12, 12, R + 12), h = 0.25.
+
+    Every system has its own grid (49 x 49 x 52 .. 73) and device geometry; one batched solve runs
+    them together (one filter launch per CheFSI iteration for all 48). Reports systems per second of
+    the batched solve (the geometry builds timed separately) and, for comparison, of one-by-one solves.
+    """
+    import torch
+
+    import __graft_entry__
+    from oracle import scf as oscf  # the system definitions only
+
+    pkg = __graft_entry__.package()
+    dev = torch.device("cuda:0")
+    bonds = [0.8 + k * 5.2 / 47 for k in range(48)]
+    precision = torch.float32 if args.form == "mixed" else torch.float64
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        out = fn()
+        end.record(stream)
+        end.synchronize()
+        return out, start.elapsed_time(end) / 1e3
+
+    def build_all():
+        geos = []
+        for bond in bonds:
+            system = oscf.h2_plus(bond, spacing=0.25, transverse=12.0)
+            grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev)
+            geos.append(pkg.build_cusp_geometry(grid, system.charges, system.positions))
+        return geos
+
+    geos, build_s = timed(build_all)
+    for _ in range(max(1, args.warmup)):
+        pkg.batch.solve_noninteracting_batch(geos, 1.0, filter_precision=precision)
+    batched, batched_s = timed(lambda: pkg.batch.solve_noninteracting_batch(geos, 1.0, filter_precision=precision))
+    _, single_s = timed(lambda: [pkg.solve_noninteracting(g, n_electrons=1.0) for g in geos])
+    golden = json.loads((ROOT / "tests" / "golden" / "reference_values.json").read_text())
+    errors = [abs(batched[k]["total"] - golden[f"h2plus_scan_R{bonds[k]:.4f}"]["total"])
+              for k in range(48) if f"h2plus_scan_R{bonds[k]:.4f}" in golden]
+    print(json.dumps({
+        "metric": "H2+ bond scan (48 systems, own grids) solves/s", "value": 48 / batched_s, "unit": "solves/s",
+        "n_gpus": 1, "form": args.form, "batched_solve_s": batched_s, "one_by_one_solve_s": single_s,
+        "geometry_build_s": build_s, "grids": sorted({g.grid.shape for g in geos}),
+        "max_energy_error_vs_reference_ha": max(errors) if errors else None, "reference_members_checked": len(errors),
+        "data": "synthetic (the H2+ systems themselves)"}), flush=True)
+
+
 def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str]:
     """Seconds for one full solve of the CPU restatement, from a bounded, measured sample.
 
@@ -331,6 +384,9 @@ def main() -> None:
         return
     if args.kernel_only:
         run_kernel_only(args)
+        return
+    if args.workload == "h2plus-scan":
+        run_scan(args)
         return
     import torch
 

@@ -234,3 +234,26 @@ def test_h2plus_scan_members(pkg, cuda, golden_values, bond):
     out = pkg.solve_noninteracting(_geometry(pkg, system, cuda), n_electrons=1.0)
     assert abs(out["total"] - ref["total"]) < 1e-11
     assert out["iterations"] == ref["iterations"]
+
+
+@pytest.mark.parametrize("precision", [torch.float64, torch.float32])
+def test_config3_h2_pbe_81x81x91(pkg, cuda, golden_values, precision):
+    """Config 3: H2 (R = 1.4) PBE, box 16 x 16 x 18, h = 0.20 (81 x 81 x 91), degree 16, unanchored.
+
+    float64: the reference's CPU float64 energy to 1e-10 Ha in the same number of SCF iterations;
+    mixed (float32 filter, float64 Ritz, float64 refinement): to 1e-8 Ha.
+    """
+    ref = golden_values.get("h2_pbe_h020")
+    if ref is None:
+        pytest.skip("no config 3 fixture (make_golden.py --with-config3)")
+    system = oscf.h2_pbe()
+    geo = _geometry(pkg, system, cuda)
+    assert geo.grid.shape == (81, 81, 91)
+    step = pkg.KohnShamStep(geo, "pbe", 2.0, pkg.EigenConfig(chebyshev_degree=16), filter_precision=precision)
+    out = pkg.solve_self_consistent(step, pkg.MixingConfig())
+    assert out.converged
+    if precision == torch.float64:
+        assert abs(out.energies["total"] - ref["total"]) < 1e-10
+        assert out.scf_iterations == ref["iterations"]
+    else:
+        assert abs(out.energies["total"] - ref["total"]) < 1e-8

@@ -403,6 +403,7 @@ class BatchedPotentials:
     hartree_energy: torch.Tensor   # (B,)
     xc_energy: torch.Tensor        # (B,)
     xc_double_counting: torch.Tensor  # (B,)
+    v_smooth: torch.Tensor | None = None  # (B, N): the Poisson solution of the smooth density
 
 
 class BatchedKohnShamStep:
@@ -434,8 +435,14 @@ class BatchedKohnShamStep:
         self.bare_potential = self.quadrature.bare_operator_terms()[0]
         self.occ = torch.from_numpy(aufbau_occupations(self.n_states, self.n_electrons)[0]).to(self.grid.device)
 
-    def potentials(self, density: torch.Tensor) -> BatchedPotentials:
-        """(``src/cdft/scf/step.py:224-313``) for ``(B, N)`` total densities, LDA."""
+    def potentials(self, density: torch.Tensor, v_smooth: torch.Tensor | None = None) -> BatchedPotentials:
+        """(``src/cdft/scf/step.py:224-313``) for ``(B, N)`` total densities, LDA.
+
+        The smooth density (the total minus the cusp terms, whose coefficients solve a fixed linear
+        system) and its Poisson solution are linear in the density. A caller that already holds
+        ``v_smooth`` for this density -- the same linear combination of earlier solutions as the
+        density is of earlier densities -- passes it and the solve is skipped.
+        """
         g = self.geometry
         q = self.quadrature
         grid = self.grid
@@ -457,9 +464,12 @@ class BatchedKohnShamStep:
         coef = torch.empty((b, na), **f)
         call("cdftb_cusp_coefficients_f64", ptr(rho_nuc), ptr(g.step.nucleus_f2), ptr(g.step.overlap), na, b,
              ptr(coef), stream)
-        call("cdftb_hartree_split_f64", ptr(n_grid), ptr(self.f2), ptr(g.step.cusp_grid), ptr(coef), na, n, b,
-             ptr(rho), ptr(n_smooth), stream)
-        self.poisson.solve_batch(n_smooth, out=fields[1])
+        if v_smooth is None:
+            call("cdftb_hartree_split_f64", ptr(n_grid), ptr(self.f2), ptr(g.step.cusp_grid), ptr(coef), na, n, b,
+                 ptr(rho), ptr(n_smooth), stream)
+            self.poisson.solve_batch(n_smooth, out=fields[1])
+        else:
+            fields[1].copy_(v_smooth)
         node = q._interp_raw(fields.reshape(2 * b, n), 2 * b).reshape(2, b, m)
         lift_in = torch.empty((b, 2, m), **f)
         e_w = torch.empty((b, m), **f)
@@ -475,7 +485,7 @@ class BatchedKohnShamStep:
         sums = row_sums(terms)  # (b, 3)
         node_sum = row_sums(e_w)  # (b,)
         return BatchedPotentials(effective=effective, v_hartree=v_hartree, hartree_energy=0.5 * sums[:, 0],
-                                 xc_energy=node_sum + sums[:, 2], xc_double_counting=sums[:, 1])
+                                 xc_energy=node_sum + sums[:, 2], xc_double_counting=sums[:, 1], v_smooth=fields[1])
 
     def hamiltonian(self, effective: torch.Tensor, dtype=torch.float64) -> BatchedHamiltonian:
         return BatchedHamiltonian(self.grid, self.factor, self.quadrature, self.bare_potential[None, :] + effective,
@@ -600,6 +610,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         n_in = n_in.expand(b, -1).contiguous()
     initial_block = None
     previous_effective = None
+    vs_in = None  # v_smooth of n_in, carried by linearity while every mixer is linear
     limit = scf.max_iterations if max_iterations is None else max_iterations
     active = list(range(b))
     last_p_in = [None] * b
@@ -611,7 +622,8 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         sel = torch.tensor(active, dtype=torch.long, device=dev)
         full = len(active) == b
         nin = n_in if full else n_in.index_select(0, sel)
-        p_in = step.potentials(nin)
+        vs = None if vs_in is None else (vs_in if full else vs_in.index_select(0, sel))
+        p_in = step.potentials(nin, v_smooth=vs)
         h = step.hamiltonian(p_in.effective)
         float_now = [systems[s].float_phase for s in active]
         h32 = step.hamiltonian(p_in.effective, dtype=torch.float32) if all(float_now) else None
@@ -651,8 +663,12 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         host = torch.stack([*terms.values(), res_norm]).cpu().numpy()  # (len(keys)+1, S)
         # mixing (per system: linear in one batched expression when all are linear)
         n_next = torch.empty_like(nin)
+        linear = all(isinstance(systems[s].mixer, LinearMixer) for s in active)
+        vs_next = torch.empty_like(nin) if linear else None
         for j, s in enumerate(active):
             n_next[j] = systems[s].mixer.mix(nin[j:j + 1], n_out[j:j + 1], iteration)[0]
+            if linear:  # the same combination of the two Poisson solutions (a stateless mixer)
+                vs_next[j] = systems[s].mixer.mix(p_in.v_smooth[j:j + 1], p_out.v_smooth[j:j + 1], iteration)[0]
         new_active = []
         for j, s in enumerate(active):
             st = systems[s]
@@ -684,16 +700,20 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
                 st.worsened = 0
                 st.rung_changed = True
                 n_next[j] = nin[j] + 0.5 * mixing.alpha * residual[j]
+                if vs_next is not None:
+                    vs_next[j] = p_in.v_smooth[j] + 0.5 * mixing.alpha * (p_out.v_smooth[j] - p_in.v_smooth[j])
             new_active.append(s)
         # write back the per-system state of this iteration
         if full:
             n_in = n_next
             previous_effective = p_in.effective
             initial_block = vectors
+            vs_in = vs_next
         else:
             n_in = n_in.index_copy(0, sel, n_next)
             previous_effective = previous_effective.index_copy(0, sel, p_in.effective)
             initial_block = initial_block.index_copy(0, sel, vectors)
+            vs_in = None if (vs_next is None or vs_in is None) else vs_in.index_copy(0, sel, vs_next)
         if previous_effective is None:
             previous_effective = p_in.effective
         active = new_active

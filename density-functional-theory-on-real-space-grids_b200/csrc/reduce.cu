@@ -29,7 +29,7 @@ CrossShape cross_shape(int ma, int mb, int64_t n, int groups) {
     s.tiles_i = static_cast<int>(ceil_div(ma, s.ti));
     s.tiles_j = static_cast<int>(ceil_div(mb, s.tj));
     const int64_t blocks_per_chunkset = static_cast<int64_t>(s.tiles_i) * s.tiles_j * groups;
-    int64_t chunks = ceil_div(2 * 148, blocks_per_chunkset);
+    int64_t chunks = ceil_div(8 * 148, blocks_per_chunkset);  // about 8 CTAs of 256 threads per SM
     const int64_t max_chunks = ceil_div(n, 2048);
     if (chunks > max_chunks) chunks = max_chunks;
     if (chunks < 1) chunks = 1;
@@ -38,12 +38,16 @@ CrossShape cross_shape(int ma, int mb, int64_t n, int groups) {
     return s;
 }
 
-template <int TI, int TJ>
+// SAME: a and b are the same rows (a Gram matrix), each row is loaded once. Each thread takes the
+// columns p0 + t, p0 + t + RT, ... four at a time (independent loads in flight), always in the
+// same order, so the partial of a chunk does not depend on scheduling.
+template <int TI, int TJ, bool SAME>
 __global__ void __launch_bounds__(RT) cross_partial_kernel(const double* __restrict__ a, int ma, int64_t sa,
                                                             const double* __restrict__ b, int mb, int64_t sb,
                                                             const double* __restrict__ q, int64_t q_stride, int64_t n,
                                                             int tiles_j, int64_t chunk, int chunks,
                                                             double* __restrict__ partial) {
+    constexpr int U = 4;
     const int c = blockIdx.x;
     const int tile = blockIdx.y;
     const int g = blockIdx.z;
@@ -59,17 +63,43 @@ __global__ void __launch_bounds__(RT) cross_partial_kernel(const double* __restr
     for (int i = 0; i < TI; ++i)
 #pragma unroll
         for (int j = 0; j < TJ; ++j) acc[i][j] = 0.0;
-    for (int64_t p = p0 + threadIdx.x; p < p1; p += RT) {
+    int64_t p = p0 + threadIdx.x;
+    for (; p + (U - 1) * RT < p1; p += U * RT) {
+        double w[U], av[U][TI], bv[U][TJ];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t pu = p + u * RT;
+            w[u] = qg ? qg[pu] : 1.0;
+#pragma unroll
+            for (int i = 0; i < TI; ++i) av[u][i] = (i0 + i < ma) ? ag[(i0 + i) * n + pu] : 0.0;
+            if (!SAME) {
+#pragma unroll
+                for (int j = 0; j < TJ; ++j) bv[u][j] = (j0 + j < mb) ? bg[(j0 + j) * n + pu] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int i = 0; i < TI; ++i) {
+                const double wa = av[u][i] * w[u];
+#pragma unroll
+                for (int j = 0; j < TJ; ++j) acc[i][j] = fma(wa, SAME ? av[u][j] : bv[u][j], acc[i][j]);
+            }
+        }
+    }
+    for (; p < p1; p += RT) {
         const double w = qg ? qg[p] : 1.0;
         double av[TI], bv[TJ];
 #pragma unroll
-        for (int i = 0; i < TI; ++i) av[i] = (i0 + i < ma) ? ag[(i0 + i) * n + p] * w : 0.0;
+        for (int i = 0; i < TI; ++i) av[i] = (i0 + i < ma) ? ag[(i0 + i) * n + p] : 0.0;
 #pragma unroll
-        for (int j = 0; j < TJ; ++j) bv[j] = (j0 + j < mb) ? bg[(j0 + j) * n + p] : 0.0;
+        for (int j = 0; j < TJ; ++j) bv[j] = SAME ? av[j] : ((j0 + j < mb) ? bg[(j0 + j) * n + p] : 0.0);
 #pragma unroll
-        for (int i = 0; i < TI; ++i)
+        for (int i = 0; i < TI; ++i) {
+            const double wa = av[i] * w;
 #pragma unroll
-            for (int j = 0; j < TJ; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+            for (int j = 0; j < TJ; ++j) acc[i][j] = fma(wa, bv[j], acc[i][j]);
+        }
     }
     __shared__ double red[RT / 32][TI * TJ];
     const int lane = threadIdx.x & 31;
@@ -137,15 +167,22 @@ int launch_cross(const double* a, int ma, int64_t group_stride_a, const double* 
     double* partial = static_cast<double*>(scratch);
     const int tiles = s.tiles_i * s.tiles_j;
     dim3 grid(s.chunks, tiles, groups);
-    if (s.ti == 1)
-        cross_partial_kernel<1, 1><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, q_group_stride,
-                                                        n, s.tiles_j, s.chunk, s.chunks, partial);
-    else if (s.ti == 6)
-        cross_partial_kernel<6, 6><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, q_group_stride,
-                                                        n, s.tiles_j, s.chunk, s.chunks, partial);
-    else
-        cross_partial_kernel<4, 4><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, q_group_stride,
-                                                        n, s.tiles_j, s.chunk, s.chunks, partial);
+    // the same rows on both sides (a Gram matrix): one load per element
+    const bool same = a == b && ma == mb && group_stride_a == group_stride_b && s.tiles_i == 1 && s.tiles_j == 1;
+#define CDFTB_CROSS_LAUNCH(TI_, TJ_, SAME_)                                                                 \
+    cross_partial_kernel<TI_, TJ_, SAME_><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, \
+                                                               q_group_stride, n, s.tiles_j, s.chunk, s.chunks,  \
+                                                               partial)
+    if (s.ti == 1) {
+        if (same) CDFTB_CROSS_LAUNCH(1, 1, true);
+        else CDFTB_CROSS_LAUNCH(1, 1, false);
+    } else if (s.ti == 6) {
+        if (same) CDFTB_CROSS_LAUNCH(6, 6, true);
+        else CDFTB_CROSS_LAUNCH(6, 6, false);
+    } else {
+        CDFTB_CROSS_LAUNCH(4, 4, false);
+    }
+#undef CDFTB_CROSS_LAUNCH
     int rc = check_launch();
     if (rc != CDFTB_OK) return rc;
     const int64_t total = static_cast<int64_t>(groups) * ma * mb;

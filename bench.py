@@ -354,6 +354,11 @@ def _breakdown(solve, n0) -> None:
     print(f"wall {wall * 1e3:.0f} ms per step, GPU busy {busy:.1f} ms")
     for k in sorted(rows, key=lambda r: -r.self_device_time_total)[:30]:
         print(f"{k.self_device_time_total / 1e3:9.2f} ms  {k.count:7d}  {k.key[:110]}")
+    last = getattr(solve, "last", None)
+    if last is not None:
+        ms = last.measurements
+        print("scf iterations", last.scf_iterations)
+        print("float64 refinement from iteration", ms.get("fp64_refinement_from_iteration"))
 
 
 def replica_seeds(rank: int, batch: int) -> list[int]:
@@ -435,6 +440,7 @@ def main() -> None:
 
         def solve(initial):
             out = pkg.batch.solve_self_consistent_batch(step, mixing, initial_density=initial)
+            solve.last = out
             return ([e["total"] for e in out.energies], out.density, max(out.scf_iterations), out.applications)
 
     for _ in range(max(0, args.warmup)):

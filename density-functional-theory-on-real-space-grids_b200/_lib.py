@@ -63,6 +63,9 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_small_eigh_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
     "cdftb_block_rotate_f64": (c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int, c_int64, c_int, c_int, c_int64,
                                        c_int, c_void_p]),
+    "cdftb_block_ritz_scratch_bytes": (c_int64, [c_int, c_int64, c_int]),
+    "cdftb_block_ritz_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int64, c_int,
+                                     c_void_p, c_void_p, c_void_p, c_int64, c_void_p]),
     "cdftb_block_residual_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int64, c_int, c_int64,
                                          c_void_p]),
     "cdftb_lanczos_update_f64": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int,

@@ -164,16 +164,27 @@ def batched_rayleigh_ritz(h: BatchedHamiltonian, block: torch.Tensor):
     sub = measure_cross(basis, applied, q, b)
     call("cdftb_small_eigh_f64", ptr(sub), ptr(rb.evals), ptr(rb.rot), m, b, stream)
     vectors = torch.empty_like(flat)
-    call("cdftb_block_rotate_f64", ptr(rb.rot), ptr(basis), m * n, ptr(vectors), F64, m * n, m, m, n, b, stream)
-    rot_applied = torch.empty_like(flat)
-    call("cdftb_block_rotate_f64", ptr(rb.rot), ptr(applied), m * n, ptr(rot_applied), F64, m * n, m, m, n, b, stream)
+    evals = rb.evals.clone()
+    if m <= 8:
+        # the rotations, the residual and its norm in one pass (no rotated A Q or residual block)
+        norms_sq = torch.empty((b, m), dtype=torch.float64, device=dev)
+        need = _lib.library().cdftb_block_ritz_scratch_bytes(m, n, b)
+        scratch = torch.empty(need, dtype=torch.uint8, device=dev)
+        q_stride = 0 if q.dim() == 1 else n
+        call("cdftb_block_ritz_f64", ptr(rb.rot), ptr(basis), ptr(applied), ptr(evals), ptr(q.contiguous()), q_stride,
+             m, n, b, ptr(vectors), ptr(norms_sq), ptr(scratch), need, stream)
+        norms = norms_sq.clamp_min(0.0).sqrt()
+    else:
+        call("cdftb_block_rotate_f64", ptr(rb.rot), ptr(basis), m * n, ptr(vectors), F64, m * n, m, m, n, b, stream)
+        rot_applied = torch.empty_like(flat)
+        call("cdftb_block_rotate_f64", ptr(rb.rot), ptr(applied), m * n, ptr(rot_applied), F64, m * n, m, m, n, b,
+             stream)
+        res = torch.empty_like(flat)
+        call("cdftb_block_residual_f64", ptr(rot_applied), ptr(vectors), ptr(evals), ptr(res), m, n, b, m * n, stream)
+        norms = _row_inner(res, res, q).clamp_min(0.0).sqrt()
     g2 = measure_cross(vectors, vectors, q, b)
     eye = torch.eye(m, dtype=torch.float64, device=dev)
     orth = (g2 - eye).abs().amax(dim=(1, 2))
-    evals = rb.evals.clone()
-    res = torch.empty_like(flat)
-    call("cdftb_block_residual_f64", ptr(rot_applied), ptr(vectors), ptr(evals), ptr(res), m, n, b, m * n, stream)
-    norms = _row_inner(res, res, q).clamp_min(0.0).sqrt()
     return evals, vectors, norms, orth, rb.info.clone()
 
 
@@ -258,11 +269,15 @@ def _fraction(value, low, high):
 
 def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_states: int, config: EigenConfig,
                    initial: torch.Tensor | None, streams: list[SeededStream], bounds: list, max_iterations: int,
-                   switch_residual: float | None, ritz_stop: bool = False):
+                   switch_residual: float | None, ritz_stop: bool = False, float_mask: list | None = None):
     """CheFSI for every system of ``h`` (``src/cdft/eigen/chefsi.py:442-585``).
 
     ``ritz_stop`` adds the weak-form stop of the bare-nucleus path: Ritz values stable (drift below
     a tenth of ``cross_check_tol``) on two iterations in a row.
+
+    ``float_mask[b]`` (default: every system) marks the systems that start in float filtering when
+    ``h32`` is given; each leaves it on its own at ``switch_residual``. A step filters the float
+    systems in one float launch and the others in one float64 launch.
 
     ``bounds[b]`` is ``None`` (run Lanczos) or ``(lower, upper, shift)``. Returns per-system
     eigenvalues ``(B, n_states)``, eigenvectors ``(B, n_states, N)``, residuals ``(B, n_states)``,
@@ -283,7 +298,8 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
                 blk = torch.cat([blk, streams[s].randn((m - blk.shape[0], n))], dim=0)
             blocks.append(blk)
     block = torch.stack(blocks)
-    states = [_EigenState(float_filter=h32 is not None) for _ in range(b)]
+    states = [_EigenState(float_filter=h32 is not None and (float_mask is None or bool(float_mask[s])))
+              for s in range(b)]
     need = [s for s in range(b) if bounds[s] is None]
     if need:
         starts = torch.stack([streams[s].randn(n) for s in need])
@@ -340,10 +356,19 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
         sel = None if full else torch.tensor(active, dtype=torch.long, device=dev)
         hv = h if full else h.subset(active)
         cur = vectors if full else vectors.index_select(0, sel)
-        # float filter while every active system is still in its float phase (the batch shares a launch)
+        # systems in their float phase filter in float, the others in float64 (one launch each)
         if h32 is not None and all(use_float):
             hf = h32 if full else h32.subset(active)
             filtered = hf.filter(cur, table, config.chebyshev_degree)
+        elif h32 is not None and any(use_float):
+            fpos = [j for j, u in enumerate(use_float) if u]
+            dpos = [j for j, u in enumerate(use_float) if not u]
+            filtered = torch.empty_like(cur)
+            for pos, ham in ((fpos, h32), (dpos, h)):
+                idx = torch.tensor(pos, dtype=torch.long, device=dev)
+                part = ham.subset([active[j] for j in pos])
+                filtered.index_copy_(0, idx, part.filter(cur.index_select(0, idx), table.index_select(0, idx),
+                                                         config.chebyshev_degree))
         else:
             filtered = hv.filter(cur, table, config.chebyshev_degree)
         ev, vec, res, orth, info = batched_rayleigh_ritz(hv, filtered)
@@ -626,7 +651,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         p_in = step.potentials(nin, v_smooth=vs)
         h = step.hamiltonian(p_in.effective)
         float_now = [systems[s].float_phase for s in active]
-        h32 = step.hamiltonian(p_in.effective, dtype=torch.float32) if all(float_now) else None
+        h32 = step.hamiltonian(p_in.effective, dtype=torch.float32) if any(float_now) else None
         hints = []
         shifts = None
         if previous_effective is not None:
@@ -646,7 +671,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         switch = step.FLOAT_FILTER_SWITCH_RESIDUAL if init is None else None
         h.applications = 0
         evals, vectors, _, estates = batched_chefsi(h, h32, step.n_states, step.eigen, init, streams, hints, steps_cap,
-                                                    switch)
+                                                    switch, float_mask=float_now)
         for j, s in enumerate(active):
             st = systems[s]
             es = estates[j]

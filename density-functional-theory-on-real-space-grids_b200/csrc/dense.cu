@@ -233,6 +233,114 @@ __global__ void rotate_fixed_kernel(const double* __restrict__ r, const double* 
     }
 }
 
+// The end of Rayleigh--Ritz in one pass over the block: v_i = sum_j R_ij basis_j and
+// (A v)_i = sum_j R_ij applied_j (the FMA order of rotate_fixed_kernel), the residual
+// rho_i = (A v)_i - lambda_i v_i (as residual_kernel), v written out and q rho_i^2 summed. A CTA
+// takes a fixed chunk of points of one group, two points per thread at a time, and writes one
+// partial per row; ritz_final_kernel adds the partials in chunk order (deterministic).
+constexpr int RITZ_THREADS = 256;
+
+template <int M>
+__global__ void __launch_bounds__(RITZ_THREADS) ritz_fixed_kernel(const double* __restrict__ r,
+                                                                 const double* __restrict__ basis,
+                                                                 const double* __restrict__ applied,
+                                                                 const double* __restrict__ evals,
+                                                                 const double* __restrict__ q, int64_t q_stride,
+                                                                 int64_t n, int64_t chunk,
+                                                                 double* __restrict__ vectors,
+                                                                 double* __restrict__ partial) {
+    __shared__ double rs[M * M];
+    __shared__ double lam[M];
+    __shared__ double red[RITZ_THREADS / 32][M];
+    const int g = blockIdx.y;
+    const int c = blockIdx.x;
+    for (int i = threadIdx.x; i < M * M; i += blockDim.x) rs[i] = r[static_cast<int64_t>(g) * M * M + i];
+    if (threadIdx.x < M) lam[threadIdx.x] = evals[static_cast<int64_t>(g) * M + threadIdx.x];
+    __syncthreads();
+    const int64_t base = static_cast<int64_t>(g) * M * n;
+    const double* qg = q + g * q_stride;
+    const int64_t p0 = c * chunk;
+    const int64_t p1 = (p0 + chunk < n) ? p0 + chunk : n;
+    double acc[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) acc[i] = 0.0;
+    auto point = [&](int64_t p, const double* x, const double* y, double w) {
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            double v = 0.0, av = 0.0;
+#pragma unroll
+            for (int j = 0; j < M; ++j) {
+                v = fma(rs[i * M + j], x[j], v);
+                av = fma(rs[i * M + j], y[j], av);
+            }
+            vectors[base + i * n + p] = v;
+            const double res = av - lam[i] * v;
+            acc[i] = fma(res * w, res, acc[i]);
+        }
+    };
+    int64_t p = p0 + threadIdx.x;
+    constexpr bool kPairs = M <= 5;  // two points in flight per thread where the registers allow it
+    for (; kPairs && p + RITZ_THREADS < p1; p += 2 * RITZ_THREADS) {
+        double x0[M], y0[M], x1[M], y1[M];
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            x0[j] = basis[base + j * n + p];
+            y0[j] = applied[base + j * n + p];
+            x1[j] = basis[base + j * n + p + RITZ_THREADS];
+            y1[j] = applied[base + j * n + p + RITZ_THREADS];
+        }
+        const double w0 = qg[p], w1 = qg[p + RITZ_THREADS];
+        point(p, x0, y0, w0);
+        point(p + RITZ_THREADS, x1, y1, w1);
+    }
+    for (; p < p1; p += RITZ_THREADS) {
+        double x0[M], y0[M];
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            x0[j] = basis[base + j * n + p];
+            y0[j] = applied[base + j * n + p];
+        }
+        point(p, x0, y0, qg[p]);
+    }
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        double v = acc[i];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) red[warp][i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < M) {
+        double v = 0.0;
+        for (int w = 0; w < RITZ_THREADS / 32; ++w) v += red[w][threadIdx.x];
+        partial[(static_cast<int64_t>(g) * gridDim.x + c) * M + threadIdx.x] = v;
+    }
+}
+
+// One warp per (group, row): lanes take chunks lane, lane + 32, ... in order, then a fixed shuffle tree.
+__global__ void ritz_final_kernel(const double* __restrict__ partial, int m, int chunks, int groups,
+                                  double* __restrict__ out) {
+    const int64_t idx = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (idx >= static_cast<int64_t>(groups) * m) return;
+    const int64_t g = idx / m;
+    const int i = static_cast<int>(idx - g * m);
+    double v = 0.0;
+    for (int c = lane; c < chunks; c += 32) v += partial[(g * chunks + c) * m + i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) out[idx] = v;
+}
+
+int ritz_chunks(int64_t n, int groups) {
+    int64_t chunks = ceil_div(int64_t(8) * 148, groups);  // about 8 CTAs per SM over the whole launch
+    const int64_t most = ceil_div(n, int64_t(2048));
+    if (chunks > most) chunks = most;
+    return static_cast<int>(chunks < 1 ? 1 : chunks);
+}
+
 inline unsigned point_blocks(int64_t n) {
     const int64_t b = ceil_div(n, 256);
     return static_cast<unsigned>(b < 148 * 8 ? b : 148 * 8);
@@ -318,3 +426,41 @@ extern "C" int cdftb_lanczos_update_f64(int mode, double* w, const double* v, co
     lanczos_kernel<<<grid, 256, 0, as_stream(stream)>>>(mode, w, v, v_prev, s1, s2, n);
     return check_launch();
 }
+
+extern "C" int64_t cdftb_block_ritz_scratch_bytes(int m, int64_t n, int groups) {
+    if (m <= 0 || n <= 0 || groups <= 0) return 0;
+    return static_cast<int64_t>(groups) * ritz_chunks(n, groups) * m * 8;
+}
+
+extern "C" int cdftb_block_ritz_f64(const double* r, const double* basis, const double* applied, const double* evals,
+                                    const double* q, int64_t q_group_stride, int m, int64_t n, int groups,
+                                    double* vectors, double* norms_sq, void* scratch, int64_t scratch_bytes,
+                                    cdftb_stream_t stream) {
+    if (!r || !basis || !applied || !evals || !q || !vectors || !norms_sq || m <= 0 || m > 8 || n <= 0 ||
+        groups <= 0 || groups > 65535 || q_group_stride < 0)
+        return CDFTB_ERR_ARGUMENT;
+    if (!scratch || scratch_bytes < cdftb_block_ritz_scratch_bytes(m, n, groups)) return CDFTB_ERR_ARGUMENT;
+    const int chunks = ritz_chunks(n, groups);
+    const int64_t chunk = ceil_div(n, static_cast<int64_t>(chunks));
+    const int used = static_cast<int>(ceil_div(n, chunk));
+    cudaStream_t s = as_stream(stream);
+    double* partial = static_cast<double*>(scratch);
+    dim3 grid(used, groups);
+    switch (m) {
+#define CDFTB_RITZ(M)                                                                                             \
+    case M:                                                                                                       \
+        ritz_fixed_kernel<M><<<grid, RITZ_THREADS, 0, s>>>(r, basis, applied, evals, q, q_group_stride, n, chunk, \
+                                                           vectors, partial);                                     \
+        break;
+        CDFTB_RITZ(1) CDFTB_RITZ(2) CDFTB_RITZ(3) CDFTB_RITZ(4) CDFTB_RITZ(5) CDFTB_RITZ(6) CDFTB_RITZ(7) CDFTB_RITZ(8)
+#undef CDFTB_RITZ
+        default: return CDFTB_ERR_ARGUMENT;
+    }
+    int rc = check_launch();
+    if (rc != CDFTB_OK) return rc;
+    const int64_t warps = static_cast<int64_t>(groups) * m;
+    ritz_final_kernel<<<static_cast<unsigned>(ceil_div(warps * 32, 256)), 256, 0, s>>>(partial, m, used, groups,
+                                                                                       norms_sq);
+    return check_launch();
+}
+

@@ -159,6 +159,19 @@ int cdftb_block_rotate_f64(const double* r, const double* in, int64_t in_group_s
                            int out_dtype, int64_t out_group_stride, int m_out, int m_in, int64_t n,
                            int groups, cdftb_stream_t stream);
 
+/* (e6) The end of Rayleigh--Ritz in one pass (rayleigh_ritz.py:100-115): per group g and point p,
+ * v_i = sum_j R[g][i][j] basis[g][j][p] (written to vectors), (A v)_i = sum_j R[g][i][j] applied[g][j][p],
+ * and the residual rho_i = (A v)_i - evals[g][i] v_i, whose measure norm
+ * norms_sq[g][i] = sum_p q[g][p] rho_i(p)^2 is returned squared (q_group_stride 0: one q for every
+ * group). Blocks are m consecutive rows of n; m <= 8. Deterministic: partials per fixed chunk of
+ * points in scratch (>= cdftb_block_ritz_scratch_bytes), added in chunk order. The same values as
+ * two cdftb_block_rotate_f64, cdftb_block_residual_f64 and a measure product, without the rotated
+ * applied block and the residual block in memory. */
+int64_t cdftb_block_ritz_scratch_bytes(int m, int64_t n, int groups);
+int cdftb_block_ritz_f64(const double* r, const double* basis, const double* applied, const double* evals,
+                         const double* q, int64_t q_group_stride, int m, int64_t n, int groups, double* vectors,
+                         double* norms_sq, void* scratch, int64_t scratch_bytes, cdftb_stream_t stream);
+
 /* (e5) out[g][i][p] = a[g][i][p] - evals[g][i] * b[g][i][p] (rayleigh_ritz.py:114 residual).
  * Each group's m rows are m consecutive rows of n elements, groups group_stride elements apart. */
 int cdftb_block_residual_f64(const double* a, const double* b, const double* evals, double* out, int m,

@@ -269,15 +269,17 @@ def _fraction(value, low, high):
 
 def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_states: int, config: EigenConfig,
                    initial: torch.Tensor | None, streams: list[SeededStream], bounds: list, max_iterations: int,
-                   switch_residual: float | None, ritz_stop: bool = False, float_mask: list | None = None):
+                   switch_residual: float | None, ritz_stop: bool = False, float_mask: list | None = None,
+                   stop_at_switch: bool = False):
     """CheFSI for every system of ``h`` (``src/cdft/eigen/chefsi.py:442-585``).
 
     ``ritz_stop`` adds the weak-form stop of the bare-nucleus path: Ritz values stable (drift below
     a tenth of ``cross_check_tol``) on two iterations in a row.
 
     ``float_mask[b]`` (default: every system) marks the systems that start in float filtering when
-    ``h32`` is given; each leaves it on its own at ``switch_residual``. A step filters the float
-    systems in one float launch and the others in one float64 launch.
+    ``h32`` is given; each leaves it on its own at ``switch_residual``, to go on in float64 or, with
+    ``stop_at_switch``, to stop there. A step filters the float systems in one float launch and the
+    others in one float64 launch.
 
     ``bounds[b]`` is ``None`` (run Lanczos) or ``(lower, upper, shift)``. Returns per-system
     eigenvalues ``(B, n_states)``, eigenvectors ``(B, n_states, N)``, residuals ``(B, n_states)``,
@@ -404,6 +406,11 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
                 still.append(s)
             if st.float_filter and switch_residual is not None and host[0, j] < switch_residual:
                 st.float_filter = False
+                if stop_at_switch and not st.converged:
+                    st.converged = True
+                    st.stop_reason = "residual below the float-filter switch"
+                    done.append(s)
+                    still.remove(s)
         if done:
             idx = torch.tensor(done, dtype=torch.long, device=dev)
             out_evals = out_evals.index_copy(0, idx, evals.index_select(0, idx))
@@ -670,8 +677,11 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         steps_cap = step.eigen.max_iterations if init is None else FILTER_STEPS_PER_ITERATION
         switch = step.FLOAT_FILTER_SWITCH_RESIDUAL if init is None else None
         h.applications = 0
+        # The first full diagonalisation of a mixed solve stops at the float switch: the float phase
+        # that follows holds float accuracy anyway, and the float64 refinement sweep and the final
+        # float64 diagonalisation set the result's.
         evals, vectors, _, estates = batched_chefsi(h, h32, step.n_states, step.eigen, init, streams, hints, steps_cap,
-                                                    switch, float_mask=float_now)
+                                                    switch, float_mask=float_now, stop_at_switch=mixed)
         for j, s in enumerate(active):
             st = systems[s]
             es = estates[j]

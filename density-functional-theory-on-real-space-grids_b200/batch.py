@@ -436,6 +436,8 @@ class BatchedPotentials:
     xc_energy: torch.Tensor        # (B,)
     xc_double_counting: torch.Tensor  # (B,)
     v_smooth: torch.Tensor | None = None  # (B, N): the Poisson solution of the smooth density
+    node: torch.Tensor | None = None      # (2, B, M): rho and v_smooth at the quadrature nodes
+    lifted_h: torch.Tensor | None = None  # (B, N): L^T of the Hartree node weights
 
 
 class BatchedKohnShamStep:
@@ -467,13 +469,16 @@ class BatchedKohnShamStep:
         self.bare_potential = self.quadrature.bare_operator_terms()[0]
         self.occ = torch.from_numpy(aufbau_occupations(self.n_states, self.n_electrons)[0]).to(self.grid.device)
 
-    def potentials(self, density: torch.Tensor, v_smooth: torch.Tensor | None = None) -> BatchedPotentials:
+    def potentials(self, density: torch.Tensor, v_smooth: torch.Tensor | None = None,
+                   node: torch.Tensor | None = None, lifted_h: torch.Tensor | None = None) -> BatchedPotentials:
         """(``src/cdft/scf/step.py:224-313``) for ``(B, N)`` total densities, LDA.
 
         The smooth density (the total minus the cusp terms, whose coefficients solve a fixed linear
-        system) and its Poisson solution are linear in the density. A caller that already holds
-        ``v_smooth`` for this density -- the same linear combination of earlier solutions as the
-        density is of earlier densities -- passes it and the solve is skipped.
+        system), its Poisson solution ``v_smooth``, the node values ``node`` of rho and v_smooth, and
+        the lifted Hartree weights ``lifted_h`` are all linear in the density. A caller that already
+        holds them for this density -- the same linear combination of earlier results as the density
+        is of earlier densities -- passes them, and the Poisson solve, the interpolation and the
+        Hartree half of the lift are skipped (the XC half is not linear and is always lifted).
         """
         g = self.geometry
         q = self.quadrature
@@ -502,12 +507,20 @@ class BatchedKohnShamStep:
             self.poisson.solve_batch(n_smooth, out=fields[1])
         else:
             fields[1].copy_(v_smooth)
-        node = q._interp_raw(fields.reshape(2 * b, n), 2 * b).reshape(2, b, m)
+        if node is None:
+            node = q._interp_raw(fields.reshape(2 * b, n), 2 * b).reshape(2, b, m)
+        else:
+            node = node.contiguous()
         lift_in = torch.empty((b, 2, m), **f)
         e_w = torch.empty((b, m), **f)
         call("cdftb_potentials_node_lda_f64", ptr(node), m, ptr(q.weights), ptr(q.f2), ptr(g.step.v1s_node),
              ptr(coef), na, b, ptr(lift_in), ptr(e_w), stream)
-        lifted = q._lift_raw(lift_in, 2 * b)
+        if lifted_h is None:
+            lifted = q._lift_raw(lift_in, 2 * b).reshape(b, 2, n)
+        else:
+            lifted = torch.empty((b, 2, n), **f)
+            lifted[:, 0] = lifted_h
+            lifted[:, 1] = q._lift_raw(lift_in[:, 1].contiguous(), b)
         effective = torch.empty((b, n), **f)
         v_hartree = torch.empty((b, n), **f)
         terms = torch.empty((b, 3, n), **f)
@@ -517,7 +530,8 @@ class BatchedKohnShamStep:
         sums = row_sums(terms)  # (b, 3)
         node_sum = row_sums(e_w)  # (b,)
         return BatchedPotentials(effective=effective, v_hartree=v_hartree, hartree_energy=0.5 * sums[:, 0],
-                                 xc_energy=node_sum + sums[:, 2], xc_double_counting=sums[:, 1], v_smooth=fields[1])
+                                 xc_energy=node_sum + sums[:, 2], xc_double_counting=sums[:, 1], v_smooth=fields[1],
+                                 node=node, lifted_h=lifted[:, 0])
 
     def hamiltonian(self, effective: torch.Tensor, dtype=torch.float64) -> BatchedHamiltonian:
         return BatchedHamiltonian(self.grid, self.factor, self.quadrature, self.bare_potential[None, :] + effective,
@@ -642,7 +656,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         n_in = n_in.expand(b, -1).contiguous()
     initial_block = None
     previous_effective = None
-    vs_in = None  # v_smooth of n_in, carried by linearity while every mixer is linear
+    lin_in = None  # (v_smooth, node, lifted_h) of n_in, carried by linearity while every mixer is linear
     limit = scf.max_iterations if max_iterations is None else max_iterations
     active = list(range(b))
     last_p_in = [None] * b
@@ -654,8 +668,11 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         sel = torch.tensor(active, dtype=torch.long, device=dev)
         full = len(active) == b
         nin = n_in if full else n_in.index_select(0, sel)
-        vs = None if vs_in is None else (vs_in if full else vs_in.index_select(0, sel))
-        p_in = step.potentials(nin, v_smooth=vs)
+        lin = None
+        if lin_in is not None:
+            lin = lin_in if full else (lin_in[0].index_select(0, sel), lin_in[1].index_select(1, sel),
+                                       lin_in[2].index_select(0, sel))
+        p_in = step.potentials(nin, *(lin or ()))
         h = step.hamiltonian(p_in.effective)
         float_now = [systems[s].float_phase for s in active]
         h32 = step.hamiltonian(p_in.effective, dtype=torch.float32) if any(float_now) else None
@@ -699,11 +716,19 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         # mixing (per system: linear in one batched expression when all are linear)
         n_next = torch.empty_like(nin)
         linear = all(isinstance(systems[s].mixer, LinearMixer) for s in active)
-        vs_next = torch.empty_like(nin) if linear else None
-        for j, s in enumerate(active):
-            n_next[j] = systems[s].mixer.mix(nin[j:j + 1], n_out[j:j + 1], iteration)[0]
-            if linear:  # the same combination of the two Poisson solutions (a stateless mixer)
-                vs_next[j] = systems[s].mixer.mix(p_in.v_smooth[j:j + 1], p_out.v_smooth[j:j + 1], iteration)[0]
+        lin_next = None
+        if linear:
+            # x_in + alpha (x_out - x_in) per system (LinearMixer.mix, element for element) in one expression per
+            # array, for the density and for the linear parts of the two potentials
+            alpha = torch.tensor([systems[s].mixer.alpha for s in active], dtype=torch.float64, device=dev)
+            a2 = alpha[:, None]
+            n_next = nin + a2 * (n_out - nin)
+            lin_next = (p_in.v_smooth + a2 * (p_out.v_smooth - p_in.v_smooth),
+                        p_in.node + alpha[None, :, None] * (p_out.node - p_in.node),
+                        p_in.lifted_h + a2 * (p_out.lifted_h - p_in.lifted_h))
+        else:
+            for j, s in enumerate(active):
+                n_next[j] = systems[s].mixer.mix(nin[j:j + 1], n_out[j:j + 1], iteration)[0]
         new_active = []
         for j, s in enumerate(active):
             st = systems[s]
@@ -735,20 +760,27 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
                 st.worsened = 0
                 st.rung_changed = True
                 n_next[j] = nin[j] + 0.5 * mixing.alpha * residual[j]
-                if vs_next is not None:
-                    vs_next[j] = p_in.v_smooth[j] + 0.5 * mixing.alpha * (p_out.v_smooth[j] - p_in.v_smooth[j])
+                if lin_next is not None:
+                    a = 0.5 * mixing.alpha
+                    lin_next[0][j] = p_in.v_smooth[j] + a * (p_out.v_smooth[j] - p_in.v_smooth[j])
+                    lin_next[1][:, j] = p_in.node[:, j] + a * (p_out.node[:, j] - p_in.node[:, j])
+                    lin_next[2][j] = p_in.lifted_h[j] + a * (p_out.lifted_h[j] - p_in.lifted_h[j])
             new_active.append(s)
         # write back the per-system state of this iteration
         if full:
             n_in = n_next
             previous_effective = p_in.effective
             initial_block = vectors
-            vs_in = vs_next
+            lin_in = lin_next
         else:
             n_in = n_in.index_copy(0, sel, n_next)
             previous_effective = previous_effective.index_copy(0, sel, p_in.effective)
             initial_block = initial_block.index_copy(0, sel, vectors)
-            vs_in = None if (vs_next is None or vs_in is None) else vs_in.index_copy(0, sel, vs_next)
+            if lin_next is None or lin_in is None:
+                lin_in = None
+            else:
+                lin_in = (lin_in[0].index_copy(0, sel, lin_next[0]), lin_in[1].index_copy(1, sel, lin_next[1]),
+                          lin_in[2].index_copy(0, sel, lin_next[2]))
         if previous_effective is None:
             previous_effective = p_in.effective
         active = new_active

@@ -309,18 +309,26 @@ __global__ void __launch_bounds__(256) interpolate_many_kernel(const int* __rest
         const int bx = base[node * 3 + 0] - HALFD, by = base[node * 3 + 1] - HALFD, bz = base[node * 3 + 2] - HALFD;
         const double* w = w1d + node * 24;
         const double wl = w[lane < 24 ? lane : 0];  // the 24 1-D weights, one per lane, then shuffled
+        double wz[KTAP], wy[KTAP];
+#pragma unroll
+        for (int c = 0; c < KTAP; ++c) {
+            wy[c] = __shfl_sync(0xffffffffu, wl, 8 + c);
+            wz[c] = __shfl_sync(0xffffffffu, wl, 16 + c);
+        }
+        // separable contraction: z sums of the 8 rows of each (a, b) are independent chains, then y, then x
         double acc = 0.0;
         for (int a = 0; a < KTAP; ++a) {
-            const double wa = __shfl_sync(0xffffffffu, wl, a);
-            for (int b = 0; b < KTAP; ++b) {
-                const double wab = wa * __shfl_sync(0xffffffffu, wl, 8 + b);
-                const double* row = rows + ((int64_t(bx + a) * ny + (by + b)) * nz + bz) * MANY + lane;
+            const double* plane = rows + (int64_t(bx + a) * ny + by) * int64_t(nz) * MANY + int64_t(bz) * MANY + lane;
+            double sa = 0.0;
 #pragma unroll
-                for (int c = 0; c < KTAP; ++c) {
-                    const double v = wab * __shfl_sync(0xffffffffu, wl, 16 + c);
-                    acc += v * row[c * MANY];
-                }
+            for (int b = 0; b < KTAP; ++b) {
+                const double* row = plane + int64_t(b) * nz * MANY;
+                double t = 0.0;
+#pragma unroll
+                for (int c = 0; c < KTAP; ++c) t = fma(wz[c], row[c * MANY], t);
+                sa = fma(wy[b], t, sa);
             }
+            acc = fma(__shfl_sync(0xffffffffu, wl, a), sa, acc);
         }
         tile[r][lane] = acc;
     }
@@ -440,7 +448,7 @@ __global__ void __launch_bounds__(256) lift_segments_kernel(const long long* __r
     const int r = seg_row[sgi];
     const long long eb0 = row_ptr[r] + (sgi - seg_ptr[r]) * int64_t(kLiftSegment);
     const long long ee = min(row_ptr[r + 1], eb0 + kLiftSegment);
-    double acc = 0.0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};  // four independent chains, added in a fixed order at the end
     for (long long eb = eb0; eb < ee; eb += 32) {
         int node_l = 0;
         double v_l = 0.0;
@@ -455,12 +463,13 @@ __global__ void __launch_bounds__(256) lift_segments_kernel(const long long* __r
 #pragma unroll
             for (int u = 0; u < 8; ++u) g[u] = rows[int64_t(__shfl_sync(0xffffffffu, node_l, k + u)) * MANY + lane];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) acc += g[u] * __shfl_sync(0xffffffffu, v_l, k + u);
+            for (int u = 0; u < 8; ++u) acc[u & 3] = fma(g[u], __shfl_sync(0xffffffffu, v_l, k + u), acc[u & 3]);
         }
         for (; k < count; ++k)
-            acc += rows[int64_t(__shfl_sync(0xffffffffu, node_l, k)) * MANY + lane] * __shfl_sync(0xffffffffu, v_l, k);
+            acc[0] = fma(rows[int64_t(__shfl_sync(0xffffffffu, node_l, k)) * MANY + lane],
+                         __shfl_sync(0xffffffffu, v_l, k), acc[0]);
     }
-    partial[sgi * MANY + lane] = acc;
+    partial[sgi * MANY + lane] = (acc[0] + acc[1]) + (acc[2] + acc[3]);
 }
 
 __global__ void __launch_bounds__(256) lift_segments_sum_kernel(const int* __restrict__ seg_ptr, int64_t n_points,

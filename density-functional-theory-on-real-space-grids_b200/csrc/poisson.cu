@@ -279,8 +279,10 @@ __global__ void kernel_table_kernel(double* __restrict__ out, int n0, int n1, in
 constexpr int kPoissonSmem = 200 * 1024;
 constexpr int kThreads = 256;
 
-// Lines per CTA for transforms of length n: 16 while two [n][17] complex buffers fit, else 8.
-int lines_for(int n) { return size_t(2) * n * 17 * sizeof(cplx) <= size_t(kPoissonSmem) ? 16 : 8; }
+// Lines per CTA for transforms of length n: 8 while two [n][9] complex buffers fit, else 4. (At
+// n = 180, 32 systems: 8 lines 3.0 ms per solve, 16 lines 3.8 ms -- two CTAs per SM instead of
+// four -- and 4 lines 3.9 ms.)
+int lines_for(int n) { return size_t(2) * n * 9 * sizeof(cplx) <= size_t(kPoissonSmem) ? 8 : 4; }
 
 size_t smem_for(int n, int L) { return size_t(2) * n * (L + 1) * sizeof(cplx); }
 
@@ -303,6 +305,7 @@ int configure_lines() {
 int configure_poisson_kernels() {
     int st = configure_lines<16>();
     if (st == CDFTB_OK) st = configure_lines<8>();
+    if (st == CDFTB_OK) st = configure_lines<4>();
     return st;
 }
 
@@ -514,8 +517,10 @@ extern "C" int cdftb_poisson_solve(void* plan, const double* density, double* po
     const int axis_of_pass[6] = {0, 2, 1, 0, 1, 2};
     for (int pass = 1; pass <= 5; ++pass) {
         const int n = p->pad[axis_of_pass[pass]];
-        const int st = lines_for(n) == 16 ? run_passes<16>(p, density, potential, batch, s, pass)
-                                          : run_passes<8>(p, density, potential, batch, s, pass);
+        const int lines = lines_for(n);
+        const int st = lines == 16  ? run_passes<16>(p, density, potential, batch, s, pass)
+                       : lines == 8 ? run_passes<8>(p, density, potential, batch, s, pass)
+                                    : run_passes<4>(p, density, potential, batch, s, pass);
         if (st != CDFTB_OK) return st;
     }
     return CDFTB_OK;

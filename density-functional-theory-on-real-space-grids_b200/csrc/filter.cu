@@ -290,8 +290,12 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
     const int xa = blockIdx.y * a.xchunk;
     const int xe = min(xa + a.xchunk, nx) - 1;
     const int lane = static_cast<int>(a.lane_first) + blockIdx.z;
-    const int q0 = xa - HALO;              // first plane: nodes xa-7 .. xe+7 are read
-    const int npl = xe - xa + 1 + 2 * HALO;  // planes marched
+    // Planes marched: nodes xa-7 .. xe+7. A chunk that starts at the grid's first plane skips the 7
+    // planes before it: phi is zero there (the Dirichlet boundary), and nothing formed at those
+    // planes reaches an output -- the x faces that outputs 0.. need are all formed from plane 0 on,
+    // with the zeroed queues standing for the nodes outside.
+    const int q0 = xa > 0 ? xa - HALO : 0;
+    const int npl = xe + HALO + 1 - q0;
     const bool has_prev = a.has_prev != 0;
 
     // the lane's orbitals (an empty second half borrows the first's group for its lookups)

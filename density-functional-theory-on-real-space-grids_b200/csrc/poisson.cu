@@ -1,5 +1,7 @@
 // (c) The Coulomb-cutoff Poisson solve (src/cdft/operators/poisson.py:21-107) as five pruned
-// axis-wise FFT passes on the device, with the truncated kernel K(G) fused into the x pass.
+// axis-wise FFT passes on the device, with the truncated kernel K(G) fused into the x pass. Passes
+// 2-4 use the four-step register kernels below when the axis length has a factor pair (A, B), the
+// shared-memory Stockham kernels otherwise.
 //
 // The density occupies the first n of the N = fft_friendly(ceil(pad n)) points of every padded
 // axis and only the first n outputs are read back, so each pass transforms only lines that can be
@@ -141,6 +143,188 @@ __device__ cplx* fft_lines(cplx* x, cplx* y, const FftPlan& P, int sign, int lp,
     }
     return x;
 }
+
+// ---------------------------------------------------------------------------------------------
+// Four-step transforms in registers, for line lengths N = A B with A, B in {8, 9, 10, 12, 15, 16,
+// 18, 20}. For n = B n1 + n2 and k = k1 + A k2:
+//   X[k1 + A k2] = sum_n2 W_B^(n2 k2) W_N^(n2 k1) sum_n1 x[B n1 + n2] W_A^(n1 k1),
+// so a thread does one A-point DFT (over n1, fixed n2) and, after an in-place exchange through
+// shared memory, one B-point DFT (over n2, fixed k1), each entirely in registers. The small DFTs
+// are nested radix 2/3/4/5 butterflies with their internal twiddles from a constant table of the
+// 720th roots of unity (every size here divides 720); W_N comes from a per-axis table.
+
+__constant__ cplx kUnit720[720];  // exp(-2 pi i j / 720)
+
+template <int R>
+__device__ __forceinline__ cplx unit_root(int m, int sign) {
+    const cplx w = kUnit720[(m % R) * (720 / R)];
+    return sign < 0 ? w : cplx{w.re, -w.im};
+}
+
+template <int R>
+struct FirstFactor {
+    static constexpr int value = R % 4 == 0 ? 4 : (R % 2 == 0 ? 2 : (R % 3 == 0 ? 3 : 5));
+};
+
+// In-place DFT of R values held in registers (natural order in and out), sign -1 forward.
+template <int R>
+__device__ __forceinline__ void small_dft(cplx* a, int sign) {
+    if constexpr (R == 2 || R == 3 || R == 4 || R == 5) {
+        dft_radix<R>(a, sign);
+    } else {
+        constexpr int P = FirstFactor<R>::value;
+        constexpr int Q = R / P;
+        static_assert(P * Q == R && 720 % R == 0, "small DFT sizes divide 720");
+        cplx b[R];
+#pragma unroll
+        for (int n2 = 0; n2 < Q; ++n2) {
+            cplx c[P];
+#pragma unroll
+            for (int n1 = 0; n1 < P; ++n1) c[n1] = a[Q * n1 + n2];
+            small_dft<P>(c, sign);
+#pragma unroll
+            for (int k1 = 0; k1 < P; ++k1) b[k1 * Q + n2] = (n2 * k1 == 0) ? c[k1] : cmul(c[k1], unit_root<R>(n2 * k1, sign));
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < P; ++k1) {
+            cplx c[Q];
+#pragma unroll
+            for (int n2 = 0; n2 < Q; ++n2) c[n2] = b[k1 * Q + n2];
+            small_dft<Q>(c, sign);
+#pragma unroll
+            for (int k2 = 0; k2 < Q; ++k2) a[k1 + P * k2] = c[k2];
+        }
+    }
+}
+
+constexpr int kLines4 = 8;     // lines per CTA of the four-step kernels
+constexpr int kThreads4 = 128;
+
+// Step 1 of a forward (sign -1) or inverse (+1) transform of the L lines in buf ([N][L+1]): per
+// (line, n2), the A-point DFT over n1 of x[B n1 + n2], times W_N^(+-n2 k1), back in place.
+template <int A, int B>
+__device__ __forceinline__ void fourstep_first(cplx* buf, const cplx* __restrict__ twn, int sign) {
+    constexpr int N = A * B, L = kLines4, LP = L + 1;
+    for (int task = threadIdx.x; task < B * L; task += kThreads4) {
+        const int line = task % L, n2 = task / L;
+        cplx v[A];
+#pragma unroll
+        for (int n1 = 0; n1 < A; ++n1) v[n1] = buf[(B * n1 + n2) * LP + line];
+        small_dft<A>(v, sign);
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) {
+            const cplx w = twn[(n2 * k1) % N];
+            buf[(B * k1 + n2) * LP + line] = sign < 0 ? cmul(v[k1], w) : cmulc(v[k1], w);
+        }
+    }
+}
+
+// Pass 3, four-step: the x lines of one system ([nx][inner]) -- forward, times K, inverse -- with
+// the K multiply and the first inverse step on the registers of the second forward step.
+template <int A, int B>
+__global__ void __launch_bounds__(kThreads4) fft_x_fourstep_kernel(cplx* __restrict__ data, int nx, int64_t inner,
+                                                                  const double* __restrict__ kernel,
+                                                                  const cplx* __restrict__ twn) {
+    constexpr int N = A * B, L = kLines4, LP = L + 1;
+    __shared__ cplx buf[N * LP];
+    const int64_t c0 = int64_t(blockIdx.x) * L;
+    cplx* col = data + int64_t(blockIdx.y) * nx * inner + c0;
+    for (int idx = threadIdx.x; idx < N * L; idx += kThreads4) {
+        const int line = idx % L, x = idx / L;
+        buf[x * LP + line] = (x < nx && c0 + line < inner) ? col[int64_t(x) * inner + line] : cplx{0.0, 0.0};
+    }
+    __syncthreads();
+    fourstep_first<A, B>(buf, twn, -1);
+    __syncthreads();
+    for (int task = threadIdx.x; task < A * L; task += kThreads4) {
+        const int line = task % L, k1 = task / L;
+        const bool live = c0 + line < inner;
+        cplx v[B];
+#pragma unroll
+        for (int n2 = 0; n2 < B; ++n2) v[n2] = buf[(B * k1 + n2) * LP + line];
+        small_dft<B>(v, -1);  // X[k1 + A k2] = v[k2]
+#pragma unroll
+        for (int k2 = 0; k2 < B; ++k2)
+            v[k2] = scale(v[k2], live ? kernel[int64_t(k1 + A * k2) * inner + c0 + line] : 0.0);
+        small_dft<B>(v, +1);  // inverse, first step: Z[k1][n2] = v[n2]
+#pragma unroll
+        for (int n2 = 0; n2 < B; ++n2) buf[(B * k1 + n2) * LP + line] = cmulc(v[n2], twn[(n2 * k1) % N]);
+    }
+    __syncthreads();
+    for (int task = threadIdx.x; task < B * L; task += kThreads4) {
+        const int line = task % L, n2 = task / L;
+        cplx v[A];
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) v[k1] = buf[(B * k1 + n2) * LP + line];
+        small_dft<A>(v, +1);
+        if (c0 + line < inner) {
+#pragma unroll
+            for (int n1 = 0; n1 < A; ++n1) {
+                const int x = B * n1 + n2;
+                if (x < nx) col[int64_t(x) * inner + line] = v[n1];
+            }
+        }
+    }
+}
+
+// Passes 2 and 4, four-step: middle-axis lines of [outer][n][inner]; reads n_in elements per line
+// (zero beyond), transforms (sign), writes the first n_out.
+template <int A, int B>
+__global__ void __launch_bounds__(kThreads4) fft_middle_fourstep_kernel(const cplx* __restrict__ in,
+                                                                       int64_t in_outer_stride, int n_in,
+                                                                       cplx* __restrict__ out,
+                                                                       int64_t out_outer_stride, int n_out,
+                                                                       int64_t inner, const cplx* __restrict__ twn,
+                                                                       int sign) {
+    constexpr int N = A * B, L = kLines4, LP = L + 1;
+    __shared__ cplx buf[N * LP];
+    const int64_t o = blockIdx.x;
+    const int64_t c0 = int64_t(blockIdx.y) * L;
+    const cplx* src = in + o * in_outer_stride + c0;
+    for (int idx = threadIdx.x; idx < N * L; idx += kThreads4) {
+        const int line = idx % L, j = idx / L;
+        buf[j * LP + line] = (j < n_in && c0 + line < inner) ? src[int64_t(j) * inner + line] : cplx{0.0, 0.0};
+    }
+    __syncthreads();
+    fourstep_first<A, B>(buf, twn, sign);
+    __syncthreads();
+    cplx* dst = out + o * out_outer_stride + c0;
+    for (int task = threadIdx.x; task < A * L; task += kThreads4) {
+        const int line = task % L, k1 = task / L;
+        cplx v[B];
+#pragma unroll
+        for (int n2 = 0; n2 < B; ++n2) v[n2] = buf[(B * k1 + n2) * LP + line];
+        small_dft<B>(v, sign);
+        if (c0 + line < inner) {
+#pragma unroll
+            for (int k2 = 0; k2 < B; ++k2) {
+                const int k = k1 + A * k2;
+                if (k < n_out) dst[int64_t(k) * inner + line] = v[k2];
+            }
+        }
+    }
+}
+
+// The factor pair (A, B) of a length the four-step kernels take, A * B = n; false otherwise.
+bool fourstep_pair(int n, int* a, int* b) {
+    static const int pairs[][3] = {{64, 8, 8},     {72, 8, 9},     {80, 8, 10},   {90, 9, 10},    {96, 8, 12},
+                                   {100, 10, 10},  {108, 9, 12},   {120, 10, 12}, {128, 8, 16},   {135, 9, 15},
+                                   {144, 12, 12},  {150, 10, 15},  {160, 10, 16}, {162, 9, 18},   {180, 12, 15},
+                                   {192, 12, 16},  {200, 10, 20},  {216, 12, 18}, {225, 15, 15},  {240, 15, 16},
+                                   {256, 16, 16},  {270, 15, 18},  {288, 16, 18}, {300, 15, 20},  {320, 16, 20}};
+    for (const auto& q : pairs)
+        if (q[0] == n) {
+            *a = q[1];
+            *b = q[2];
+            return true;
+        }
+    return false;
+}
+
+#define CDFTB_FOURSTEP_PAIRS(X)                                                                                    \
+    X(8, 8) X(8, 9) X(8, 10) X(9, 10) X(8, 12) X(10, 10) X(9, 12) X(10, 12) X(8, 16) X(9, 15) X(12, 12) X(10, 15) \
+        X(10, 16) X(9, 18) X(12, 15) X(12, 16) X(10, 20) X(12, 18) X(15, 15) X(15, 16) X(16, 16) X(15, 18)        \
+            X(16, 18) X(15, 20) X(16, 20)
 
 // Pass 1: z lines (contiguous, nz real values zero-padded to N) -> half spectrum kz < nk.
 template <int L>
@@ -372,6 +556,35 @@ bool make_fft_plan(int n, FftPlan* plan, cplx** device_tw) {
     return true;
 }
 
+// exp(-2 pi i j / n) for j < n on the device (the angle reduced exactly in integers first).
+bool make_root_table(int n, cplx** device) {
+    cplx* host = new cplx[n];
+    for (int j = 0; j < n; ++j) {
+        const double t = -2.0 * 3.14159265358979323846 * static_cast<double>(j) / static_cast<double>(n);
+        host[j] = {cos(t), sin(t)};
+    }
+    cplx* dev = nullptr;
+    const bool ok = cudaMalloc(&dev, sizeof(cplx) * n) == cudaSuccess &&
+                    cudaMemcpy(dev, host, sizeof(cplx) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+    delete[] host;
+    if (!ok) {
+        cudaFree(dev);
+        return false;
+    }
+    *device = dev;
+    return true;
+}
+
+// The small-DFT roots of unity in constant memory (this device's copy of the module).
+int load_unit_roots() {
+    cplx host[720];
+    for (int j = 0; j < 720; ++j) {
+        const double t = -2.0 * 3.14159265358979323846 * static_cast<double>(j) / 720.0;
+        host[j] = {cos(t), sin(t)};
+    }
+    return check(cudaMemcpyToSymbol(kUnit720, host, sizeof(host)));
+}
+
 }  // namespace
 
 }  // namespace cdftb
@@ -388,6 +601,8 @@ struct cdftb_poisson_plan {
     double* kernel;  // [pad0][pad1][nk]
     FftPlan fft[3];
     cplx* tw[3];
+    cplx* twn[3];  // W_N^j, j < pad[d] (the four-step kernels' outer twiddles)
+    int four[3][2];  // the four-step factor pair of each axis, {0, 0} if its length has none
     cplx* a;  // [batch][n0][n1][nk]
     cplx* b;  // [batch][n0][pad1][nk]
     int max_batch;
@@ -396,6 +611,7 @@ struct cdftb_poisson_plan {
 static void free_plan(cdftb_poisson_plan* p) {
     cudaFree(p->kernel);
     for (int d = 0; d < 3; ++d) cudaFree(p->tw[d]);
+    for (int d = 0; d < 3; ++d) cudaFree(p->twn[d]);
     cudaFree(p->a);
     cudaFree(p->b);
     delete p;
@@ -430,6 +646,14 @@ extern "C" int cdftb_poisson_plan_create(int nx, int ny, int nz, double spacing,
     st = check(cudaMalloc(&p->kernel, nkern * sizeof(double)));
     for (int d = 0; d < 3 && st == CDFTB_OK; ++d)
         if (!make_fft_plan(p->pad[d], &p->fft[d], &p->tw[d])) st = CDFTB_ERR_LAUNCH;
+    for (int d = 0; d < 3 && st == CDFTB_OK; ++d) {
+        if (!fourstep_pair(p->pad[d], &p->four[d][0], &p->four[d][1])) {
+            p->four[d][0] = p->four[d][1] = 0;
+            continue;
+        }
+        if (!make_root_table(p->pad[d], &p->twn[d])) st = CDFTB_ERR_LAUNCH;
+    }
+    if (st == CDFTB_OK) st = load_unit_roots();
     if (st == CDFTB_OK)
         st = check(cudaMalloc(&p->a, static_cast<int64_t>(max_batch) * nx * ny * p->nk * sizeof(cplx)));
     if (st == CDFTB_OK)
@@ -506,6 +730,44 @@ int run_passes(cdftb_poisson_plan* p, const double* density, double* potential, 
     return check_launch();
 }
 
+// Passes 2-4 with the four-step kernels (the axis length has a factor pair).
+int run_fourstep(cdftb_poisson_plan* p, int batch, cudaStream_t s, int pass) {
+    const int nx = p->n[0], ny = p->n[1];
+    const int N1 = p->pad[1], nk = p->nk;
+    const int d = pass == 3 ? 0 : 1;
+    const int A = p->four[d][0], B = p->four[d][1];
+    const dim3 blk(kThreads4);
+    if (pass == 3) {
+        const int64_t inner = static_cast<int64_t>(N1) * nk;
+        const dim3 grid(static_cast<unsigned>(ceil_div(inner, kLines4)), static_cast<unsigned>(batch));
+#define CDFTB_X4(A_, B_)                                                                                     \
+    if (A == A_ && B == B_) {                                                                                \
+        fft_x_fourstep_kernel<A_, B_><<<grid, blk, 0, s>>>(p->b, nx, inner, p->kernel, p->twn[0]);           \
+        return check_launch();                                                                               \
+    }
+        CDFTB_FOURSTEP_PAIRS(CDFTB_X4)
+#undef CDFTB_X4
+        return CDFTB_ERR_ARGUMENT;
+    }
+    const dim3 grid(static_cast<unsigned>(batch * nx), static_cast<unsigned>(ceil_div(nk, kLines4)));
+    const cplx* in = pass == 2 ? p->a : p->b;
+    cplx* out = pass == 2 ? p->b : p->a;
+    const int64_t in_stride = pass == 2 ? static_cast<int64_t>(ny) * nk : static_cast<int64_t>(N1) * nk;
+    const int64_t out_stride = pass == 2 ? static_cast<int64_t>(N1) * nk : static_cast<int64_t>(ny) * nk;
+    const int n_in = pass == 2 ? ny : N1;
+    const int n_out = pass == 2 ? N1 : ny;
+    const int sign = pass == 2 ? -1 : +1;
+#define CDFTB_M4(A_, B_)                                                                                      \
+    if (A == A_ && B == B_) {                                                                                 \
+        fft_middle_fourstep_kernel<A_, B_><<<grid, blk, 0, s>>>(in, in_stride, n_in, out, out_stride, n_out, nk, \
+                                                                p->twn[1], sign);                             \
+        return check_launch();                                                                                \
+    }
+    CDFTB_FOURSTEP_PAIRS(CDFTB_M4)
+#undef CDFTB_M4
+    return CDFTB_ERR_ARGUMENT;
+}
+
 }  // namespace
 
 extern "C" int cdftb_poisson_solve(void* plan, const double* density, double* potential, int batch,
@@ -516,6 +778,11 @@ extern "C" int cdftb_poisson_solve(void* plan, const double* density, double* po
     cudaStream_t s = as_stream(stream);
     const int axis_of_pass[6] = {0, 2, 1, 0, 1, 2};
     for (int pass = 1; pass <= 5; ++pass) {
+        if (pass >= 2 && pass <= 4 && p->four[axis_of_pass[pass]][0] != 0) {
+            const int st = run_fourstep(p, batch, s, pass);
+            if (st != CDFTB_OK) return st;
+            continue;
+        }
         const int n = p->pad[axis_of_pass[pass]];
         const int lines = lines_for(n);
         const int st = lines == 16  ? run_passes<16>(p, density, potential, batch, s, pass)

@@ -229,6 +229,7 @@ __global__ void __launch_bounds__(kThreads4) fft_x_fourstep_kernel(cplx* __restr
     __shared__ cplx buf[N * LP];
     const int64_t c0 = int64_t(blockIdx.x) * L;
     cplx* col = data + int64_t(blockIdx.y) * nx * inner + c0;
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < N * L; idx += kThreads4) {
         const int line = idx % L, x = idx / L;
         buf[x * LP + line] = (x < nx && c0 + line < inner) ? col[int64_t(x) * inner + line] : cplx{0.0, 0.0};
@@ -281,6 +282,7 @@ __global__ void __launch_bounds__(kThreads4) fft_middle_fourstep_kernel(const cp
     const int64_t o = blockIdx.x;
     const int64_t c0 = int64_t(blockIdx.y) * L;
     const cplx* src = in + o * in_outer_stride + c0;
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < N * L; idx += kThreads4) {
         const int line = idx % L, j = idx / L;
         buf[j * LP + line] = (j < n_in && c0 + line < inner) ? src[int64_t(j) * inner + line] : cplx{0.0, 0.0};

@@ -128,7 +128,7 @@ def _profile_traffic(kernel_tag: str):
     for line in path.read_text().splitlines():
         if line.startswith(f"traffic_bytes_per_launch[{kernel_tag}]"):
             try:
-                return float(line.split("=", 1)[1].strip())
+                return float(line.rsplit("=", 1)[1].strip())
             except ValueError:
                 return None
     return None

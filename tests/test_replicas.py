@@ -60,3 +60,13 @@ def test_single_process_helpers():
     assert bench.replica_seeds(0, 3) == [0, 1, 2]
     assert bench.max_over_ranks(1.25, None, None) == 1.25
     assert bench.whole_job_rate(1, 32, 3, 2.0) == pytest.approx(48.0)
+
+
+def test_profile_traffic_reads_the_committed_summary():
+    """The bench's roofline traffic comes from the committed ncu summary (keys hold an '=' themselves)."""
+    import bench
+
+    for key in ("f32,batch=32", "f32,batch=8", "f64,batch=1"):
+        value = bench._profile_traffic(key)
+        assert value is not None and value > 1e6, key
+    assert bench._profile_traffic("f32,batch=7") is None

@@ -72,6 +72,8 @@ SIGNATURES: dict[str, tuple] = {
                                          c_void_p]),
     "cdftb_cast": (c_int, [c_void_p, c_int, c_void_p, c_int, c_int64, c_void_p]),
     "cdftb_stencil_set_tile": (c_int, [c_int, c_int, c_int]),
+    "cdftb_filter_autotune": (c_int, [c_int]),
+    "cdftb_filter_tuned_tile": (c_int, [c_int, c_int, c_int, c_int, c_int64, c_void_p, c_void_p]),
     "cdftb_poisson_plan_create": (c_int, [c_int, c_int, c_int, c_double, c_double, c_int, ctypes.POINTER(c_void_p),
                                           ctypes.POINTER(c_int), ctypes.POINTER(c_double)]),
     "cdftb_poisson_plan_destroy": (c_int, [c_void_p]),
@@ -157,6 +159,9 @@ def library() -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = restype
         fn.argtypes = argtypes
+    # The slab kernels' tiling is tuned on first use per grid shape and lane count (the first filter
+    # call for a shape times the candidates and synchronises; results do not depend on the tiling).
+    lib.cdftb_filter_autotune(0 if os.environ.get("CDFTB_AUTOTUNE", "1") == "0" else 1)
     _LIB = lib
     return lib
 

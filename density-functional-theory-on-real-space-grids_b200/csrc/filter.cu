@@ -31,6 +31,9 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "common.cuh"
 
@@ -728,7 +731,7 @@ int sm_count() {
 }
 
 template <typename Lane, int TZ>
-int launch_slab(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream) {
+int launch_slab(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
     using SH = Shape<TZ, sizeof(typename Lane::S)>;
     static bool configured = false;
     if (!configured) {
@@ -740,7 +743,7 @@ int launch_slab(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_
     const int tiles_y = static_cast<int>(ceil_div(a.ny, TY));
     a.tiles_z = static_cast<int>(ceil_div(a.nzp, TZ));
     const int64_t tiles = int64_t(tiles_y) * a.tiles_z;
-    a.xchunk = choose_chunk(a.nx, tiles * lanes, sm_count());
+    a.xchunk = xchunk > 0 ? (xchunk < a.nx ? xchunk : a.nx) : choose_chunk(a.nx, tiles * lanes, sm_count());
     const int chunks = static_cast<int>(ceil_div(a.nx, a.xchunk));
     static unsigned next_token = 0;
     for (int64_t first = 0; first < lanes; first += 65535) {
@@ -854,8 +857,97 @@ FilterArgs base_args(const cdftb_operator* op, int64_t batch) {
 }
 
 template <typename Lane>
-int launch_any_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lanes, cudaStream_t stream) {
-    return tz == 36 ? launch_slab<Lane, 36>(m, a, lanes, stream) : launch_slab<Lane, 32>(m, a, lanes, stream);
+int launch_any_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lanes, cudaStream_t stream,
+                  int xchunk = 0) {
+    return tz == 36 ? launch_slab<Lane, 36>(m, a, lanes, stream, xchunk)
+                    : launch_slab<Lane, 32>(m, a, lanes, stream, xchunk);
+}
+
+// ---- the tile autotuner
+// The z tile (32 or 36 columns) and the x chunk of a slab launch decide the CTA count, the waves
+// and the halo work; which wins depends on the grid, the lane count and the GPU. With the autotuner
+// on, the first filter call for a (device, grid, precision, lanes) key times every candidate on the
+// call's own buffers (the first Chebyshev step, which the real run then recomputes), keeps the
+// fastest in a host table, and every later filter or apply launch for that key uses it. Every
+// candidate gives bit-identical results: each output is formed by the same arithmetic in the same
+// order whatever the tiling. Off, the heuristics choose_tz / choose_chunk decide.
+struct TileChoice {
+    int tz;
+    int xchunk;  // 0: choose_chunk
+};
+
+using TuneKey = std::tuple<int, int, int, int, int, int64_t>;  // device, nx, ny, nz, precision, lanes
+std::mutex g_tune_mutex;
+std::map<TuneKey, TileChoice> g_tuned;
+bool g_autotune = false;
+
+TuneKey tune_key(const cdftb_operator* op, int64_t lanes) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return TuneKey(dev, op->nx, op->ny, op->nz, op->dtype, lanes);
+}
+
+bool tuned_choice(const TuneKey& key, TileChoice* out) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tuned.find(key);
+    if (it == g_tuned.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+// Times the first Chebyshev step (packed block in buf[2] -> buf[0]) for every candidate tiling:
+// one untimed launch, then three timed ones per candidate. Synchronises the stream.
+template <typename Lane>
+int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf[3], int64_t lanes,
+              const double* coefficients, int degree, cudaStream_t stream, TileChoice* best) {
+    const int nx = op->nx, ny = op->ny, nzp = padded_z(op->nz);
+    cudaEvent_t e0, e1;
+    int st = check(cudaEventCreate(&e0));
+    if (st != CDFTB_OK) return st;
+    if ((st = check(cudaEventCreate(&e1))) != CDFTB_OK) {
+        cudaEventDestroy(e0);
+        return st;
+    }
+    float best_ms = -1.0f;
+    *best = TileChoice{choose_tz(nzp), 0};
+    for (int tz : {32, 36}) {
+        FilterMaps m{};
+        if ((st = prepare_geometry<Lane>(op, batch, geo_base, tz, false, &m, stream)) != CDFTB_OK) break;
+        if ((st = encode_lane_maps(buf[2], nzp, ny, nx, lanes, tz, &m.phi, &m.prev)) != CDFTB_OK) break;
+        FilterArgs a = base_args(op, batch);
+        a.coef = coefficients;
+        a.degree = degree;
+        a.step = 0;
+        a.has_prev = 0;
+        a.final_out = 0;
+        a.out = buf[0];
+        a.out_dtype = 0;
+        const int64_t tiles = int64_t(ceil_div(ny, TY)) * ceil_div(nzp, tz);
+        int chunks_list[5] = {1, 2, 3, 4, 0};
+        chunks_list[4] = static_cast<int>(ceil_div(nx, choose_chunk(nx, tiles * lanes, sm_count())));
+        for (int c = 0; c < 5 && st == CDFTB_OK; ++c) {
+            const int chunks = chunks_list[c];
+            if (chunks < 1 || (c == 4 && chunks <= 4)) continue;  // the heuristic's chunk, when not already tried
+            const int xchunk = static_cast<int>(ceil_div(nx, chunks));
+            if (chunks > 1 && (xchunk < 8 || ceil_div(nx, xchunk) != chunks)) continue;
+            if ((st = launch_any_tz<Lane>(tz, m, a, lanes, stream, xchunk)) != CDFTB_OK) break;
+            if ((st = check(cudaEventRecord(e0, stream))) != CDFTB_OK) break;
+            for (int r = 0; r < 3 && st == CDFTB_OK; ++r) st = launch_any_tz<Lane>(tz, m, a, lanes, stream, xchunk);
+            if (st != CDFTB_OK) break;
+            if ((st = check(cudaEventRecord(e1, stream))) != CDFTB_OK) break;
+            if ((st = check(cudaEventSynchronize(e1))) != CDFTB_OK) break;
+            float ms = 0.0f;
+            if ((st = check(cudaEventElapsedTime(&ms, e0, e1))) != CDFTB_OK) break;
+            if (best_ms < 0.0f || ms < best_ms) {
+                best_ms = ms;
+                *best = TileChoice{tz, xchunk};
+            }
+        }
+        if (st != CDFTB_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st;
 }
 
 template <typename Lane>
@@ -867,9 +959,23 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
     const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
     char* w = static_cast<char*>(work);
     void* buf[3] = {w, w + lanes * lane_bytes, w + 2 * lanes * lane_bytes};
-    const int tz = choose_tz(nzp);
     int st = pack_block<Lane>(op, block, in_dtype, batch, nx, ny, nz, nzp, lanes, buf[2], stream);
     if (st != CDFTB_OK) return st;
+    TileChoice choice{choose_tz(nzp), 0};
+    const TuneKey key = tune_key(op, lanes);
+    bool autotune;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        autotune = g_autotune;
+    }
+    if (!tuned_choice(key, &choice) && autotune) {
+        if ((st = tune_slab<Lane>(op, batch, w + 3 * lanes * lane_bytes, buf, lanes, coefficients, degree, stream,
+                                  &choice)) != CDFTB_OK)
+            return st;
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned[key] = choice;
+    }
+    const int tz = choice.tz;
     FilterMaps geo_maps{};
     if ((st = prepare_geometry<Lane>(op, batch, w + 3 * lanes * lane_bytes, tz, false, &geo_maps, stream)) != CDFTB_OK)
         return st;
@@ -892,7 +998,7 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
         FilterMaps m = geo_maps;
         m.phi = maps[y].phi;
         m.prev = maps[prev >= 0 ? prev : y].prev;
-        if ((st = launch_any_tz<Lane>(tz, m, a, lanes, stream)) != CDFTB_OK) return st;
+        if ((st = launch_any_tz<Lane>(tz, m, a, lanes, stream, choice.xchunk)) != CDFTB_OK) return st;
         prev = y;
         y = dst;
     }
@@ -907,7 +1013,9 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
     const int64_t lanes = lanes_of(op, batch);
     const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
     char* w = static_cast<char*>(work);
-    const int tz = choose_tz(nzp);
+    TileChoice choice{choose_tz(nzp), 0};
+    tuned_choice(tune_key(op, lanes), &choice);
+    const int tz = choice.tz;
     int st = pack_block<Lane>(op, phi, in_dtype, batch, nx, ny, nz, nzp, lanes, w, stream);
     if (st != CDFTB_OK) return st;
     FilterMaps m{};
@@ -922,7 +1030,7 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
     a.final_out = 1;
     a.out = out;
     a.out_dtype = out_dtype;
-    return launch_any_tz<Lane>(tz, m, a, lanes, stream);
+    return launch_any_tz<Lane>(tz, m, a, lanes, stream, choice.xchunk);
 }
 
 }  // namespace
@@ -950,6 +1058,28 @@ int slab_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dt
 }
 
 }  // namespace cdftb
+
+extern "C" int cdftb_filter_autotune(int enable) {
+    std::lock_guard<std::mutex> lock(cdftb::g_tune_mutex);
+    cdftb::g_autotune = enable != 0;
+    return CDFTB_OK;
+}
+
+extern "C" int cdftb_filter_tuned_tile(int nx, int ny, int nz, int dtype, int64_t lanes, int* tile_z, int* x_chunk) {
+    if (!tile_z || !x_chunk || nx <= 0 || ny <= 0 || nz <= 0 || lanes <= 0) return CDFTB_ERR_ARGUMENT;
+    int dev = 0;
+    int st = cdftb::check(cudaGetDevice(&dev));
+    if (st != CDFTB_OK) return st;
+    cdftb::TileChoice c{};
+    if (!cdftb::tuned_choice(cdftb::TuneKey(dev, nx, ny, nz, dtype, lanes), &c)) {
+        *tile_z = 0;
+        *x_chunk = 0;
+        return CDFTB_OK;
+    }
+    *tile_z = c.tz;
+    *x_chunk = c.xchunk;
+    return CDFTB_OK;
+}
 
 extern "C" int cdftb_device_status(int* flags) {
     if (!flags) return CDFTB_ERR_ARGUMENT;

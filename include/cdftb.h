@@ -100,6 +100,19 @@ int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_d
                            void* work, int64_t work_bytes, int64_t batch, const double* coefficients, int degree,
                            cdftb_stream_t stream);
 
+/* No reference counterpart (the reference has no kernels of its own to tune): the tile autotuner of
+ * the order-8 slab kernels. With it enabled, the first cdftb_chebyshev_filter call for a (device,
+ * grid, precision, lane count) key times each candidate tiling -- z tiles of 32 or 36 columns, 1 to
+ * 4 x chunks and the heuristic's chunk -- on that call's own buffers, keeps the fastest, and every
+ * later filter or apply launch for the key uses it. That first call synchronises its stream (make
+ * it before any stream capture); results are bit-identical whatever the tiling. Disabled (the
+ * default in the C library), heuristics choose the tiling. cdftb_filter_tuned_tile reports the
+ * table's entry for a key (tile_z 32 or 36, x_chunk in planes; both 0 when the key is not tuned);
+ * dtype is CDFTB_F32 or CDFTB_F64 and lanes is the launch's lane count (cdftb_operator orbitals in
+ * pairs for float32, one each for float64). */
+int cdftb_filter_autotune(int enable);
+int cdftb_filter_tuned_tile(int nx, int ny, int nz, int dtype, int64_t lanes, int* tile_z, int* x_chunk);
+
 /* No reference counterpart: the error flags the library's kernels set on the device (bit 0: a
  * bounded wait on a TMA barrier gave up). Synchronises the device, returns the flags in *flags and
  * clears them; status CDFTB_ERR_TIMEOUT when any flag was set. */

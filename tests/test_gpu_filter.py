@@ -127,3 +127,35 @@ def test_filter_work_bytes_is_checked(pkg, cuda):
     status = lib.cdftb_chebyshev_filter(ctypes.byref(op), block.data_ptr(), 0, out.data_ptr(), 0, work.data_ptr(),
                                         need - 8, 3, table.data_ptr(), 2, None)
     assert status == 1  # CDFTB_ERR_ARGUMENT: the work buffer is too small
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_autotuned_tiling_is_bit_identical(pkg, cuda, dtype):
+    """The tile autotuner only changes the tiling: its choice gives the heuristic's result bit for bit.
+
+    The shape is used by no other test, so its first call with the autotuner off runs the heuristic
+    tiling and leaves no table entry; the next call, with it on, times the candidates and keeps one.
+    """
+    shape = (37, 23, 71) if dtype == torch.float64 else (35, 21, 69)
+    faces, inv, q = _random_operator(shape, seed=11)
+    pot = np.random.default_rng(12).standard_normal(int(np.prod(shape)))
+    _, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot, dtype=dtype)
+    block = _t(np.random.default_rng(13).standard_normal((5, int(np.prod(shape)))), cuda)
+    lib = pkg._lib.library()
+    code = 1 if dtype == torch.float32 else 0  # CDFTB_F32 / CDFTB_F64
+    lanes = 3 if dtype == torch.float32 else 5
+    tz, xc = ctypes.c_int(-1), ctypes.c_int(-1)
+    try:
+        lib.cdftb_filter_autotune(0)
+        heuristic = pkg.chebyshev_filter(ham, block, 6, 0.5, 3.0, -1.0)
+        assert lib.cdftb_filter_tuned_tile(*shape, code, lanes, ctypes.byref(tz), ctypes.byref(xc)) == 0
+        assert (tz.value, xc.value) == (0, 0)
+        lib.cdftb_filter_autotune(1)
+        tuned = pkg.chebyshev_filter(ham, block, 6, 0.5, 3.0, -1.0)
+        assert lib.cdftb_filter_tuned_tile(*shape, code, lanes, ctypes.byref(tz), ctypes.byref(xc)) == 0
+        assert tz.value in (32, 36) and 1 <= xc.value <= shape[0]
+        again = pkg.chebyshev_filter(ham, block, 6, 0.5, 3.0, -1.0)
+    finally:
+        lib.cdftb_filter_autotune(1)
+    assert torch.equal(tuned, heuristic) and torch.equal(again, heuristic)
+    assert _device_status(pkg) == (0, 0)

@@ -51,8 +51,9 @@ def _args():
                    help="time only the fused Chebyshev step on a He grid of --edge points (for profiling)")
     p.add_argument("--breakdown", action="store_true",
                    help="device time per kernel of one solve (torch.profiler, no replay) instead of the bench line")
-    p.add_argument("--workload", choices=("he-lda", "h2plus-scan"), default="he-lda",
-                   help="he-lda: the headline He-LDA 65^3 solve; h2plus-scan: the 48-system bond scan")
+    p.add_argument("--workload", choices=("he-lda", "h2plus-scan", "adjoint"), default="he-lda",
+                   help="he-lda: the headline He-LDA 65^3 solve; h2plus-scan: the 48-system bond scan; "
+                        "adjoint: energy gradients of He-LDA at h 0.16 (101^3) against central differences")
     p.add_argument("--edge", type=int, default=65)
     p.add_argument("--orbitals", type=int, default=5)
     return p.parse_args()
@@ -220,6 +221,79 @@ def run_kernel_only(args) -> None:
                       "orbitals": args.orbitals, "form": args.form, "us_per_launch": per_launch_s * 1e6,
                       "algorithmic_bytes": algorithmic, "achieved_gbs": achieved, "peak_gbs": peak,
                       "peak_kind": kind, "frac": achieved / peak}), flush=True)
+
+
+def run_adjoint(args) -> None:
+    """Energy gradients of He-LDA at h = 0.16 (box 16 bohr, 101^3), float64, against central differences.
+
+    The gradient with respect to the seeded Gaussian external perturbation (8 centres, widths
+    U[0.5, 1.5] bohr) is the Hellmann--Feynman expectation value at the converged density (one SCF
+    solve and 8 quadratures); it is checked against central differences of tightly converged total
+    energies (step 1e-4 Ha, 16 more solves). The nuclear gradient is taken by central differences
+    (step 1e-4 bohr, 6 solves) on the fixed grid. One JSON line: timings and the agreement.
+    """
+    import torch
+
+    import __graft_entry__
+    from oracle import scf as oscf  # the system definition only
+
+    pkg = __graft_entry__.package()
+    dev = torch.device("cuda:0")
+    system = oscf.he_lda(spacing=0.16, edge=16.0)
+    grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev)
+    geo = pkg.build_cusp_geometry(grid, system.charges, system.positions)
+    scf = pkg.SCFConfig(energy_tol=1e-11, density_tol=1e-8, max_iterations=400)
+    mixing = pkg.MixingConfig(scheme="linear", alpha=0.3)
+
+    def solve(step):
+        out = pkg.solve_self_consistent(step, mixing, scf)
+        if not out.converged:
+            raise RuntimeError("an SCF solve of the adjoint workload did not converge")
+        return out
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - t
+
+    centres, widths, _ = pkg.adjoint.seeded_gaussians()
+    base, t_scf = timed(lambda: solve(pkg.KohnShamStep(geo, "lda_vwn", system.n_electrons)))
+
+    def gradient():
+        g_node, g_grid = pkg.adjoint.perturbation_fields(geo, centres, widths)
+        return pkg.adjoint.external_potential_gradient(geo, base.density, g_node, g_grid).cpu().numpy()
+
+    grad, t_grad = timed(gradient)
+    g_node, g_grid = pkg.adjoint.perturbation_fields(geo, centres, widths)
+    dv = pkg.adjoint.effective_perturbation(geo, g_node, g_grid)
+    step = 1.0e-4
+    fd = []
+    t0 = time.perf_counter()
+    for k in range(dv.shape[0]):
+        e = [float(solve(pkg.KohnShamStep(geo, "lda_vwn", system.n_electrons,
+                                          external_potential=sign * step * dv[k])).energies["total"])
+             for sign in (+1, -1)]
+        fd.append((e[0] - e[1]) / (2 * step))
+    t_fd = time.perf_counter() - t0
+    rel = [abs(f - g) / abs(g) for f, g in zip(fd, grad)]
+
+    def energy_at(positions):
+        moved = pkg.build_cusp_geometry(grid, system.charges, [tuple(p) for p in positions])
+        return float(solve(pkg.KohnShamStep(moved, "lda_vwn", system.n_electrons)).energies["total"])
+
+    t0 = time.perf_counter()
+    nuclear = pkg.adjoint.nuclear_gradient(energy_at, system.positions, delta=1.0e-4)
+    t_nuc = time.perf_counter() - t0
+    print(json.dumps({
+        "workload": "adjoint: He-LDA h 0.16, box 16 bohr (101^3), float64; 8 seeded Gaussian perturbations",
+        "energy_ha": float(base.energies["total"]), "scf_iterations": base.scf_iterations,
+        "scf_seconds": t_scf, "gradient_seconds_after_scf": t_grad,
+        "hellmann_feynman": [float(g) for g in grad], "central_differences": fd,
+        "relative_difference": rel, "max_relative_difference": max(rel), "finite_difference_seconds": t_fd,
+        "nuclear_gradient_central_differences": nuclear.tolist(), "nuclear_seconds": t_nuc,
+        "grid": list(grid.shape)}), flush=True)
 
 
 def run_scan(args) -> None:
@@ -392,6 +466,9 @@ def main() -> None:
         return
     if args.workload == "h2plus-scan":
         run_scan(args)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args)
         return
     import torch
 

@@ -182,3 +182,24 @@ def test_h2plus_bond_derivative(pkg, cuda, golden_values):
     if ref is not None:
         assert abs(energies[1] - ref["plus"]) < 1e-11 and abs(energies[-1] - ref["minus"]) < 1e-11
         assert abs(derivative - ref["derivative"]) < 1e-7
+
+
+def test_config5_external_gradient_101(pkg, cuda):
+    """Config 5 at its own size (He-LDA, h = 0.16, box 16, 101^3, float64): the gradient with respect to
+    the seeded Gaussian perturbation against central differences (step 1e-4) on its three largest
+    components, to 1e-6 relative."""
+    system = oscf.he_lda(spacing=0.16, edge=16.0)
+    geo = _geometry(pkg, system, cuda)
+    assert geo.grid.shape == (101, 101, 101)
+    centres, widths, _ = pkg.adjoint.seeded_gaussians()
+    g_node, g_grid = pkg.adjoint.perturbation_fields(geo, centres, widths)
+    dv = pkg.adjoint.effective_perturbation(geo, g_node, g_grid)
+    base = _solve(pkg, pkg.KohnShamStep(geo, "lda_vwn", system.n_electrons))
+    grad = pkg.adjoint.external_potential_gradient(geo, base.density, g_node, g_grid).cpu().numpy()
+    step = 1e-4
+    for k in np.argsort(-np.abs(grad))[:3]:
+        e = [float(_solve(pkg, pkg.KohnShamStep(geo, "lda_vwn", system.n_electrons,
+                                                external_potential=sign * step * dv[k])).energies["total"])
+             for sign in (+1, -1)]
+        fd = (e[0] - e[1]) / (2 * step)
+        assert abs(fd - grad[k]) <= 1e-6 * abs(grad[k]), (int(k), fd, grad[k])

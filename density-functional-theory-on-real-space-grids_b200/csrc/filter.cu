@@ -895,11 +895,14 @@ bool tuned_choice(const TuneKey& key, TileChoice* out) {
     return true;
 }
 
-// Times the first Chebyshev step (packed block in buf[2] -> buf[0]) for every candidate tiling:
-// one untimed launch, then three timed ones per candidate. Synchronises the stream.
+// Times every candidate tiling: one untimed launch, then three timed ones each. With apply null,
+// the launch is the first Chebyshev step (packed block in buf[2] -> buf[0]); otherwise it is the
+// apply described by *apply (packed block in buf[2], written to the caller's output, which the
+// real launch then rewrites). Synchronises the stream.
 template <typename Lane>
 int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf[3], int64_t lanes,
-              const double* coefficients, int degree, cudaStream_t stream, TileChoice* best) {
+              const double* coefficients, int degree, cudaStream_t stream, TileChoice* best,
+              const FilterArgs* apply = nullptr) {
     const int nx = op->nx, ny = op->ny, nzp = padded_z(op->nz);
     cudaEvent_t e0, e1;
     int st = check(cudaEventCreate(&e0));
@@ -912,16 +915,21 @@ int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf
     *best = TileChoice{choose_tz(nzp), 0};
     for (int tz : {32, 36}) {
         FilterMaps m{};
-        if ((st = prepare_geometry<Lane>(op, batch, geo_base, tz, false, &m, stream)) != CDFTB_OK) break;
+        const bool kinetic = apply != nullptr && apply->kinetic_only;
+        if ((st = prepare_geometry<Lane>(op, batch, geo_base, tz, kinetic, &m, stream)) != CDFTB_OK) break;
         if ((st = encode_lane_maps(buf[2], nzp, ny, nx, lanes, tz, &m.phi, &m.prev)) != CDFTB_OK) break;
         FilterArgs a = base_args(op, batch);
-        a.coef = coefficients;
-        a.degree = degree;
-        a.step = 0;
-        a.has_prev = 0;
-        a.final_out = 0;
-        a.out = buf[0];
-        a.out_dtype = 0;
+        if (apply) {
+            a = *apply;
+        } else {
+            a.coef = coefficients;
+            a.degree = degree;
+            a.step = 0;
+            a.has_prev = 0;
+            a.final_out = 0;
+            a.out = buf[0];
+            a.out_dtype = 0;
+        }
         const int64_t tiles = int64_t(ceil_div(ny, TY)) * ceil_div(nzp, tz);
         int chunks_list[5] = {1, 2, 3, 4, 0};
         chunks_list[4] = static_cast<int>(ceil_div(nx, choose_chunk(nx, tiles * lanes, sm_count())));
@@ -1014,10 +1022,31 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
     const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
     char* w = static_cast<char*>(work);
     TileChoice choice{choose_tz(nzp), 0};
-    tuned_choice(tune_key(op, lanes), &choice);
-    const int tz = choice.tz;
+    const TuneKey key = tune_key(op, lanes);
+    const bool known = tuned_choice(key, &choice);
     int st = pack_block<Lane>(op, phi, in_dtype, batch, nx, ny, nz, nzp, lanes, w, stream);
     if (st != CDFTB_OK) return st;
+    bool autotune;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        autotune = g_autotune;
+    }
+    if (!known && autotune) {
+        FilterArgs t = base_args(op, batch);
+        t.apply_only = 1;
+        t.kinetic_only = kinetic_only != 0;
+        t.degree = 1;
+        t.final_out = 1;
+        t.out = out;
+        t.out_dtype = out_dtype;
+        void* bufs[3] = {nullptr, nullptr, w};
+        if ((st = tune_slab<Lane>(op, batch, w + lanes * lane_bytes, bufs, lanes, nullptr, 1, stream, &choice, &t)) !=
+            CDFTB_OK)
+            return st;
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned[key] = choice;
+    }
+    const int tz = choice.tz;
     FilterMaps m{};
     if ((st = prepare_geometry<Lane>(op, batch, w + lanes * lane_bytes, tz, kinetic_only != 0, &m, stream)) !=
         CDFTB_OK)

@@ -101,11 +101,11 @@ int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_d
                            cdftb_stream_t stream);
 
 /* No reference counterpart (the reference has no kernels of its own to tune): the tile autotuner of
- * the order-8 slab kernels. With it enabled, the first cdftb_chebyshev_filter call for a (device,
- * grid, precision, lane count) key times each candidate tiling -- z tiles of 32 or 36 columns, 1 to
- * 4 x chunks and the heuristic's chunk -- on that call's own buffers, keeps the fastest, and every
- * later filter or apply launch for the key uses it. That first call synchronises its stream (make
- * it before any stream capture); results are bit-identical whatever the tiling. Disabled (the
+ * the order-8 slab kernels. With it enabled, the first cdftb_chebyshev_filter or cdftb_cusp_apply
+ * call for a (device, grid, precision, lane count) key times each candidate tiling -- z tiles of 32
+ * or 36 columns, 1 to 4 x chunks and the heuristic's chunk -- on that call's own buffers, keeps the
+ * fastest, and every later filter or apply launch for the key uses it. That first call synchronises
+ * its stream (make it before any stream capture); results are bit-identical whatever the tiling. Disabled (the
  * default in the C library), heuristics choose the tiling. cdftb_filter_tuned_tile reports the
  * table's entry for a key (tile_z 32 or 36, x_chunk in planes; both 0 when the key is not tuned);
  * dtype is CDFTB_F32 or CDFTB_F64 and lanes is the launch's lane count (cdftb_operator orbitals in

@@ -159,3 +159,25 @@ def test_autotuned_tiling_is_bit_identical(pkg, cuda, dtype):
         lib.cdftb_filter_autotune(1)
     assert torch.equal(tuned, heuristic) and torch.equal(again, heuristic)
     assert _device_status(pkg) == (0, 0)
+
+
+def test_autotuned_apply_is_bit_identical(pkg, cuda):
+    """The one-launch apply tunes its own (grid, precision, lanes) key the same way, bit for bit."""
+    shape = (33, 19, 67)
+    faces, inv, q = _random_operator(shape, seed=21)
+    pot = np.random.default_rng(22).standard_normal(int(np.prod(shape)))
+    _, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot)
+    block = _t(np.random.default_rng(23).standard_normal((3, int(np.prod(shape)))), cuda)
+    lib = pkg._lib.library()
+    tz, xc = ctypes.c_int(-1), ctypes.c_int(-1)
+    try:
+        lib.cdftb_filter_autotune(0)
+        heuristic = ham.apply(block)
+        lib.cdftb_filter_autotune(1)
+        tuned = ham.apply(block)
+        assert lib.cdftb_filter_tuned_tile(*shape, 0, 3, ctypes.byref(tz), ctypes.byref(xc)) == 0
+        assert tz.value in (32, 36) and 1 <= xc.value <= shape[0]
+    finally:
+        lib.cdftb_filter_autotune(1)
+    assert torch.equal(tuned, heuristic)
+    assert _device_status(pkg) == (0, 0)

@@ -111,14 +111,6 @@ struct LaneF2 {
     static __device__ __forceinline__ E neg(E a) { return make_float2(-a.x, -a.y); }
     static __device__ __forceinline__ E splat(S s) { return make_float2(s, s); }
     static __device__ __forceinline__ E zero() { return make_float2(0.f, 0.f); }
-    static __device__ __forceinline__ void load2(const E* p, E& a, E& b) {
-        const float4 v = *reinterpret_cast<const float4*>(p);
-        a = make_float2(v.x, v.y);
-        b = make_float2(v.z, v.w);
-    }
-    static __device__ __forceinline__ void store2(E* p, E a, E b) {
-        *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
-    }
     static constexpr int ORBITALS = 2;
     static constexpr CUtensorMapDataType GEO_TYPE = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
 };
@@ -132,12 +124,6 @@ struct LaneD {
     static __device__ __forceinline__ E neg(E a) { return -a; }
     static __device__ __forceinline__ E splat(S s) { return s; }
     static __device__ __forceinline__ E zero() { return 0.0; }
-    static __device__ __forceinline__ void load2(const E* p, E& a, E& b) {
-        const double2 v = *reinterpret_cast<const double2*>(p);
-        a = v.x;
-        b = v.y;
-    }
-    static __device__ __forceinline__ void store2(E* p, E a, E b) { *reinterpret_cast<double2*>(p) = make_double2(a, b); }
     static constexpr int ORBITALS = 1;
     static constexpr CUtensorMapDataType GEO_TYPE = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
 };
@@ -236,14 +222,6 @@ __device__ __forceinline__ bool wait_full(unsigned bar, unsigned parity, unsigne
 // makes the warp leave together, so no lane waits in __syncwarp for an exited one).
 __device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, unsigned token) {
     return __all_sync(0xffffffffu, wait_full(bar, parity, token)) != 0;
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, unsigned bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
-        : "memory");
 }
 
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,

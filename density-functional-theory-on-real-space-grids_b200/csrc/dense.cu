@@ -196,17 +196,34 @@ __global__ void trsm_lower_fixed_kernel(const double* __restrict__ lower, const 
     for (int i = threadIdx.x; i < M * M; i += blockDim.x) l[i] = lower[static_cast<int64_t>(g) * M * M + i];
     __syncthreads();
     const double* src = in + g * in_stride;
-    for (int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; p < n;
-         p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        double x[M];
+    auto solve = [&](int64_t p, double* x) {
 #pragma unroll
         for (int i = 0; i < M; ++i) {
-            double v = src[i * n + p];
+            double v = x[i];
 #pragma unroll
             for (int k = 0; k < i; ++k) v -= l[i * M + k] * x[k];
             x[i] = v / l[i * M + i];
             store_as<double>(out, out_dtype, g * out_stride + i * n + p, x[i]);
         }
+    };
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    int64_t p = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    // two points per thread at a time: both points' loads are in flight before either is solved
+    for (; p + stride < n; p += 2 * stride) {
+        double x0[M], x1[M];
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            x0[i] = src[i * n + p];
+            x1[i] = src[i * n + p + stride];
+        }
+        solve(p, x0);
+        solve(p + stride, x1);
+    }
+    if (p < n) {
+        double x0[M];
+#pragma unroll
+        for (int i = 0; i < M; ++i) x0[i] = src[i * n + p];
+        solve(p, x0);
     }
 }
 
@@ -341,9 +358,14 @@ int ritz_chunks(int64_t n, int groups) {
     return static_cast<int>(chunks < 1 ? 1 : chunks);
 }
 
-inline unsigned point_blocks(int64_t n) {
+// CTAs along the points of each group: about 8 per SM over the whole launch (all groups), so that
+// with many groups every thread loops over several points instead of the launch running many
+// short waves of one point per thread.
+inline unsigned point_blocks(int64_t n, int groups) {
     const int64_t b = ceil_div(n, 256);
-    return static_cast<unsigned>(b < 148 * 8 ? b : 148 * 8);
+    int64_t cap = ceil_div(int64_t(148) * 8, groups > 0 ? groups : 1);
+    if (cap < 1) cap = 1;
+    return static_cast<unsigned>(b < cap ? b : cap);
 }
 
 }  // namespace
@@ -363,7 +385,7 @@ extern "C" int cdftb_block_trsm_lower_f64(const double* lower, const double* in,
                                           int out_dtype, int64_t out_group_stride, int m, int64_t n, int groups,
                                           cdftb_stream_t stream) {
     if (!lower || !in || !out || m <= 0 || m > MMAX || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
-    dim3 grid(point_blocks(n), groups);
+    dim3 grid(point_blocks(n, groups), groups);
     cudaStream_t s = as_stream(stream);
     switch (m) {
 #define CDFTB_TRSM(M)                                                                                             \
@@ -392,7 +414,7 @@ extern "C" int cdftb_block_rotate_f64(const double* r, const double* in, int64_t
     if (!r || !in || !out || m_out <= 0 || m_in <= 0 || m_out > MMAX || m_in > MMAX || n <= 0 || groups <= 0 ||
         groups > 65535)
         return CDFTB_ERR_ARGUMENT;
-    dim3 grid(point_blocks(n), groups);
+    dim3 grid(point_blocks(n, groups), groups);
     cudaStream_t s = as_stream(stream);
     if (m_out == m_in) {
         switch (m_in) {
@@ -412,7 +434,7 @@ extern "C" int cdftb_block_rotate_f64(const double* r, const double* in, int64_t
 extern "C" int cdftb_block_residual_f64(const double* a, const double* b, const double* evals, double* out, int m,
                                         int64_t n, int groups, int64_t group_stride, cdftb_stream_t stream) {
     if (!a || !b || !evals || !out || m <= 0 || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
-    dim3 grid(point_blocks(n), groups);
+    dim3 grid(point_blocks(n, groups), groups);
     residual_kernel<<<grid, 256, 0, as_stream(stream)>>>(a, b, evals, out, m, n, group_stride);
     return check_launch();
 }
@@ -422,7 +444,7 @@ extern "C" int cdftb_lanczos_update_f64(int mode, double* w, const double* v, co
     if (!w || mode < 0 || mode > 2 || n <= 0 || groups <= 0 || groups > 65535) return CDFTB_ERR_ARGUMENT;
     if (mode < 2 && (!v || !v_prev || !s1 || !s2)) return CDFTB_ERR_ARGUMENT;
     if (mode == 2 && !s1) return CDFTB_ERR_ARGUMENT;
-    dim3 grid(point_blocks(n), groups);
+    dim3 grid(point_blocks(n, groups), groups);
     lanczos_kernel<<<grid, 256, 0, as_stream(stream)>>>(mode, w, v, v_prev, s1, s2, n);
     return check_launch();
 }

@@ -22,7 +22,7 @@ CrossShape cross_shape(int ma, int mb, int64_t n, int groups) {
     if (ma == 1 && mb == 1) {
         s.ti = s.tj = 1;
     } else if (ma <= 6 && mb <= 6) {
-        s.ti = s.tj = 6;
+        s.ti = s.tj = ma > mb ? ma : mb;  // one tile of exactly the block width (2 .. 6)
     } else {
         s.ti = s.tj = 4;
     }
@@ -39,15 +39,17 @@ CrossShape cross_shape(int ma, int mb, int64_t n, int groups) {
 }
 
 // SAME: a and b are the same rows (a Gram matrix), each row is loaded once. Each thread takes the
-// columns p0 + t, p0 + t + RT, ... four at a time (independent loads in flight), always in the
-// same order, so the partial of a chunk does not depend on scheduling.
+// columns p0 + t, p0 + t + RT, ... U at a time (independent loads in flight), always in the same
+// order, so the partial of a chunk does not depend on scheduling (nor on U or the tile shape: an
+// entry's sum runs over the same columns in the same order). Tiles of 16 entries or more take two
+// points at a time, smaller ones four; tiles of up to 5 x 5 fit two CTAs per SM.
 template <int TI, int TJ, bool SAME>
-__global__ void __launch_bounds__(RT) cross_partial_kernel(const double* __restrict__ a, int ma, int64_t sa,
+__global__ void __launch_bounds__(RT, (TI <= 5 && TJ <= 5) ? 2 : 1) cross_partial_kernel(const double* __restrict__ a, int ma, int64_t sa,
                                                             const double* __restrict__ b, int mb, int64_t sb,
                                                             const double* __restrict__ q, int64_t q_stride, int64_t n,
                                                             int tiles_j, int64_t chunk, int chunks,
                                                             double* __restrict__ partial) {
-    constexpr int U = 4;
+    constexpr int U = (TI * TJ >= 16) ? 2 : 4;
     const int c = blockIdx.x;
     const int tile = blockIdx.y;
     const int g = blockIdx.z;
@@ -173,14 +175,20 @@ int launch_cross(const double* a, int ma, int64_t group_stride_a, const double* 
     cross_partial_kernel<TI_, TJ_, SAME_><<<grid, RT, 0, st>>>(a, ma, group_stride_a, b, mb, group_stride_b, q, \
                                                                q_group_stride, n, s.tiles_j, s.chunk, s.chunks,  \
                                                                partial)
-    if (s.ti == 1) {
-        if (same) CDFTB_CROSS_LAUNCH(1, 1, true);
-        else CDFTB_CROSS_LAUNCH(1, 1, false);
-    } else if (s.ti == 6) {
-        if (same) CDFTB_CROSS_LAUNCH(6, 6, true);
-        else CDFTB_CROSS_LAUNCH(6, 6, false);
-    } else {
+    if (s.tiles_i * s.tiles_j > 1) {
         CDFTB_CROSS_LAUNCH(4, 4, false);
+    } else {
+        switch (s.ti) {
+#define CDFTB_CROSS_WIDTH(T_)                        \
+    case T_:                                         \
+        if (same) CDFTB_CROSS_LAUNCH(T_, T_, true);  \
+        else CDFTB_CROSS_LAUNCH(T_, T_, false);      \
+        break;
+            CDFTB_CROSS_WIDTH(1) CDFTB_CROSS_WIDTH(2) CDFTB_CROSS_WIDTH(3) CDFTB_CROSS_WIDTH(4) CDFTB_CROSS_WIDTH(5)
+            CDFTB_CROSS_WIDTH(6)
+#undef CDFTB_CROSS_WIDTH
+            default: return CDFTB_ERR_ARGUMENT;
+        }
     }
 #undef CDFTB_CROSS_LAUNCH
     int rc = check_launch();

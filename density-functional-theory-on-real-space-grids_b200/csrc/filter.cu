@@ -549,32 +549,53 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
 }
 
 // Internal layout from a caller block: lanes of (nx, ny, nzp), padding and missing orbitals zero.
+// blockIdx.y walks the lanes (the lane's orbitals are found once), and each thread writes two
+// consecutive z points of a row (nzp is even) with one 16-byte store.
 template <typename Lane>
 __global__ void pack_lanes_kernel(const void* __restrict__ in, int in_dtype, int64_t batch, int nx, int ny, int nz,
                                   int nzp, int64_t lanes, int opg, int lpg, typename Lane::E* __restrict__ out) {
     using E = typename Lane::E;
-    const int64_t per_lane = int64_t(nx) * ny * nzp;
-    const int64_t total = lanes * per_lane;
+    const int half = nzp / 2;
+    const int64_t pairs = int64_t(nx) * ny * half;  // per lane
     const int64_t n_points = int64_t(nx) * ny * nz;
-    for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
-         idx += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t l = idx / per_lane;
-        const int64_t r = idx - l * per_lane;
-        const int zp = static_cast<int>(r % nzp);
-        const int64_t xy = r / nzp;
-        E v = Lane::zero();
-        if (zp < nz) {
-            const int64_t pt = xy * nz + zp;
-            if constexpr (Lane::ORBITALS == 2) {
-                const int64_t a0 = lane_orbital<2>(l, 0, batch, opg, lpg);
-                const int64_t a1 = lane_orbital<2>(l, 1, batch, opg, lpg);
-                v.x = a0 >= 0 ? load_as<float>(in, in_dtype, a0 * n_points + pt) : 0.f;
-                v.y = a1 >= 0 ? load_as<float>(in, in_dtype, a1 * n_points + pt) : 0.f;
+    const bool narrow = pairs <= 0xffffffffll;
+    for (int64_t l = blockIdx.y; l < lanes; l += gridDim.y) {
+        int64_t a0, a1;
+        if constexpr (Lane::ORBITALS == 2) {
+            a0 = lane_orbital<2>(l, 0, batch, opg, lpg);
+            a1 = lane_orbital<2>(l, 1, batch, opg, lpg);
+        } else {
+            a0 = l;
+            a1 = -1;
+        }
+        E* dst = out + l * (2 * pairs);
+        for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < pairs;
+             k += int64_t(gridDim.x) * blockDim.x) {
+            int64_t xy;
+            int zp;
+            if (narrow) {
+                const unsigned uk = static_cast<unsigned>(k), row = uk / static_cast<unsigned>(half);
+                xy = row;
+                zp = 2 * static_cast<int>(uk - row * static_cast<unsigned>(half));
             } else {
-                v = load_as<double>(in, in_dtype, l * n_points + pt);
+                xy = k / half;
+                zp = 2 * static_cast<int>(k - xy * half);
+            }
+            const int64_t pt = xy * nz + zp;
+            const bool in1 = zp + 1 < nz;  // zp < nz always (nzp - nz is 0 or 1)
+            E v0, v1;
+            if constexpr (Lane::ORBITALS == 2) {
+                v0.x = a0 >= 0 ? load_as<float>(in, in_dtype, a0 * n_points + pt) : 0.f;
+                v0.y = a1 >= 0 ? load_as<float>(in, in_dtype, a1 * n_points + pt) : 0.f;
+                v1.x = (a0 >= 0 && in1) ? load_as<float>(in, in_dtype, a0 * n_points + pt + 1) : 0.f;
+                v1.y = (a1 >= 0 && in1) ? load_as<float>(in, in_dtype, a1 * n_points + pt + 1) : 0.f;
+                reinterpret_cast<float4*>(dst)[k] = make_float4(v0.x, v0.y, v1.x, v1.y);
+            } else {
+                v0 = load_as<double>(in, in_dtype, a0 * n_points + pt);
+                v1 = in1 ? load_as<double>(in, in_dtype, a0 * n_points + pt + 1) : 0.0;
+                reinterpret_cast<double2*>(dst)[k] = make_double2(v0, v1);
             }
         }
-        out[idx] = v;
     }
 }
 
@@ -800,9 +821,13 @@ int prepare_geometry(const cdftb_operator* op, int64_t batch, void* geo_base, in
 template <typename Lane>
 int pack_block(const cdftb_operator* op, const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz,
                int nzp, int64_t lanes, void* dst, cudaStream_t stream) {
-    const int64_t total = lanes * int64_t(nx) * ny * nzp;
-    const unsigned blocks = static_cast<unsigned>(std::min<int64_t>(ceil_div(total, 256), 148 * 16));
-    pack_lanes_kernel<Lane><<<blocks, 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
+    // the lane buffers start 16-byte aligned (TMA needs it too) and a lane is an even number of points
+    if ((reinterpret_cast<uintptr_t>(dst) & 15) != 0 || (nzp & 1) != 0) return CDFTB_ERR_ARGUMENT;
+    const int64_t pairs = int64_t(nx) * ny * (nzp / 2);
+    const unsigned ly = static_cast<unsigned>(std::min<int64_t>(lanes, 65535));
+    const unsigned bx = static_cast<unsigned>(
+        std::max<int64_t>(1, std::min<int64_t>(ceil_div(pairs, 256), ceil_div(int64_t(148) * 16, ly))));
+    pack_lanes_kernel<Lane><<<dim3(bx, ly), 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
                                                         op->orbitals_per_group, aligned_lanes_per_group(op),
                                                         static_cast<typename Lane::E*>(dst));
     return check_launch();

@@ -545,15 +545,22 @@ class BatchedKohnShamStep:
         rho_out = (self.occ[None, :, None] * vectors.pow(2)).sum(dim=1)  # (B, N)
         return rho_out * self.f2[None, :], rho_out
 
-    def external_parts(self, rho: torch.Tensor):
-        """``((1/2)Q[f^2 grad rho . grad u], Q[f^2 rho W])`` per system (hamiltonian.py:557-574)."""
+    def external_parts(self, rho: torch.Tensor, rho_node: torch.Tensor | None = None):
+        """``((1/2)Q[f^2 grad rho . grad u], Q[f^2 rho W])`` per system (hamiltonian.py:557-574).
+
+        ``rho_node`` (B, M): ``L rho`` when the caller already holds it (the output potentials
+        interpolate the same density), so that only the gradient is interpolated here.
+        """
         q = self.quadrature
         factor = self.factor
         b, n = rho.shape
         grad = gradient(self.grid, rho)  # (B, 3, N)
-        fields = torch.cat([rho[:, None], grad], dim=1).contiguous()  # (B, 4, N)
-        node = q.interpolate(fields)  # (B, 4, M)
-        rho_node, grad_node = node[:, 0], node[:, 1:]
+        if rho_node is None:
+            fields = torch.cat([rho[:, None], grad], dim=1).contiguous()  # (B, 4, N)
+            node = q.interpolate(fields)  # (B, 4, M)
+            rho_node, grad_node = node[:, 0], node[:, 1:]
+        else:
+            grad_node = q.interpolate(grad.contiguous())  # (B, 3, M)
         cross_node = q.f2[None] * (grad_node * q.grad_u[None]).sum(dim=1)
         cross_grid = factor.weight[None] * (grad * factor.grad_u[None]).sum(dim=1)
         cross = 0.5 * (row_sums(q.weights[None] * cross_node) + row_sums(q.far_weights[None] * cross_grid))
@@ -571,7 +578,7 @@ class BatchedKohnShamStep:
         kin = h.apply(vectors, kinetic_only=True)
         kinetic_form = rowwise_inner(vectors.reshape(b * k, n), kin.reshape(b * k, n), h.q).reshape(b, k)
         first = (self.occ[None] * kinetic_form).sum(dim=1)
-        cross, pot = self.external_parts(rho_out)
+        cross, pot = self.external_parts(rho_out, p_out.node[0] if p_out.node is not None else None)
         kinetic = first - cross - pot
         dc_out = row_sums(p_in.effective * q.mass_weights[None] * rho_out)
         kpe = band - dc_out

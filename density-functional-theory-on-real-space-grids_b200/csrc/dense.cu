@@ -136,6 +136,110 @@ __global__ void eigh_kernel(const double* __restrict__ matrix, double* __restric
     }
 }
 
+// eigh_kernel for a width known at compile time (m <= 6): the same sweeps, rotations and sort in the
+// same order, with the matrices in registers instead of local memory.
+template <int M>
+__global__ void eigh_fixed_kernel(const double* __restrict__ matrix, double* __restrict__ evals,
+                                  double* __restrict__ vectors, int groups) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= groups) return;
+    double a[M][M];
+    double v[M][M];
+    const double* src = matrix + static_cast<int64_t>(g) * M * M;
+#pragma unroll
+    for (int i = 0; i < M; ++i)
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            a[i][j] = 0.5 * (src[i * M + j] + src[j * M + i]);
+            v[i][j] = (i == j) ? 1.0 : 0.0;
+        }
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        double off = 0.0, diag = 0.0;
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            diag += a[i][i] * a[i][i];
+#pragma unroll
+            for (int j = i + 1; j < M; ++j) off += a[i][j] * a[i][j];
+        }
+        if (off <= 1e-36 * diag || off == 0.0) break;
+#pragma unroll
+        for (int p = 0; p < M - 1; ++p) {
+#pragma unroll
+            for (int q = p + 1; q < M; ++q) {
+                const double apq = a[p][q];
+                if (apq == 0.0) continue;
+                const double app = a[p][p];
+                const double aqq = a[q][q];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0);
+                const double s = t * c;
+#pragma unroll
+                for (int k = 0; k < M; ++k) {
+                    const double akp = a[k][p];
+                    const double akq = a[k][q];
+                    a[k][p] = c * akp - s * akq;
+                    a[k][q] = s * akp + c * akq;
+                }
+#pragma unroll
+                for (int k = 0; k < M; ++k) {
+                    const double apk = a[p][k];
+                    const double aqk = a[q][k];
+                    a[p][k] = c * apk - s * aqk;
+                    a[q][k] = s * apk + c * aqk;
+                }
+                a[p][q] = 0.0;
+                a[q][p] = 0.0;
+#pragma unroll
+                for (int k = 0; k < M; ++k) {
+                    const double vkp = v[k][p];
+                    const double vkq = v[k][q];
+                    v[k][p] = c * vkp - s * vkq;
+                    v[k][q] = s * vkp + c * vkq;
+                }
+            }
+        }
+    }
+    // ascending order (the selection sort of eigh_kernel), eigenvectors written as rows
+    double d[M];
+    int order[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        d[i] = a[i][i];
+        order[i] = i;
+    }
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        int best = i;
+#pragma unroll
+        for (int j = i + 1; j < M; ++j)
+            if (d[j] < d[best]) best = j;
+        // swap entries i and best of (d, order) with register-only selects
+#pragma unroll
+        for (int j = i + 1; j < M; ++j)
+            if (j == best) {
+                const double td = d[i];
+                d[i] = d[j];
+                d[j] = td;
+                const int to = order[i];
+                order[i] = order[j];
+                order[j] = to;
+            }
+    }
+    double* ev = evals + static_cast<int64_t>(g) * M;
+    double* vec = vectors + static_cast<int64_t>(g) * M * M;
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        ev[k] = d[k];
+#pragma unroll
+        for (int col = 0; col < M; ++col)
+            if (col == order[k]) {
+#pragma unroll
+                for (int j = 0; j < M; ++j) vec[k * M + j] = v[j][col];
+            }
+    }
+}
+
 __global__ void rotate_kernel(const double* __restrict__ r, const double* __restrict__ in, int64_t in_stride, void* out,
                               int out_dtype, int64_t out_stride, int m_out, int m_in, int64_t n) {
     __shared__ double rs[MMAX * MMAX];
@@ -404,7 +508,18 @@ extern "C" int cdftb_block_trsm_lower_f64(const double* lower, const double* in,
 extern "C" int cdftb_small_eigh_f64(const double* matrix, double* evals, double* vectors, int m, int groups,
                                     cdftb_stream_t stream) {
     if (!matrix || !evals || !vectors || m <= 0 || m > MMAX || groups <= 0) return CDFTB_ERR_ARGUMENT;
-    eigh_kernel<<<static_cast<unsigned>(ceil_div(groups, 32)), 32, 0, as_stream(stream)>>>(matrix, evals, vectors, m, groups);
+    const unsigned blocks = static_cast<unsigned>(ceil_div(groups, 32));
+    cudaStream_t s = as_stream(stream);
+    switch (m) {
+#define CDFTB_EIGH(M)                                                                \
+    case M:                                                                          \
+        eigh_fixed_kernel<M><<<blocks, 32, 0, s>>>(matrix, evals, vectors, groups); \
+        return check_launch();
+        CDFTB_EIGH(1) CDFTB_EIGH(2) CDFTB_EIGH(3) CDFTB_EIGH(4) CDFTB_EIGH(5) CDFTB_EIGH(6)
+#undef CDFTB_EIGH
+        default: break;
+    }
+    eigh_kernel<<<blocks, 32, 0, s>>>(matrix, evals, vectors, m, groups);
     return check_launch();
 }
 

@@ -20,6 +20,18 @@ inline unsigned blocks_for(int64_t n, int threads) {
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < (n); i += static_cast<int64_t>(gridDim.x) * blockDim.x)
 
+// k -> (system g, point i) of a (batch, np) array; 32-bit division when the whole index fits.
+__device__ __forceinline__ void split_index(int64_t k, int64_t np, bool narrow, int64_t& g, int64_t& i) {
+    if (narrow) {
+        const unsigned uk = static_cast<unsigned>(k), un = static_cast<unsigned>(np), ug = uk / un;
+        g = ug;
+        i = uk - ug * un;
+    } else {
+        g = k / np;
+        i = k - g * np;
+    }
+}
+
 __global__ void xc_lda_kernel(const double* __restrict__ n, int64_t p, double* __restrict__ e, double* __restrict__ v) {
     GRID_STRIDE(i, p) {
         double ei, vi;
@@ -78,9 +90,10 @@ __global__ void cusp_coefficients_kernel(const double* __restrict__ rho_at_nucle
 __global__ void hartree_split_kernel(const double* __restrict__ n, const double* __restrict__ f2,
                                      const double* __restrict__ cusp_grid, const double* __restrict__ coef, int na,
                                      int64_t np, int batch, double* __restrict__ rho, double* __restrict__ n_smooth) {
+    const bool narrow = np * batch <= 0xffffffffll;
     GRID_STRIDE(k, np * batch) {
-        const int64_t g = k / np;
-        const int64_t i = k - g * np;
+        int64_t g, i;
+        split_index(k, np, narrow, g, i);
         const double nv = n[k];
         rho[k] = nv / f2[i];
         double cusp = 0.0;
@@ -100,9 +113,10 @@ __global__ void node_lda_kernel(const double* __restrict__ fields, int64_t m, co
                                 const double* __restrict__ f2n, const double* __restrict__ v1s_node,
                                 const double* __restrict__ coef, int na, int batch, double* __restrict__ x,
                                 double* __restrict__ e_w) {
+    const bool narrow = m * batch <= 0xffffffffll;
     GRID_STRIDE(k, m * batch) {
-        const int64_t g = k / m;
-        const int64_t i = k - g * m;
+        int64_t g, i;
+        split_index(k, m, narrow, g, i);
         const double rho_node = fields[g * m + i];
         double vh = 0.0;
         for (int a = 0; a < na; ++a) {
@@ -130,9 +144,10 @@ __global__ void grid_lda_kernel(const double* __restrict__ n, const double* __re
                                 const double* __restrict__ v1s_grid, const double* __restrict__ coef, int na,
                                 const double* __restrict__ lifted, int64_t np, int batch, double* __restrict__ effective,
                                 double* __restrict__ v_hartree, double* __restrict__ terms, double* __restrict__ v_xc) {
+    const bool narrow = np * batch <= 0xffffffffll;
     GRID_STRIDE(k, np * batch) {
-        const int64_t g = k / np;
-        const int64_t i = k - g * np;
+        int64_t g, i;
+        split_index(k, np, narrow, g, i);
         double vh = 0.0;
         for (int a = 0; a < na; ++a) {
             const double t = coef[g * na + a] * v1s_grid[a * np + i];
@@ -201,12 +216,28 @@ __global__ void fd_derivative_kernel(const double* __restrict__ in, double* __re
                                      int axis, int half, const double* __restrict__ coeffs_dev, double scale,
                                      int64_t batch, int accumulate, double sign) {
     const int64_t np = static_cast<int64_t>(nx) * ny * nz;
+    const bool narrow = np * batch <= 0xffffffffll;  // 32-bit index arithmetic suffices
     GRID_STRIDE(k, np * batch) {
-        const int64_t g = k / np;
-        const int64_t i = k - g * np;
-        const int ix = static_cast<int>(i / (static_cast<int64_t>(ny) * nz));
-        const int iy = static_cast<int>((i / nz) % ny);
-        const int iz = static_cast<int>(i % nz);
+        int64_t g, i;
+        int ix, iy, iz;
+        if (narrow) {
+            const unsigned uk = static_cast<unsigned>(k), unp = static_cast<unsigned>(np);
+            const unsigned ug = uk / unp, ui = uk - ug * unp;
+            const unsigned uyz = static_cast<unsigned>(ny) * static_cast<unsigned>(nz);
+            const unsigned ux = ui / uyz, r = ui - ux * uyz;
+            const unsigned uy = r / static_cast<unsigned>(nz);
+            g = ug;
+            i = ui;
+            ix = static_cast<int>(ux);
+            iy = static_cast<int>(uy);
+            iz = static_cast<int>(r - uy * static_cast<unsigned>(nz));
+        } else {
+            g = k / np;
+            i = k - g * np;
+            ix = static_cast<int>(i / (static_cast<int64_t>(ny) * nz));
+            iy = static_cast<int>((i / nz) % ny);
+            iz = static_cast<int>(i % nz);
+        }
         const int pos = axis == 0 ? ix : (axis == 1 ? iy : iz);
         const int ext = axis == 0 ? nx : (axis == 1 ? ny : nz);
         const int64_t stride = axis == 0 ? static_cast<int64_t>(ny) * nz : (axis == 1 ? nz : 1);

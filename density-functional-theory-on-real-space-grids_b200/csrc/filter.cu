@@ -548,6 +548,371 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Wide float32 lanes: four orbitals per 16-byte element (float4), two packed f32x2 instructions per
+// element operation. The instructions that do not scale with the orbitals (addressing, barrier
+// waits, loads and stores of a point, the weights) are shared by four orbitals instead of two. The
+// roles and rings are those of slab_filter_kernel; two forms keep the registers within one CTA per
+// SM:
+//   pass item   streams its 22 nodes through a window of 8, forming each face as soon as its 8
+//               nodes are in and adding it at once to the 8 outputs it reaches (8 accumulators);
+//   march       keeps the last 8 nodes and the 8 outputs still open: each new x face is added to all
+//               of them, the newest output starts from its plane's y+z part, and the oldest one is
+//               complete after its last face.
+// Lanes run over the orbitals in order (lane l: orbitals 4l .. 4l+3); lanes aligned to orbital
+// groups (per-system geometry) keep the two-orbital kernel.
+
+struct Quad {
+    using E = float4;
+    static __device__ __forceinline__ float2 lo(E v) { return make_float2(v.x, v.y); }
+    static __device__ __forceinline__ float2 hi(E v) { return make_float2(v.z, v.w); }
+    static __device__ __forceinline__ E join(float2 a, float2 b) { return make_float4(a.x, a.y, b.x, b.y); }
+    // t (a float2 holding one tap twice) times v plus c
+    static __device__ __forceinline__ E fmat(float2 t, E v, E c) {
+        return join(__ffma2_rn(t, lo(v), lo(c)), __ffma2_rn(t, hi(v), hi(c)));
+    }
+    static __device__ __forceinline__ E mult(float2 t, E v) { return join(__fmul2_rn(t, lo(v)), __fmul2_rn(t, hi(v))); }
+    static __device__ __forceinline__ E fma(E a, E b, E c) {
+        return join(__ffma2_rn(lo(a), lo(b), lo(c)), __ffma2_rn(hi(a), hi(b), hi(c)));
+    }
+    static __device__ __forceinline__ E mul(E a, E b) { return join(__fmul2_rn(lo(a), lo(b)), __fmul2_rn(hi(a), hi(b))); }
+    static __device__ __forceinline__ E add(E a, E b) { return join(__fadd2_rn(lo(a), lo(b)), __fadd2_rn(hi(a), hi(b))); }
+    static __device__ __forceinline__ E neg(E a) { return make_float4(-a.x, -a.y, -a.z, -a.w); }
+    static __device__ __forceinline__ E zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+};
+
+constexpr int RW = 4;  // plane slots of the wide kernel (16-byte elements: a slot is ~34 KB)
+static_assert(RW % NG == 0, "a slot is always served by the same pass group");
+
+template <int TZ>
+struct WideShape {
+    static constexpr int EB = 16;
+    static constexpr int MW = TY * TZ / 32;
+    static constexpr int NZS = (TZ + 7) / 8;
+    static constexpr int ITEMS = TZ + TY * NZS;
+    static constexpr int PWG = (ITEMS + 31) / 32;
+    static constexpr int PW = NG * PWG;
+    static constexpr int WARPS = MW + PW + 1;
+    static constexpr int T = WARPS * 32;
+    static constexpr int BW = TZ + 18;
+    static constexpr int ZROW = TZ + 2;
+    static constexpr unsigned TX_PHI = NROW * BW * EB;
+    static constexpr unsigned TX_PREV = TY * TZ * EB;
+    static constexpr unsigned TX_W0 = TY * TZ * 4;
+    static constexpr unsigned TX_W1 = (TY + 7) * TZ * 4;
+    static constexpr unsigned TX_W2 = TY * (TZ + 8) * 4;
+    static constexpr unsigned TX_INV = TY * TZ * 4;
+    static constexpr unsigned TX_POT = TY * TZ * 4;
+    static constexpr size_t O_PHI = 0;
+    static constexpr size_t O_PREV = O_PHI + align128(TX_PHI);
+    static constexpr size_t O_W0 = O_PREV + align128(TX_PREV);
+    static constexpr size_t O_W1 = O_W0 + align128(TX_W0);
+    static constexpr size_t O_W2 = O_W1 + align128(TX_W1);
+    static constexpr size_t O_INV = O_W2 + align128(TX_W2);
+    static constexpr size_t O_POT = O_INV + align128(TX_INV);  // four potentials, TX_POT apart (128-aligned)
+    static constexpr size_t POT_STEP = align128(TX_POT);
+    static constexpr size_t SLOT = O_POT + 4 * POT_STEP;
+    static constexpr size_t O_YZ = RW * SLOT;
+    static constexpr size_t YZ_Z = size_t(TY) * TZ * EB;
+    static constexpr size_t YZ_SLOT = align128(YZ_Z + size_t(TY) * ZROW * EB);
+    static constexpr size_t O_BAR = O_YZ + RY * YZ_SLOT;
+    static constexpr size_t BYTES = O_BAR + (2 * RW + 2 * RY) * 8;
+    static_assert(TY * TZ % 32 == 0, "march warps cover the tile");
+    static_assert(TZ >= 8 && TZ % 2 == 0, "z segments of 8 inside the tile");
+    static_assert(BYTES <= 232448, "fits the opt-in shared memory of one CTA");
+};
+
+template <int TZ>
+__global__ void __launch_bounds__(WideShape<TZ>::T, 1)
+    slab_filter_wide_kernel(const __grid_constant__ FilterMaps maps, const FilterArgs a) {
+    using E = float4;
+    using SH = WideShape<TZ>;
+    constexpr int BW = SH::BW;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const unsigned bar_full = smem_u32(smem + SH::O_BAR);
+    const unsigned bar_empty = bar_full + 8 * RW;
+    const unsigned bar_yfull = bar_empty + 8 * RW;
+    const unsigned bar_yempty = bar_yfull + 8 * RY;
+
+    const int t = threadIdx.x;
+    const int warp = t >> 5;
+    const int nx = a.nx, ny = a.ny, nz = a.nz, nzp = a.nzp;
+    const int y0 = (blockIdx.x / a.tiles_z) * TY;
+    const int z0 = (blockIdx.x % a.tiles_z) * TZ;
+    const int xa = blockIdx.y * a.xchunk;
+    const int xe = min(xa + a.xchunk, nx) - 1;
+    const int lane = static_cast<int>(a.lane_first) + blockIdx.z;
+    const int q0 = xa > 0 ? xa - HALO : 0;
+    const int npl = xe + HALO + 1 - q0;
+    const bool has_prev = a.has_prev != 0;
+
+    // the lane's four orbitals (an empty slot borrows the first orbital's group for its lookups)
+    int64_t orb[4];
+    int grp[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+        const int64_t o = int64_t(4) * lane + h;
+        orb[h] = o < a.batch ? o : -1;
+    }
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+        const int64_t o = orb[h] >= 0 ? orb[h] : orb[0];
+        grp[h] = a.shared_potential ? 0 : static_cast<int>(o / a.orb_per_group);
+    }
+
+    if (t == 0) {
+        for (int s = 0; s < RW; ++s) {
+            mbar_init(bar_full + 8 * s, 1);
+            mbar_init(bar_empty + 8 * s, SH::MW + SH::PWG);
+        }
+        for (int s = 0; s < RY; ++s) {
+            mbar_init(bar_yfull + 8 * s, SH::PWG);
+            mbar_init(bar_yempty + 8 * s, SH::MW);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+
+    float2 tap[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) tap[j] = make_float2(static_cast<float>(a.taps[j]), static_cast<float>(a.taps[j]));
+
+    if (warp == SH::MW + SH::PW) {
+        // ------------------------------------------------------------------ producer
+        if ((t & 31) != 0) return;
+        const unsigned tx = SH::TX_PHI + (has_prev ? SH::TX_PREV : 0) + SH::TX_W0 + SH::TX_W1 + SH::TX_W2 +
+                            SH::TX_INV + 4 * SH::TX_POT;
+        int issued = 0;
+        int s = 0, ph = 1;
+        for (int n = 0; n < npl; ++n) {
+            if (n >= RW && !wait_full(bar_empty + 8 * s, ph, a.token)) break;
+            const unsigned full = bar_full + 8 * s;
+            unsigned char* slot = smem + s * SH::SLOT;
+            const int q = q0 + n;
+            mbar_expect_tx(full, tx);
+            // lane buffers as 8-byte elements, two per point: x = 2 z
+            tma_load_4d(slot + SH::O_PHI, &maps.phi, 2 * (z0 - 8), y0 - HALO, q, lane, full);
+            if (has_prev) tma_load_4d(slot + SH::O_PREV, &maps.prev, 2 * z0, y0, q - HALO, lane, full);
+            tma_load_4d(slot + SH::O_W0, &maps.w0, z0, y0, q, 0, full);
+            tma_load_4d(slot + SH::O_W1, &maps.w1, z0, y0, q, 0, full);
+            tma_load_4d(slot + SH::O_W2, &maps.w2, z0, y0, q, 0, full);
+            tma_load_4d(slot + SH::O_INV, &maps.inv, z0, y0, q - HALO, 0, full);
+#pragma unroll
+            for (int h = 0; h < 4; ++h)
+                tma_load_4d(slot + SH::O_POT + h * SH::POT_STEP, &maps.pot, z0, y0, q - HALO, grp[h], full);
+            issued = n + 1;
+            if (++s == RW) {
+                s = 0;
+                ph ^= 1;
+            }
+        }
+        if (issued < npl) {
+            for (int n = max(0, issued - RW); n < issued; ++n) {
+                const unsigned long long start = globaltimer();
+                for (unsigned it = 0; it < (1u << 24); ++it)
+                    if (mbar_try_wait(bar_full + 8 * (n % RW), (n / RW) & 1) || globaltimer() - start > 100000000ull)
+                        break;
+            }
+        }
+        return;
+    }
+
+    if (warp >= SH::MW) {
+        // ------------------------------------------------------------------ pass groups
+        const int pg = (warp - SH::MW) / SH::PWG;
+        const int it = t - (SH::MW + pg * SH::PWG) * 32;
+        bool active = false;
+        int nb = 0, ns = 0, wb = 0, ws = 0, ob = 0, os = 0, first = 0;
+        if (it < TZ) {
+            const int zc = it;
+            active = z0 + zc < nz;
+            nb = zc + 8;
+            ns = BW;
+            wb = SH::O_W1 / 4 + zc;
+            ws = TZ;
+            ob = zc;
+            os = TZ;
+        } else if (it < SH::ITEMS) {
+            const int zi = it - TZ;
+            const int ry = zi % TY;
+            const int seg = zi / TY;
+            const int zs = min(seg * 8, TZ - 8);
+            first = seg * 8 - zs;
+            active = y0 + ry < ny && z0 + zs < nz;
+            nb = (ry + HALO) * BW + zs + 1;
+            ns = 1;
+            wb = SH::O_W2 / 4 + ry * (TZ + 8) + zs;
+            ws = 1;
+            ob = int(SH::YZ_Z / sizeof(E)) + ry * SH::ZROW + zs;
+            os = 1;
+        }
+        int s = pg, ph = 0;
+        for (int n = pg; n < npl; n += NG) {
+            if (!warp_wait(bar_full + 8 * s, ph, a.token)) return;
+            const int q = q0 + n;
+            if (q >= xa && q <= xe) {
+                const int m = q - xa;
+                const int ys = m & (RY - 1);
+                const unsigned uy = m / RY;
+                if (uy >= 1 && !warp_wait(bar_yempty + 8 * ys, (uy - 1) & 1, a.token)) return;
+                if (active) {
+                    const unsigned char* slot = smem + s * SH::SLOT;
+                    const E* nodes = reinterpret_cast<const E*>(slot) + nb;
+                    const float* w = reinterpret_cast<const float*>(slot) + wb;
+                    E* out = reinterpret_cast<E*>(smem + SH::O_YZ + ys * SH::YZ_SLOT) + ob;
+                    E win[8], acc[TY];
+#pragma unroll
+                    for (int r = 0; r < NROW; ++r) {
+                        win[r & 7] = nodes[r * ns];
+                        if (r >= 7) {
+                            const int rf = r - 7;  // face rf from nodes rf .. rf + 7
+                            E sum = Quad::zero();
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) sum = Quad::fmat(tap[j], win[(rf + j) & 7], sum);
+                            const float wf = w[rf * ws];
+                            const E f = Quad::mult(make_float2(wf, wf), sum);
+                            // face rf reaches outputs o = rf - 7 .. rf with tap o + 7 - rf
+#pragma unroll
+                            for (int o = 0; o < TY; ++o) {
+                                if (o < rf - 7 || o > rf) continue;
+                                acc[o] = (o == rf) ? Quad::mult(tap[7], f) : Quad::fmat(tap[o + 7 - rf], f, acc[o]);
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int o = 0; o < TY; ++o)
+                        if (o >= first) out[o * os] = acc[o];
+                }
+                __syncwarp();
+                if ((t & 31) == 0) mbar_arrive(bar_yfull + 8 * ys);
+            } else {
+                __syncwarp();
+            }
+            if ((t & 31) == 0) mbar_arrive(bar_empty + 8 * s);
+            s += NG;
+            if (s >= RW) {
+                s -= RW;
+                ph ^= 1;
+            }
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------------- march
+    const int ty = t / TZ;
+    const int tz = t - ty * TZ;
+    const int y = y0 + ty;
+    const int z = z0 + tz;
+    const bool own_in = y < ny && z < nz;
+    const bool own_pad = y < ny && z < nzp;
+    const int64_t plane_n = int64_t(ny) * nz;
+    const int own = ty * TZ + tz;
+
+    E cc = Quad::zero(), ca = Quad::zero(), cb = Quad::zero();
+    if (!a.apply_only) {
+        float c3[3][4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int64_t o = orb[h] >= 0 ? orb[h] : orb[0];
+            const double* r = a.coef + ((o / a.orb_per_group) * a.degree + a.step) * 3;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) c3[k][h] = static_cast<float>(r[k]);
+        }
+        cc = make_float4(c3[0][0], c3[0][1], c3[0][2], c3[0][3]);
+        ca = make_float4(c3[1][0], c3[1][1], c3[1][2], c3[1][3]);
+        cb = make_float4(c3[2][0], c3[2][1], c3[2][2], c3[2][3]);
+    }
+
+    E phq[8], acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        phq[j] = Quad::zero();
+        acc[j] = Quad::zero();
+    }
+
+    int s = 0, sph = 0;
+    for (int n0 = 0; n0 < npl; n0 += 8) {
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+            const int n = n0 + g;
+            if (n >= npl) break;
+            if (!warp_wait(bar_full + 8 * s, sph, a.token)) return;
+            const unsigned char* slot = smem + s * SH::SLOT;
+            const int q = q0 + n;
+            phq[g] = reinterpret_cast<const E*>(slot + SH::O_PHI)[(ty + HALO) * BW + tz + 8];
+            E face;
+            {
+                E sum = Quad::zero();
+#pragma unroll
+                for (int j = 0; j < 8; ++j) sum = Quad::fmat(tap[j], phq[(g + 1 + j) & 7], sum);
+                const float wx = own_in ? reinterpret_cast<const float*>(slot + SH::O_W0)[own] : 0.f;
+                face = Quad::mult(make_float2(wx, wx), sum);  // x face q - 4
+            }
+            // the face reaches the open outputs q - 7 .. q (slot (g - d) & 7 holds output q - d, tap 7 - d)
+#pragma unroll
+            for (int d = 1; d < 8; ++d) acc[(g - d) & 7] = Quad::fmat(tap[7 - d], face, acc[(g - d) & 7]);
+            E yz = Quad::zero();
+            if (q >= xa && q <= xe) {
+                const int m = q - xa;
+                const int ys = m & (RY - 1);
+                if (!warp_wait(bar_yfull + 8 * ys, (m / RY) & 1, a.token)) return;
+                const unsigned char* yzs = smem + SH::O_YZ + ys * SH::YZ_SLOT;
+                yz = Quad::add(reinterpret_cast<const E*>(yzs)[own],
+                               reinterpret_cast<const E*>(yzs + SH::YZ_Z)[ty * SH::ZROW + tz]);
+                __syncwarp();
+                if ((t & 31) == 0) mbar_arrive(bar_yempty + 8 * ys);
+            }
+            const int i = q - HALO;  // output complete at this plane (slot (g + 1) & 7)
+            if (i >= xa && own_pad) {
+                const E div = acc[(g + 1) & 7];
+                const int64_t pt = int64_t(i) * plane_n + (own_in ? int64_t(y) * nz + z : 0);
+                E res = Quad::zero();
+                if (own_in) {
+                    const E phi = phq[(g + 1) & 7];
+                    const float inv = reinterpret_cast<const float*>(slot + SH::O_INV)[own];
+                    const E kin = Quad::mult(make_float2(0.5f * inv, 0.5f * inv), div);
+                    if (a.kinetic_only) {
+                        res = kin;
+                    } else {
+                        const float* pot = reinterpret_cast<const float*>(slot + SH::O_POT);
+                        const E potv = make_float4(pot[own], pot[SH::POT_STEP / 4 + own], pot[2 * SH::POT_STEP / 4 + own],
+                                                   pot[3 * SH::POT_STEP / 4 + own]);
+                        const E applied = Quad::fma(phi, potv, kin);
+                        if (a.apply_only) {
+                            res = applied;
+                        } else {
+                            res = Quad::mul(Quad::fma(Quad::neg(cc), phi, applied), ca);
+                            if (has_prev)
+                                res = Quad::fma(Quad::neg(cb), reinterpret_cast<const E*>(slot + SH::O_PREV)[own], res);
+                        }
+                    }
+                }
+                if (a.final_out) {
+                    if (own_in) {
+                        const float rv[4] = {res.x, res.y, res.z, res.w};
+#pragma unroll
+                        for (int h = 0; h < 4; ++h)
+                            if (orb[h] >= 0) store_as<float>(a.out, a.out_dtype, orb[h] * (plane_n * nx) + pt, rv[h]);
+                    }
+                } else {
+                    E* out = static_cast<E*>(a.out);
+                    out[(int64_t(lane) * nx + i) * (int64_t(ny) * nzp) + int64_t(y) * nzp + z] = res;
+                }
+            }
+            // the newest output, q, opens from its y+z part and its first face (its slot held output
+            // q - 8, completed on the previous plane)
+            acc[g] = Quad::fmat(tap[7], face, yz);
+            __syncwarp();
+            if ((t & 31) == 0) mbar_arrive(bar_empty + 8 * s);
+            if (++s == RW) {
+                s = 0;
+                sph ^= 1;
+            }
+        }
+    }
+}
+
 // Internal layout from a caller block: lanes of (nx, ny, nzp), padding and missing orbitals zero.
 // blockIdx.y walks the lanes (the lane's orbitals are found once), and each thread writes two
 // consecutive z points of a row (nzp is even) with one 16-byte store.
@@ -595,6 +960,42 @@ __global__ void pack_lanes_kernel(const void* __restrict__ in, int in_dtype, int
                 v1 = in1 ? load_as<double>(in, in_dtype, a0 * n_points + pt + 1) : 0.0;
                 reinterpret_cast<double2*>(dst)[k] = make_double2(v0, v1);
             }
+        }
+    }
+}
+
+// Wide float32 lanes from a caller block: lane l holds orbitals 4l .. 4l+3 as a float4 per point,
+// padding and missing orbitals zero. blockIdx.y walks the lanes; one point per thread.
+__global__ void pack_wide_kernel(const void* __restrict__ in, int in_dtype, int64_t batch, int nx, int ny, int nz,
+                                 int nzp, int64_t lanes, float4* __restrict__ out) {
+    const int64_t per_lane = int64_t(nx) * ny * nzp;
+    const int64_t n_points = int64_t(nx) * ny * nz;
+    const bool narrow = per_lane <= 0xffffffffll;
+    for (int64_t l = blockIdx.y; l < lanes; l += gridDim.y) {
+        float4* dst = out + l * per_lane;
+        int64_t orb[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) orb[h] = (4 * l + h < batch) ? 4 * l + h : -1;
+        for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < per_lane;
+             k += int64_t(gridDim.x) * blockDim.x) {
+            int64_t xy;
+            int zp;
+            if (narrow) {
+                const unsigned uk = static_cast<unsigned>(k), row = uk / static_cast<unsigned>(nzp);
+                xy = row;
+                zp = static_cast<int>(uk - row * static_cast<unsigned>(nzp));
+            } else {
+                xy = k / nzp;
+                zp = static_cast<int>(k - xy * nzp);
+            }
+            float v[4] = {0.f, 0.f, 0.f, 0.f};
+            if (zp < nz) {
+                const int64_t pt = xy * nz + zp;
+#pragma unroll
+                for (int h = 0; h < 4; ++h)
+                    if (orb[h] >= 0) v[h] = load_as<float>(in, in_dtype, orb[h] * n_points + pt);
+            }
+            dst[k] = make_float4(v[0], v[1], v[2], v[3]);
         }
     }
 }
@@ -1065,11 +1466,129 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
     return launch_any_tz<Lane>(tz, m, a, lanes, stream, choice.xchunk);
 }
 
+// ---- wide float32 lanes (slab_filter_wide_kernel)
+bool g_wide = true;  // guarded by g_tune_mutex
+
+int64_t wide_lanes(int64_t batch) { return ceil_div(batch, 4); }
+
+// The wide kernel serves float32 filters whose lanes need not follow orbital groups (one shared
+// geometry) and that have enough lanes to fill the GPU.
+bool wide_applies(const cdftb_operator* op, int64_t batch) {
+    bool on;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        on = g_wide;
+    }
+    return on && op->dtype == CDFTB_F32 && !op->per_system_geometry && wide_lanes(batch) >= 16;
+}
+
+template <int TZ>
+int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
+    using SH = WideShape<TZ>;
+    static bool configured = false;
+    if (!configured) {
+        int st = check(cudaFuncSetAttribute(slab_filter_wide_kernel<TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(SH::BYTES)));
+        if (st != CDFTB_OK) return st;
+        configured = true;
+    }
+    const int tiles_y = static_cast<int>(ceil_div(a.ny, TY));
+    a.tiles_z = static_cast<int>(ceil_div(a.nzp, TZ));
+    const int64_t tiles = int64_t(tiles_y) * a.tiles_z;
+    a.xchunk = xchunk > 0 ? (xchunk < a.nx ? xchunk : a.nx) : choose_chunk(a.nx, tiles * lanes, sm_count());
+    const int chunks = static_cast<int>(ceil_div(a.nx, a.xchunk));
+    static unsigned next_token = 0x40000000u;
+    for (int64_t first = 0; first < lanes; first += 65535) {
+        const int64_t count = (lanes - first) < 65535 ? (lanes - first) : 65535;
+        a.lane_first = first;
+        next_token = 0x40000000u | ((next_token + 1) & 0x3fffffffu);
+        a.token = next_token;
+        dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(chunks), static_cast<unsigned>(count));
+        slab_filter_wide_kernel<TZ><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
+        int st = check_launch();
+        if (st != CDFTB_OK) return st;
+    }
+    return CDFTB_OK;
+}
+
+int launch_wide_any_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lanes, cudaStream_t stream,
+                       int xchunk = 0) {
+    return tz == 36 ? launch_wide<36>(m, a, lanes, stream, xchunk) : launch_wide<32>(m, a, lanes, stream, xchunk);
+}
+
+// Lane buffers of 16-byte points described as 8-byte elements, two per point.
+int encode_wide_lane_maps(void* buf, int nzp, int ny, int nx, int64_t lanes, int tz, CUtensorMap* phi,
+                          CUtensorMap* prev) {
+    const int64_t lane_dims[4] = {2 * int64_t(nzp), ny, nx, lanes};
+    const unsigned phi_box[4] = {unsigned(2 * (tz + 18)), unsigned(NROW), 1, 1};
+    const unsigned prev_box[4] = {unsigned(2 * tz), unsigned(TY), 1, 1};
+    int st = encode_map(phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, phi_box);
+    if (st == CDFTB_OK) st = encode_map(prev, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, prev_box);
+    return st;
+}
+
+int pack_wide(const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz, int nzp, int64_t lanes,
+              void* dst, cudaStream_t stream) {
+    if ((reinterpret_cast<uintptr_t>(dst) & 15) != 0) return CDFTB_ERR_ARGUMENT;
+    const int64_t per_lane = int64_t(nx) * ny * nzp;
+    const unsigned ly = static_cast<unsigned>(std::min<int64_t>(lanes, 65535));
+    const unsigned bx = static_cast<unsigned>(
+        std::max<int64_t>(1, std::min<int64_t>(ceil_div(per_lane, 256), ceil_div(int64_t(148) * 16, ly))));
+    pack_wide_kernel<<<dim3(bx, ly), 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
+                                                       static_cast<float4*>(dst));
+    return check_launch();
+}
+
+int slab_filter_wide(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype, void* work,
+                     int64_t batch, const double* coefficients, int degree, cudaStream_t stream) {
+    const int nx = op->nx, ny = op->ny, nz = op->nz;
+    const int nzp = padded_z(nz);
+    const int64_t lanes = wide_lanes(batch);
+    const int64_t lane_bytes = int64_t(nx) * ny * nzp * 16;
+    char* w = static_cast<char*>(work);
+    void* buf[3] = {w, w + lanes * lane_bytes, w + 2 * lanes * lane_bytes};
+    int st = pack_wide(block, in_dtype, batch, nx, ny, nz, nzp, lanes, buf[2], stream);
+    if (st != CDFTB_OK) return st;
+    const int tz = choose_tz(nzp);
+    FilterMaps geo_maps{};
+    if ((st = prepare_geometry<LaneF2>(op, batch, w + 3 * lanes * lane_bytes, tz, false, &geo_maps, stream)) !=
+        CDFTB_OK)
+        return st;
+    FilterMaps maps[3];
+    for (int b = 0; b < 3; ++b)
+        if ((st = encode_wide_lane_maps(buf[b], nzp, ny, nx, lanes, tz, &maps[b].phi, &maps[b].prev)) != CDFTB_OK)
+            return st;
+    FilterArgs a = base_args(op, batch);
+    a.lanes_per_group = 0;
+    a.coef = coefficients;
+    a.degree = degree;
+    int y = 2, prev = -1;
+    for (int k = 1; k <= degree; ++k) {
+        const int dst = (k == 1) ? 0 : (k == 2 ? 1 : prev);
+        a.has_prev = prev >= 0;
+        a.step = k - 1;
+        a.final_out = k == degree;
+        a.out = a.final_out ? out : buf[dst];
+        a.out_dtype = out_dtype;
+        FilterMaps m = geo_maps;
+        m.phi = maps[y].phi;
+        m.prev = maps[prev >= 0 ? prev : y].prev;
+        if ((st = launch_wide_any_tz(tz, m, a, lanes, stream)) != CDFTB_OK) return st;
+        prev = y;
+        y = dst;
+    }
+    return CDFTB_OK;
+}
+
 }  // namespace
 
 int64_t slab_filter_work_bytes(const cdftb_operator* op, int64_t batch) {
     const int64_t sb = op->dtype == CDFTB_F32 ? 4 : 8;
-    return 3 * lanes_of(op, batch) * int64_t(op->nx) * op->ny * padded_z(op->nz) * 8 + geo_pack(op, batch).total() * sb;
+    const int64_t points = int64_t(op->nx) * op->ny * padded_z(op->nz);
+    int64_t lane_total = lanes_of(op, batch) * points * 8;
+    if (op->dtype == CDFTB_F32 && !op->per_system_geometry)  // room for the wide lanes too
+        lane_total = std::max<int64_t>(lane_total, wide_lanes(batch) * points * 16);
+    return 3 * lane_total + geo_pack(op, batch).total() * sb;
 }
 
 bool slab_filter_applies(const cdftb_operator* op) {
@@ -1084,6 +1603,8 @@ int64_t slab_apply_work_bytes(const cdftb_operator* op, int64_t batch) {
 
 int slab_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
                           void* work, int64_t batch, const double* coefficients, int degree, cudaStream_t stream) {
+    if (wide_applies(op, batch))
+        return slab_filter_wide(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
     if (op->dtype == CDFTB_F32)
         return slab_filter<LaneF2>(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
     return slab_filter<LaneD>(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
@@ -1094,6 +1615,12 @@ int slab_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dt
 extern "C" int cdftb_filter_autotune(int enable) {
     std::lock_guard<std::mutex> lock(cdftb::g_tune_mutex);
     cdftb::g_autotune = enable != 0;
+    return CDFTB_OK;
+}
+
+extern "C" int cdftb_filter_wide(int enable) {
+    std::lock_guard<std::mutex> lock(cdftb::g_tune_mutex);
+    cdftb::g_wide = enable != 0;
     return CDFTB_OK;
 }
 

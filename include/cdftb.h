@@ -113,6 +113,13 @@ int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_d
 int cdftb_filter_autotune(int enable);
 int cdftb_filter_tuned_tile(int nx, int ny, int nz, int dtype, int64_t lanes, int* tile_z, int* x_chunk);
 
+/* No reference counterpart: wide float32 lanes for cdftb_chebyshev_filter. Enabled (the default),
+ * a float32 filter with one shared geometry (no per-system geometry) and at least 16 lanes of four
+ * orbitals runs a kernel that holds four orbitals per 16-byte lane point instead of two: the same
+ * operator and recurrence, its sums in another order (float32 rounding differs from the two-orbital
+ * kernel). cdftb_chebyshev_filter_work_bytes covers both layouts. */
+int cdftb_filter_wide(int enable);
+
 /* No reference counterpart: the error flags the library's kernels set on the device (bit 0: a
  * bounded wait on a TMA barrier gave up). Synchronises the device, returns the flags in *flags and
  * clears them; status CDFTB_ERR_TIMEOUT when any flag was set. */

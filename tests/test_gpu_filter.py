@@ -181,3 +181,44 @@ def test_autotuned_apply_is_bit_identical(pkg, cuda):
         lib.cdftb_filter_autotune(1)
     assert torch.equal(tuned, heuristic)
     assert _device_status(pkg) == (0, 0)
+
+
+@pytest.mark.parametrize("shape", [(14, 13, 29), (21, 9, 65)])
+def test_wide_lanes_many_systems(pkg, cuda, shape):
+    """Four float32 orbitals per lane: 23 systems x 3 orbitals (lanes that mix systems, an empty last
+    slot), both z tiles (nz 29 -> 32 columns, nz 65 -> 36), against the oracle and against the
+    two-orbital lanes."""
+    from importlib import import_module
+
+    eigen = import_module(pkg.__name__ + ".eigen")
+    n = int(np.prod(shape))
+    systems, per = 23, 3
+    faces, inv, q = _random_operator(shape, seed=31)
+    rng = np.random.default_rng(32)
+    pots = rng.standard_normal((systems, n))
+    blocks = rng.standard_normal((systems, per, n))
+    bounds = [(0.5 + 0.01 * s, 3.0 + 0.05 * s, -1.0 - 0.02 * s) for s in range(systems)]
+    degree = 5
+    table = torch.tensor([eigen.chebyshev_coefficients(degree, *b) for b in bounds], dtype=torch.float64,
+                         device=cuda)
+    _, ham = _pair(pkg, cuda, shape, 0.25, faces, inv, q, pots[0], dtype=torch.float32)
+    lib = pkg._lib.library()
+
+    def run():
+        return eigen.filter_with_table(ham, _t(blocks, cuda), table, degree, orbitals_per_group=per,
+                                       potential=_t(pots, cuda)).cpu().numpy()
+
+    try:
+        lib.cdftb_filter_wide(1)
+        wide = run()
+        lib.cdftb_filter_wide(0)
+        narrow = run()
+    finally:
+        lib.cdftb_filter_wide(1)
+    for s in (0, 7, 22):
+        ham_o, _ = _pair(pkg, cuda, shape, 0.25, faces, inv, q, pots[s])
+        want = oeigen.chebyshev_filter(ham_o, blocks[s], degree, *bounds[s])
+        np.testing.assert_allclose(wide[s], want, rtol=0, atol=2e-5 * np.abs(want).max())
+    np.testing.assert_allclose(wide, narrow, rtol=0, atol=2e-5 * np.abs(narrow).max())
+    assert not np.array_equal(wide, narrow)  # the wide kernel ran (its sums run in another order)
+    assert _device_status(pkg) == (0, 0)

@@ -112,6 +112,7 @@ struct LaneF2 {
     static __device__ __forceinline__ E splat(S s) { return make_float2(s, s); }
     static __device__ __forceinline__ E zero() { return make_float2(0.f, 0.f); }
     static constexpr int ORBITALS = 2;
+    static constexpr bool WIDE = false;
     static constexpr CUtensorMapDataType GEO_TYPE = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
 };
 
@@ -125,6 +126,7 @@ struct LaneD {
     static __device__ __forceinline__ E splat(S s) { return s; }
     static __device__ __forceinline__ E zero() { return 0.0; }
     static constexpr int ORBITALS = 1;
+    static constexpr bool WIDE = false;
     static constexpr CUtensorMapDataType GEO_TYPE = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
 };
 
@@ -549,29 +551,34 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Wide float32 lanes: four orbitals per 16-byte element (float4), two packed f32x2 instructions per
-// element operation. The instructions that do not scale with the orbitals (addressing, barrier
-// waits, loads and stores of a point, the weights) are shared by four orbitals instead of two. The
-// roles and rings are those of slab_filter_kernel; two forms keep the registers within one CTA per
-// SM:
+// Wide lanes: 16 bytes per lane point -- four float32 orbitals (two packed f32x2 instructions per
+// element operation) or two float64 orbitals. The instructions that do not scale with the orbitals
+// (addressing, barrier waits, loads and stores of a point, the weights) are shared by twice as many
+// orbitals as in slab_filter_kernel. The roles and rings are those of slab_filter_kernel; two
+// forms keep the registers within one CTA per SM:
 //   pass item   streams its 22 nodes through a window of 8, forming each face as soon as its 8
 //               nodes are in and adding it at once to the 8 outputs it reaches (8 accumulators);
 //   march       keeps the last 8 nodes and the 8 outputs still open: each new x face is added to all
 //               of them, the newest output starts from its plane's y+z part, and the oldest one is
 //               complete after its last face.
-// Lanes run over the orbitals in order (lane l: orbitals 4l .. 4l+3); lanes aligned to orbital
-// groups (per-system geometry) keep the two-orbital kernel.
+// Lanes run over the orbitals in order (lane l: orbitals ORB l .. ORB l + ORB - 1); lanes aligned to
+// orbital groups (per-system geometry) keep slab_filter_kernel.
 
-struct Quad {
+struct WideF4 {  // four float32 orbitals
     using E = float4;
+    using T = float2;  // a tap or weight, twice
+    using S = float;
+    static constexpr int ORB = 4;
+    static constexpr bool WIDE = true;
+    static constexpr CUtensorMapDataType GEO_TYPE = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     static __device__ __forceinline__ float2 lo(E v) { return make_float2(v.x, v.y); }
     static __device__ __forceinline__ float2 hi(E v) { return make_float2(v.z, v.w); }
     static __device__ __forceinline__ E join(float2 a, float2 b) { return make_float4(a.x, a.y, b.x, b.y); }
-    // t (a float2 holding one tap twice) times v plus c
-    static __device__ __forceinline__ E fmat(float2 t, E v, E c) {
+    static __device__ __forceinline__ T splat(S s) { return make_float2(s, s); }
+    static __device__ __forceinline__ E fmat(T t, E v, E c) {
         return join(__ffma2_rn(t, lo(v), lo(c)), __ffma2_rn(t, hi(v), hi(c)));
     }
-    static __device__ __forceinline__ E mult(float2 t, E v) { return join(__fmul2_rn(t, lo(v)), __fmul2_rn(t, hi(v))); }
+    static __device__ __forceinline__ E mult(T t, E v) { return join(__fmul2_rn(t, lo(v)), __fmul2_rn(t, hi(v))); }
     static __device__ __forceinline__ E fma(E a, E b, E c) {
         return join(__ffma2_rn(lo(a), lo(b), lo(c)), __ffma2_rn(hi(a), hi(b), hi(c)));
     }
@@ -579,12 +586,43 @@ struct Quad {
     static __device__ __forceinline__ E add(E a, E b) { return join(__fadd2_rn(lo(a), lo(b)), __fadd2_rn(hi(a), hi(b))); }
     static __device__ __forceinline__ E neg(E a) { return make_float4(-a.x, -a.y, -a.z, -a.w); }
     static __device__ __forceinline__ E zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+    static __device__ __forceinline__ E make(const S* v) { return make_float4(v[0], v[1], v[2], v[3]); }
+    static __device__ __forceinline__ void parts(E v, S* out) {
+        out[0] = v.x;
+        out[1] = v.y;
+        out[2] = v.z;
+        out[3] = v.w;
+    }
 };
 
-constexpr int RW = 4;  // plane slots of the wide kernel (16-byte elements: a slot is ~34 KB)
+struct WideD2 {  // two float64 orbitals
+    using E = double2;
+    using T = double;
+    using S = double;
+    static constexpr int ORB = 2;
+    static constexpr bool WIDE = true;
+    static constexpr CUtensorMapDataType GEO_TYPE = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    static __device__ __forceinline__ T splat(S s) { return s; }
+    static __device__ __forceinline__ E fmat(T t, E v, E c) { return make_double2(::fma(t, v.x, c.x), ::fma(t, v.y, c.y)); }
+    static __device__ __forceinline__ E mult(T t, E v) { return make_double2(t * v.x, t * v.y); }
+    static __device__ __forceinline__ E fma(E a, E b, E c) {
+        return make_double2(::fma(a.x, b.x, c.x), ::fma(a.y, b.y, c.y));
+    }
+    static __device__ __forceinline__ E mul(E a, E b) { return make_double2(a.x * b.x, a.y * b.y); }
+    static __device__ __forceinline__ E add(E a, E b) { return make_double2(a.x + b.x, a.y + b.y); }
+    static __device__ __forceinline__ E neg(E a) { return make_double2(-a.x, -a.y); }
+    static __device__ __forceinline__ E zero() { return make_double2(0.0, 0.0); }
+    static __device__ __forceinline__ E make(const S* v) { return make_double2(v[0], v[1]); }
+    static __device__ __forceinline__ void parts(E v, S* out) {
+        out[0] = v.x;
+        out[1] = v.y;
+    }
+};
+
+constexpr int RW = 4;  // plane slots of the wide kernel (16-byte elements: a slot is 34-40 KB)
 static_assert(RW % NG == 0, "a slot is always served by the same pass group");
 
-template <int TZ>
+template <int TZ, int SB, int ORB>  // SB: bytes of a geometry element; ORB: potentials per lane
 struct WideShape {
     static constexpr int EB = 16;
     static constexpr int MW = TY * TZ / 32;
@@ -598,20 +636,20 @@ struct WideShape {
     static constexpr int ZROW = TZ + 2;
     static constexpr unsigned TX_PHI = NROW * BW * EB;
     static constexpr unsigned TX_PREV = TY * TZ * EB;
-    static constexpr unsigned TX_W0 = TY * TZ * 4;
-    static constexpr unsigned TX_W1 = (TY + 7) * TZ * 4;
-    static constexpr unsigned TX_W2 = TY * (TZ + 8) * 4;
-    static constexpr unsigned TX_INV = TY * TZ * 4;
-    static constexpr unsigned TX_POT = TY * TZ * 4;
+    static constexpr unsigned TX_W0 = TY * TZ * SB;
+    static constexpr unsigned TX_W1 = (TY + 7) * TZ * SB;
+    static constexpr unsigned TX_W2 = TY * (TZ + 8) * SB;
+    static constexpr unsigned TX_INV = TY * TZ * SB;
+    static constexpr unsigned TX_POT = TY * TZ * SB;
     static constexpr size_t O_PHI = 0;
     static constexpr size_t O_PREV = O_PHI + align128(TX_PHI);
     static constexpr size_t O_W0 = O_PREV + align128(TX_PREV);
     static constexpr size_t O_W1 = O_W0 + align128(TX_W0);
     static constexpr size_t O_W2 = O_W1 + align128(TX_W1);
     static constexpr size_t O_INV = O_W2 + align128(TX_W2);
-    static constexpr size_t O_POT = O_INV + align128(TX_INV);  // four potentials, TX_POT apart (128-aligned)
+    static constexpr size_t O_POT = O_INV + align128(TX_INV);  // ORB potentials, POT_STEP apart
     static constexpr size_t POT_STEP = align128(TX_POT);
-    static constexpr size_t SLOT = O_POT + 4 * POT_STEP;
+    static constexpr size_t SLOT = O_POT + ORB * POT_STEP;
     static constexpr size_t O_YZ = RW * SLOT;
     static constexpr size_t YZ_Z = size_t(TY) * TZ * EB;
     static constexpr size_t YZ_SLOT = align128(YZ_Z + size_t(TY) * ZROW * EB);
@@ -622,11 +660,13 @@ struct WideShape {
     static_assert(BYTES <= 232448, "fits the opt-in shared memory of one CTA");
 };
 
-template <int TZ>
-__global__ void __launch_bounds__(WideShape<TZ>::T, 1)
+template <typename W, int TZ>
+__global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::T, 1)
     slab_filter_wide_kernel(const __grid_constant__ FilterMaps maps, const FilterArgs a) {
-    using E = float4;
-    using SH = WideShape<TZ>;
+    using E = typename W::E;
+    using S = typename W::S;
+    constexpr int ORB = W::ORB;
+    using SH = WideShape<TZ, sizeof(S), ORB>;
     constexpr int BW = SH::BW;
     extern __shared__ __align__(1024) unsigned char smem[];
     const unsigned bar_full = smem_u32(smem + SH::O_BAR);
@@ -646,16 +686,16 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
     const int npl = xe + HALO + 1 - q0;
     const bool has_prev = a.has_prev != 0;
 
-    // the lane's four orbitals (an empty slot borrows the first orbital's group for its lookups)
-    int64_t orb[4];
-    int grp[4];
+    // the lane's orbitals (an empty slot borrows the first orbital's group for its lookups)
+    int64_t orb[ORB];
+    int grp[ORB];
 #pragma unroll
-    for (int h = 0; h < 4; ++h) {
-        const int64_t o = int64_t(4) * lane + h;
+    for (int h = 0; h < ORB; ++h) {
+        const int64_t o = int64_t(ORB) * lane + h;
         orb[h] = o < a.batch ? o : -1;
     }
 #pragma unroll
-    for (int h = 0; h < 4; ++h) {
+    for (int h = 0; h < ORB; ++h) {
         const int64_t o = orb[h] >= 0 ? orb[h] : orb[0];
         grp[h] = a.shared_potential ? 0 : static_cast<int>(o / a.orb_per_group);
     }
@@ -674,15 +714,15 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
     }
     __syncthreads();
 
-    float2 tap[8];
+    typename W::T tap[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) tap[j] = make_float2(static_cast<float>(a.taps[j]), static_cast<float>(a.taps[j]));
+    for (int j = 0; j < 8; ++j) tap[j] = W::splat(static_cast<S>(a.taps[j]));
 
     if (warp == SH::MW + SH::PW) {
         // ------------------------------------------------------------------ producer
         if ((t & 31) != 0) return;
         const unsigned tx = SH::TX_PHI + (has_prev ? SH::TX_PREV : 0) + SH::TX_W0 + SH::TX_W1 + SH::TX_W2 +
-                            SH::TX_INV + 4 * SH::TX_POT;
+                            SH::TX_INV + ORB * SH::TX_POT;
         int issued = 0;
         int s = 0, ph = 1;
         for (int n = 0; n < npl; ++n) {
@@ -699,7 +739,7 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
             tma_load_4d(slot + SH::O_W2, &maps.w2, z0, y0, q, 0, full);
             tma_load_4d(slot + SH::O_INV, &maps.inv, z0, y0, q - HALO, 0, full);
 #pragma unroll
-            for (int h = 0; h < 4; ++h)
+            for (int h = 0; h < ORB; ++h)
                 tma_load_4d(slot + SH::O_POT + h * SH::POT_STEP, &maps.pot, z0, y0, q - HALO, grp[h], full);
             issued = n + 1;
             if (++s == RW) {
@@ -729,7 +769,7 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
             active = z0 + zc < nz;
             nb = zc + 8;
             ns = BW;
-            wb = SH::O_W1 / 4 + zc;
+            wb = SH::O_W1 / sizeof(S) + zc;
             ws = TZ;
             ob = zc;
             os = TZ;
@@ -742,7 +782,7 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
             active = y0 + ry < ny && z0 + zs < nz;
             nb = (ry + HALO) * BW + zs + 1;
             ns = 1;
-            wb = SH::O_W2 / 4 + ry * (TZ + 8) + zs;
+            wb = SH::O_W2 / sizeof(S) + ry * (TZ + 8) + zs;
             ws = 1;
             ob = int(SH::YZ_Z / sizeof(E)) + ry * SH::ZROW + zs;
             os = 1;
@@ -759,7 +799,7 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
                 if (active) {
                     const unsigned char* slot = smem + s * SH::SLOT;
                     const E* nodes = reinterpret_cast<const E*>(slot) + nb;
-                    const float* w = reinterpret_cast<const float*>(slot) + wb;
+                    const S* w = reinterpret_cast<const S*>(slot) + wb;
                     E* out = reinterpret_cast<E*>(smem + SH::O_YZ + ys * SH::YZ_SLOT) + ob;
                     E win[8], acc[TY];
 #pragma unroll
@@ -767,16 +807,15 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
                         win[r & 7] = nodes[r * ns];
                         if (r >= 7) {
                             const int rf = r - 7;  // face rf from nodes rf .. rf + 7
-                            E sum = Quad::zero();
+                            E sum = W::zero();
 #pragma unroll
-                            for (int j = 0; j < 8; ++j) sum = Quad::fmat(tap[j], win[(rf + j) & 7], sum);
-                            const float wf = w[rf * ws];
-                            const E f = Quad::mult(make_float2(wf, wf), sum);
+                            for (int j = 0; j < 8; ++j) sum = W::fmat(tap[j], win[(rf + j) & 7], sum);
+                            const E f = W::mult(W::splat(w[rf * ws]), sum);
                             // face rf reaches outputs o = rf - 7 .. rf with tap o + 7 - rf
 #pragma unroll
                             for (int o = 0; o < TY; ++o) {
                                 if (o < rf - 7 || o > rf) continue;
-                                acc[o] = (o == rf) ? Quad::mult(tap[7], f) : Quad::fmat(tap[o + 7 - rf], f, acc[o]);
+                                acc[o] = (o == rf) ? W::mult(tap[7], f) : W::fmat(tap[o + 7 - rf], f, acc[o]);
                             }
                         }
                     }
@@ -809,26 +848,26 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
     const int64_t plane_n = int64_t(ny) * nz;
     const int own = ty * TZ + tz;
 
-    E cc = Quad::zero(), ca = Quad::zero(), cb = Quad::zero();
+    E cc = W::zero(), ca = W::zero(), cb = W::zero();
     if (!a.apply_only) {
-        float c3[3][4];
+        S c3[3][ORB];
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
+        for (int h = 0; h < ORB; ++h) {
             const int64_t o = orb[h] >= 0 ? orb[h] : orb[0];
             const double* r = a.coef + ((o / a.orb_per_group) * a.degree + a.step) * 3;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) c3[k][h] = static_cast<float>(r[k]);
+            for (int k = 0; k < 3; ++k) c3[k][h] = static_cast<S>(r[k]);
         }
-        cc = make_float4(c3[0][0], c3[0][1], c3[0][2], c3[0][3]);
-        ca = make_float4(c3[1][0], c3[1][1], c3[1][2], c3[1][3]);
-        cb = make_float4(c3[2][0], c3[2][1], c3[2][2], c3[2][3]);
+        cc = W::make(c3[0]);
+        ca = W::make(c3[1]);
+        cb = W::make(c3[2]);
     }
 
     E phq[8], acc[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        phq[j] = Quad::zero();
-        acc[j] = Quad::zero();
+        phq[j] = W::zero();
+        acc[j] = W::zero();
     }
 
     int s = 0, sph = 0;
@@ -843,22 +882,22 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
             phq[g] = reinterpret_cast<const E*>(slot + SH::O_PHI)[(ty + HALO) * BW + tz + 8];
             E face;
             {
-                E sum = Quad::zero();
+                E sum = W::zero();
 #pragma unroll
-                for (int j = 0; j < 8; ++j) sum = Quad::fmat(tap[j], phq[(g + 1 + j) & 7], sum);
-                const float wx = own_in ? reinterpret_cast<const float*>(slot + SH::O_W0)[own] : 0.f;
-                face = Quad::mult(make_float2(wx, wx), sum);  // x face q - 4
+                for (int j = 0; j < 8; ++j) sum = W::fmat(tap[j], phq[(g + 1 + j) & 7], sum);
+                const S wx = own_in ? reinterpret_cast<const S*>(slot + SH::O_W0)[own] : S(0);
+                face = W::mult(W::splat(wx), sum);  // x face q - 4
             }
             // the face reaches the open outputs q - 7 .. q (slot (g - d) & 7 holds output q - d, tap 7 - d)
 #pragma unroll
-            for (int d = 1; d < 8; ++d) acc[(g - d) & 7] = Quad::fmat(tap[7 - d], face, acc[(g - d) & 7]);
-            E yz = Quad::zero();
+            for (int d = 1; d < 8; ++d) acc[(g - d) & 7] = W::fmat(tap[7 - d], face, acc[(g - d) & 7]);
+            E yz = W::zero();
             if (q >= xa && q <= xe) {
                 const int m = q - xa;
                 const int ys = m & (RY - 1);
                 if (!warp_wait(bar_yfull + 8 * ys, (m / RY) & 1, a.token)) return;
                 const unsigned char* yzs = smem + SH::O_YZ + ys * SH::YZ_SLOT;
-                yz = Quad::add(reinterpret_cast<const E*>(yzs)[own],
+                yz = W::add(reinterpret_cast<const E*>(yzs)[own],
                                reinterpret_cast<const E*>(yzs + SH::YZ_Z)[ty * SH::ZROW + tz]);
                 __syncwarp();
                 if ((t & 31) == 0) mbar_arrive(bar_yempty + 8 * ys);
@@ -867,33 +906,36 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
             if (i >= xa && own_pad) {
                 const E div = acc[(g + 1) & 7];
                 const int64_t pt = int64_t(i) * plane_n + (own_in ? int64_t(y) * nz + z : 0);
-                E res = Quad::zero();
+                E res = W::zero();
                 if (own_in) {
                     const E phi = phq[(g + 1) & 7];
-                    const float inv = reinterpret_cast<const float*>(slot + SH::O_INV)[own];
-                    const E kin = Quad::mult(make_float2(0.5f * inv, 0.5f * inv), div);
+                    const S inv = reinterpret_cast<const S*>(slot + SH::O_INV)[own];
+                    const E kin = W::mult(W::splat(S(0.5) * inv), div);
                     if (a.kinetic_only) {
                         res = kin;
                     } else {
-                        const float* pot = reinterpret_cast<const float*>(slot + SH::O_POT);
-                        const E potv = make_float4(pot[own], pot[SH::POT_STEP / 4 + own], pot[2 * SH::POT_STEP / 4 + own],
-                                                   pot[3 * SH::POT_STEP / 4 + own]);
-                        const E applied = Quad::fma(phi, potv, kin);
+                        S pv[ORB];
+#pragma unroll
+                        for (int h = 0; h < ORB; ++h)
+                            pv[h] = reinterpret_cast<const S*>(slot + SH::O_POT + h * SH::POT_STEP)[own];
+                        const E potv = W::make(pv);
+                        const E applied = W::fma(phi, potv, kin);
                         if (a.apply_only) {
                             res = applied;
                         } else {
-                            res = Quad::mul(Quad::fma(Quad::neg(cc), phi, applied), ca);
+                            res = W::mul(W::fma(W::neg(cc), phi, applied), ca);
                             if (has_prev)
-                                res = Quad::fma(Quad::neg(cb), reinterpret_cast<const E*>(slot + SH::O_PREV)[own], res);
+                                res = W::fma(W::neg(cb), reinterpret_cast<const E*>(slot + SH::O_PREV)[own], res);
                         }
                     }
                 }
                 if (a.final_out) {
                     if (own_in) {
-                        const float rv[4] = {res.x, res.y, res.z, res.w};
+                        S rv[ORB];
+                        W::parts(res, rv);
 #pragma unroll
-                        for (int h = 0; h < 4; ++h)
-                            if (orb[h] >= 0) store_as<float>(a.out, a.out_dtype, orb[h] * (plane_n * nx) + pt, rv[h]);
+                        for (int h = 0; h < ORB; ++h)
+                            if (orb[h] >= 0) store_as<S>(a.out, a.out_dtype, orb[h] * (plane_n * nx) + pt, rv[h]);
                     }
                 } else {
                     E* out = static_cast<E*>(a.out);
@@ -902,7 +944,7 @@ __global__ void __launch_bounds__(WideShape<TZ>::T, 1)
             }
             // the newest output, q, opens from its y+z part and its first face (its slot held output
             // q - 8, completed on the previous plane)
-            acc[g] = Quad::fmat(tap[7], face, yz);
+            acc[g] = W::fmat(tap[7], face, yz);
             __syncwarp();
             if ((t & 31) == 0) mbar_arrive(bar_empty + 8 * s);
             if (++s == RW) {
@@ -964,18 +1006,22 @@ __global__ void pack_lanes_kernel(const void* __restrict__ in, int in_dtype, int
     }
 }
 
-// Wide float32 lanes from a caller block: lane l holds orbitals 4l .. 4l+3 as a float4 per point,
-// padding and missing orbitals zero. blockIdx.y walks the lanes; one point per thread.
+// Wide lanes from a caller block: lane l holds orbitals ORB l .. ORB l + ORB - 1 as one 16-byte
+// element per point, padding and missing orbitals zero. blockIdx.y walks the lanes; one point per
+// thread.
+template <typename W>
 __global__ void pack_wide_kernel(const void* __restrict__ in, int in_dtype, int64_t batch, int nx, int ny, int nz,
-                                 int nzp, int64_t lanes, float4* __restrict__ out) {
+                                 int nzp, int64_t lanes, typename W::E* __restrict__ out) {
+    using S = typename W::S;
+    constexpr int ORB = W::ORB;
     const int64_t per_lane = int64_t(nx) * ny * nzp;
     const int64_t n_points = int64_t(nx) * ny * nz;
     const bool narrow = per_lane <= 0xffffffffll;
     for (int64_t l = blockIdx.y; l < lanes; l += gridDim.y) {
-        float4* dst = out + l * per_lane;
-        int64_t orb[4];
+        typename W::E* dst = out + l * per_lane;
+        int64_t orb[ORB];
 #pragma unroll
-        for (int h = 0; h < 4; ++h) orb[h] = (4 * l + h < batch) ? 4 * l + h : -1;
+        for (int h = 0; h < ORB; ++h) orb[h] = (ORB * l + h < batch) ? ORB * l + h : -1;
         for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < per_lane;
              k += int64_t(gridDim.x) * blockDim.x) {
             int64_t xy;
@@ -988,14 +1034,16 @@ __global__ void pack_wide_kernel(const void* __restrict__ in, int in_dtype, int6
                 xy = k / nzp;
                 zp = static_cast<int>(k - xy * nzp);
             }
-            float v[4] = {0.f, 0.f, 0.f, 0.f};
+            S v[ORB];
+#pragma unroll
+            for (int h = 0; h < ORB; ++h) v[h] = S(0);
             if (zp < nz) {
                 const int64_t pt = xy * nz + zp;
 #pragma unroll
-                for (int h = 0; h < 4; ++h)
-                    if (orb[h] >= 0) v[h] = load_as<float>(in, in_dtype, orb[h] * n_points + pt);
+                for (int h = 0; h < ORB; ++h)
+                    if (orb[h] >= 0) v[h] = load_as<S>(in, in_dtype, orb[h] * n_points + pt);
             }
-            dst[k] = make_float4(v[0], v[1], v[2], v[3]);
+            dst[k] = W::make(v);
         }
     }
 }
@@ -1267,6 +1315,103 @@ int launch_any_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lane
                     : launch_slab<Lane, 32>(m, a, lanes, stream, xchunk);
 }
 
+// ---- wide lanes (slab_filter_wide_kernel): launch, lane maps, packing
+bool g_wide = true;  // guarded by g_tune_mutex (declared below with the tuner)
+
+template <typename W, int TZ>
+int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
+    using SH = WideShape<TZ, sizeof(typename W::S), W::ORB>;
+    static bool configured = false;
+    if (!configured) {
+        int st = check(cudaFuncSetAttribute(slab_filter_wide_kernel<W, TZ>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(SH::BYTES)));
+        if (st != CDFTB_OK) return st;
+        configured = true;
+    }
+    const int tiles_y = static_cast<int>(ceil_div(a.ny, TY));
+    a.tiles_z = static_cast<int>(ceil_div(a.nzp, TZ));
+    const int64_t tiles = int64_t(tiles_y) * a.tiles_z;
+    a.xchunk = xchunk > 0 ? (xchunk < a.nx ? xchunk : a.nx) : choose_chunk(a.nx, tiles * lanes, sm_count());
+    a.lanes_per_group = 0;
+    const int chunks = static_cast<int>(ceil_div(a.nx, a.xchunk));
+    static unsigned next_token = 0x40000000u;
+    for (int64_t first = 0; first < lanes; first += 65535) {
+        const int64_t count = (lanes - first) < 65535 ? (lanes - first) : 65535;
+        a.lane_first = first;
+        next_token = 0x40000000u | ((next_token + 1) & 0x3fffffffu);
+        a.token = next_token;
+        dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(chunks), static_cast<unsigned>(count));
+        slab_filter_wide_kernel<W, TZ><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
+        int st = check_launch();
+        if (st != CDFTB_OK) return st;
+    }
+    return CDFTB_OK;
+}
+
+// Lane buffers of 16-byte points described as 8-byte elements, two per point.
+int encode_wide_lane_maps(void* buf, int nzp, int ny, int nx, int64_t lanes, int tz, CUtensorMap* phi,
+                          CUtensorMap* prev) {
+    const int64_t lane_dims[4] = {2 * int64_t(nzp), ny, nx, lanes};
+    const unsigned phi_box[4] = {unsigned(2 * (tz + 18)), unsigned(NROW), 1, 1};
+    const unsigned prev_box[4] = {unsigned(2 * tz), unsigned(TY), 1, 1};
+    int st = encode_map(phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, phi_box);
+    if (st == CDFTB_OK) st = encode_map(prev, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, prev_box);
+    return st;
+}
+
+template <typename W>
+int pack_wide(const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz, int nzp, int64_t lanes,
+              void* dst, cudaStream_t stream) {
+    if ((reinterpret_cast<uintptr_t>(dst) & 15) != 0) return CDFTB_ERR_ARGUMENT;
+    const int64_t per_lane = int64_t(nx) * ny * nzp;
+    const unsigned ly = static_cast<unsigned>(std::min<int64_t>(lanes, 65535));
+    const unsigned bx = static_cast<unsigned>(
+        std::max<int64_t>(1, std::min<int64_t>(ceil_div(per_lane, 256), ceil_div(int64_t(148) * 16, ly))));
+    pack_wide_kernel<W><<<dim3(bx, ly), 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
+                                                          static_cast<typename W::E*>(dst));
+    return check_launch();
+}
+
+// The same steps for both lane layouts: two-orbital (LaneF2) or one-orbital (LaneD) lane points of
+// 8 bytes, or wide ones of 16 bytes (WideF4, WideD2).
+template <typename L>
+int64_t lane_count(const cdftb_operator* op, int64_t batch) {
+    if constexpr (L::WIDE)
+        return ceil_div(batch, L::ORB);
+    else
+        return lanes_of(op, batch);
+}
+
+template <typename L>
+constexpr int64_t lane_point_bytes() {
+    return L::WIDE ? 16 : 8;
+}
+
+template <typename L>
+int encode_lanes(void* buf, int nzp, int ny, int nx, int64_t lanes, int tz, CUtensorMap* phi, CUtensorMap* prev) {
+    if constexpr (L::WIDE)
+        return encode_wide_lane_maps(buf, nzp, ny, nx, lanes, tz, phi, prev);
+    else
+        return encode_lane_maps(buf, nzp, ny, nx, lanes, tz, phi, prev);
+}
+
+template <typename L>
+int pack_lanes(const cdftb_operator* op, const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz,
+               int nzp, int64_t lanes, void* dst, cudaStream_t stream) {
+    if constexpr (L::WIDE)
+        return pack_wide<L>(block, in_dtype, batch, nx, ny, nz, nzp, lanes, dst, stream);
+    else
+        return pack_block<L>(op, block, in_dtype, batch, nx, ny, nz, nzp, lanes, dst, stream);
+}
+
+template <typename L>
+int launch_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
+    if constexpr (L::WIDE)
+        return tz == 36 ? launch_wide<L, 36>(m, a, lanes, stream, xchunk) : launch_wide<L, 32>(m, a, lanes, stream, xchunk);
+    else
+        return launch_any_tz<L>(tz, m, a, lanes, stream, xchunk);
+}
+
 // ---- the tile autotuner
 // The z tile (32 or 36 columns) and the x chunk of a slab launch decide the CTA count, the waves
 // and the halo work; which wins depends on the grid, the lane count and the GPU. With the autotuner
@@ -1280,15 +1425,16 @@ struct TileChoice {
     int xchunk;  // 0: choose_chunk
 };
 
-using TuneKey = std::tuple<int, int, int, int, int, int64_t>;  // device, nx, ny, nz, precision, lanes
+// device, nx, ny, nz, precision (+ CDFTB_WIDE_LANES for the wide kernel), lanes
+using TuneKey = std::tuple<int, int, int, int, int, int64_t>;
 std::mutex g_tune_mutex;
 std::map<TuneKey, TileChoice> g_tuned;
 bool g_autotune = false;
 
-TuneKey tune_key(const cdftb_operator* op, int64_t lanes) {
+TuneKey tune_key(const cdftb_operator* op, int64_t lanes, bool wide) {
     int dev = 0;
     cudaGetDevice(&dev);
-    return TuneKey(dev, op->nx, op->ny, op->nz, op->dtype, lanes);
+    return TuneKey(dev, op->nx, op->ny, op->nz, op->dtype + (wide ? CDFTB_WIDE_LANES : 0), lanes);
 }
 
 bool tuned_choice(const TuneKey& key, TileChoice* out) {
@@ -1321,7 +1467,7 @@ int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf
         FilterMaps m{};
         const bool kinetic = apply != nullptr && apply->kinetic_only;
         if ((st = prepare_geometry<Lane>(op, batch, geo_base, tz, kinetic, &m, stream)) != CDFTB_OK) break;
-        if ((st = encode_lane_maps(buf[2], nzp, ny, nx, lanes, tz, &m.phi, &m.prev)) != CDFTB_OK) break;
+        if ((st = encode_lanes<Lane>(buf[2], nzp, ny, nx, lanes, tz, &m.phi, &m.prev)) != CDFTB_OK) break;
         FilterArgs a = base_args(op, batch);
         if (apply) {
             a = *apply;
@@ -1342,9 +1488,9 @@ int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf
             if (chunks < 1 || (c == 4 && chunks <= 4)) continue;  // the heuristic's chunk, when not already tried
             const int xchunk = static_cast<int>(ceil_div(nx, chunks));
             if (chunks > 1 && (xchunk < 8 || ceil_div(nx, xchunk) != chunks)) continue;
-            if ((st = launch_any_tz<Lane>(tz, m, a, lanes, stream, xchunk)) != CDFTB_OK) break;
+            if ((st = launch_tz<Lane>(tz, m, a, lanes, stream, xchunk)) != CDFTB_OK) break;
             if ((st = check(cudaEventRecord(e0, stream))) != CDFTB_OK) break;
-            for (int r = 0; r < 3 && st == CDFTB_OK; ++r) st = launch_any_tz<Lane>(tz, m, a, lanes, stream, xchunk);
+            for (int r = 0; r < 3 && st == CDFTB_OK; ++r) st = launch_tz<Lane>(tz, m, a, lanes, stream, xchunk);
             if (st != CDFTB_OK) break;
             if ((st = check(cudaEventRecord(e1, stream))) != CDFTB_OK) break;
             if ((st = check(cudaEventSynchronize(e1))) != CDFTB_OK) break;
@@ -1367,14 +1513,14 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
                 int64_t batch, const double* coefficients, int degree, cudaStream_t stream) {
     const int nx = op->nx, ny = op->ny, nz = op->nz;
     const int nzp = padded_z(nz);
-    const int64_t lanes = lanes_of(op, batch);
-    const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
+    const int64_t lanes = lane_count<Lane>(op, batch);
+    const int64_t lane_bytes = int64_t(nx) * ny * nzp * lane_point_bytes<Lane>();
     char* w = static_cast<char*>(work);
     void* buf[3] = {w, w + lanes * lane_bytes, w + 2 * lanes * lane_bytes};
-    int st = pack_block<Lane>(op, block, in_dtype, batch, nx, ny, nz, nzp, lanes, buf[2], stream);
+    int st = pack_lanes<Lane>(op, block, in_dtype, batch, nx, ny, nz, nzp, lanes, buf[2], stream);
     if (st != CDFTB_OK) return st;
     TileChoice choice{choose_tz(nzp), 0};
-    const TuneKey key = tune_key(op, lanes);
+    const TuneKey key = tune_key(op, lanes, Lane::WIDE);
     bool autotune;
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -1393,7 +1539,8 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
         return st;
     FilterMaps maps[3];
     for (int b = 0; b < 3; ++b)
-        if ((st = encode_lane_maps(buf[b], nzp, ny, nx, lanes, tz, &maps[b].phi, &maps[b].prev)) != CDFTB_OK) return st;
+        if ((st = encode_lanes<Lane>(buf[b], nzp, ny, nx, lanes, tz, &maps[b].phi, &maps[b].prev)) != CDFTB_OK)
+            return st;
     FilterArgs a = base_args(op, batch);
     a.coef = coefficients;
     a.degree = degree;
@@ -1410,7 +1557,7 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
         FilterMaps m = geo_maps;
         m.phi = maps[y].phi;
         m.prev = maps[prev >= 0 ? prev : y].prev;
-        if ((st = launch_any_tz<Lane>(tz, m, a, lanes, stream, choice.xchunk)) != CDFTB_OK) return st;
+        if ((st = launch_tz<Lane>(tz, m, a, lanes, stream, choice.xchunk)) != CDFTB_OK) return st;
         prev = y;
         y = dst;
     }
@@ -1422,13 +1569,13 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
                int64_t batch, int kinetic_only, cudaStream_t stream) {
     const int nx = op->nx, ny = op->ny, nz = op->nz;
     const int nzp = padded_z(nz);
-    const int64_t lanes = lanes_of(op, batch);
-    const int64_t lane_bytes = int64_t(nx) * ny * nzp * 8;
+    const int64_t lanes = lane_count<Lane>(op, batch);
+    const int64_t lane_bytes = int64_t(nx) * ny * nzp * lane_point_bytes<Lane>();
     char* w = static_cast<char*>(work);
     TileChoice choice{choose_tz(nzp), 0};
-    const TuneKey key = tune_key(op, lanes);
+    const TuneKey key = tune_key(op, lanes, Lane::WIDE);
     const bool known = tuned_choice(key, &choice);
-    int st = pack_block<Lane>(op, phi, in_dtype, batch, nx, ny, nz, nzp, lanes, w, stream);
+    int st = pack_lanes<Lane>(op, phi, in_dtype, batch, nx, ny, nz, nzp, lanes, w, stream);
     if (st != CDFTB_OK) return st;
     bool autotune;
     {
@@ -1455,7 +1602,7 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
     if ((st = prepare_geometry<Lane>(op, batch, w + lanes * lane_bytes, tz, kinetic_only != 0, &m, stream)) !=
         CDFTB_OK)
         return st;
-    if ((st = encode_lane_maps(w, nzp, ny, nx, lanes, tz, &m.phi, &m.prev)) != CDFTB_OK) return st;
+    if ((st = encode_lanes<Lane>(w, nzp, ny, nx, lanes, tz, &m.phi, &m.prev)) != CDFTB_OK) return st;
     FilterArgs a = base_args(op, batch);
     a.apply_only = 1;
     a.kinetic_only = kinetic_only != 0;
@@ -1463,132 +1610,37 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
     a.final_out = 1;
     a.out = out;
     a.out_dtype = out_dtype;
-    return launch_any_tz<Lane>(tz, m, a, lanes, stream, choice.xchunk);
+    return launch_tz<Lane>(tz, m, a, lanes, stream, choice.xchunk);
 }
 
-// ---- wide float32 lanes (slab_filter_wide_kernel)
-bool g_wide = true;  // guarded by g_tune_mutex
-
-int64_t wide_lanes(int64_t batch) { return ceil_div(batch, 4); }
-
-// The wide kernel serves float32 filters whose lanes need not follow orbital groups (one shared
-// geometry) and that have enough lanes to fill the GPU.
+// Wide lanes serve filters and applies with one shared geometry (lanes need not follow orbital
+// groups) and at least 16 wide lanes, so that the launch still fills the GPU.
 bool wide_applies(const cdftb_operator* op, int64_t batch) {
     bool on;
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         on = g_wide;
     }
-    return on && op->dtype == CDFTB_F32 && !op->per_system_geometry && wide_lanes(batch) >= 16;
+    const int per = op->dtype == CDFTB_F32 ? WideF4::ORB : WideD2::ORB;
+    return on && !op->per_system_geometry && ceil_div(batch, per) >= 16;
 }
 
-template <int TZ>
-int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
-    using SH = WideShape<TZ>;
-    static bool configured = false;
-    if (!configured) {
-        int st = check(cudaFuncSetAttribute(slab_filter_wide_kernel<TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(SH::BYTES)));
-        if (st != CDFTB_OK) return st;
-        configured = true;
+// Lane bytes of the larger layout a call may use (the wide one when it can apply).
+int64_t lane_bytes_total(const cdftb_operator* op, int64_t batch) {
+    const int64_t points = int64_t(op->nx) * op->ny * padded_z(op->nz);
+    int64_t total = lanes_of(op, batch) * points * 8;
+    if (!op->per_system_geometry) {
+        const int per = op->dtype == CDFTB_F32 ? WideF4::ORB : WideD2::ORB;
+        total = std::max<int64_t>(total, ceil_div(batch, per) * points * 16);
     }
-    const int tiles_y = static_cast<int>(ceil_div(a.ny, TY));
-    a.tiles_z = static_cast<int>(ceil_div(a.nzp, TZ));
-    const int64_t tiles = int64_t(tiles_y) * a.tiles_z;
-    a.xchunk = xchunk > 0 ? (xchunk < a.nx ? xchunk : a.nx) : choose_chunk(a.nx, tiles * lanes, sm_count());
-    const int chunks = static_cast<int>(ceil_div(a.nx, a.xchunk));
-    static unsigned next_token = 0x40000000u;
-    for (int64_t first = 0; first < lanes; first += 65535) {
-        const int64_t count = (lanes - first) < 65535 ? (lanes - first) : 65535;
-        a.lane_first = first;
-        next_token = 0x40000000u | ((next_token + 1) & 0x3fffffffu);
-        a.token = next_token;
-        dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(chunks), static_cast<unsigned>(count));
-        slab_filter_wide_kernel<TZ><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
-        int st = check_launch();
-        if (st != CDFTB_OK) return st;
-    }
-    return CDFTB_OK;
-}
-
-int launch_wide_any_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lanes, cudaStream_t stream,
-                       int xchunk = 0) {
-    return tz == 36 ? launch_wide<36>(m, a, lanes, stream, xchunk) : launch_wide<32>(m, a, lanes, stream, xchunk);
-}
-
-// Lane buffers of 16-byte points described as 8-byte elements, two per point.
-int encode_wide_lane_maps(void* buf, int nzp, int ny, int nx, int64_t lanes, int tz, CUtensorMap* phi,
-                          CUtensorMap* prev) {
-    const int64_t lane_dims[4] = {2 * int64_t(nzp), ny, nx, lanes};
-    const unsigned phi_box[4] = {unsigned(2 * (tz + 18)), unsigned(NROW), 1, 1};
-    const unsigned prev_box[4] = {unsigned(2 * tz), unsigned(TY), 1, 1};
-    int st = encode_map(phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, phi_box);
-    if (st == CDFTB_OK) st = encode_map(prev, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, prev_box);
-    return st;
-}
-
-int pack_wide(const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz, int nzp, int64_t lanes,
-              void* dst, cudaStream_t stream) {
-    if ((reinterpret_cast<uintptr_t>(dst) & 15) != 0) return CDFTB_ERR_ARGUMENT;
-    const int64_t per_lane = int64_t(nx) * ny * nzp;
-    const unsigned ly = static_cast<unsigned>(std::min<int64_t>(lanes, 65535));
-    const unsigned bx = static_cast<unsigned>(
-        std::max<int64_t>(1, std::min<int64_t>(ceil_div(per_lane, 256), ceil_div(int64_t(148) * 16, ly))));
-    pack_wide_kernel<<<dim3(bx, ly), 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
-                                                       static_cast<float4*>(dst));
-    return check_launch();
-}
-
-int slab_filter_wide(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype, void* work,
-                     int64_t batch, const double* coefficients, int degree, cudaStream_t stream) {
-    const int nx = op->nx, ny = op->ny, nz = op->nz;
-    const int nzp = padded_z(nz);
-    const int64_t lanes = wide_lanes(batch);
-    const int64_t lane_bytes = int64_t(nx) * ny * nzp * 16;
-    char* w = static_cast<char*>(work);
-    void* buf[3] = {w, w + lanes * lane_bytes, w + 2 * lanes * lane_bytes};
-    int st = pack_wide(block, in_dtype, batch, nx, ny, nz, nzp, lanes, buf[2], stream);
-    if (st != CDFTB_OK) return st;
-    const int tz = choose_tz(nzp);
-    FilterMaps geo_maps{};
-    if ((st = prepare_geometry<LaneF2>(op, batch, w + 3 * lanes * lane_bytes, tz, false, &geo_maps, stream)) !=
-        CDFTB_OK)
-        return st;
-    FilterMaps maps[3];
-    for (int b = 0; b < 3; ++b)
-        if ((st = encode_wide_lane_maps(buf[b], nzp, ny, nx, lanes, tz, &maps[b].phi, &maps[b].prev)) != CDFTB_OK)
-            return st;
-    FilterArgs a = base_args(op, batch);
-    a.lanes_per_group = 0;
-    a.coef = coefficients;
-    a.degree = degree;
-    int y = 2, prev = -1;
-    for (int k = 1; k <= degree; ++k) {
-        const int dst = (k == 1) ? 0 : (k == 2 ? 1 : prev);
-        a.has_prev = prev >= 0;
-        a.step = k - 1;
-        a.final_out = k == degree;
-        a.out = a.final_out ? out : buf[dst];
-        a.out_dtype = out_dtype;
-        FilterMaps m = geo_maps;
-        m.phi = maps[y].phi;
-        m.prev = maps[prev >= 0 ? prev : y].prev;
-        if ((st = launch_wide_any_tz(tz, m, a, lanes, stream)) != CDFTB_OK) return st;
-        prev = y;
-        y = dst;
-    }
-    return CDFTB_OK;
+    return total;
 }
 
 }  // namespace
 
 int64_t slab_filter_work_bytes(const cdftb_operator* op, int64_t batch) {
     const int64_t sb = op->dtype == CDFTB_F32 ? 4 : 8;
-    const int64_t points = int64_t(op->nx) * op->ny * padded_z(op->nz);
-    int64_t lane_total = lanes_of(op, batch) * points * 8;
-    if (op->dtype == CDFTB_F32 && !op->per_system_geometry)  // room for the wide lanes too
-        lane_total = std::max<int64_t>(lane_total, wide_lanes(batch) * points * 16);
-    return 3 * lane_total + geo_pack(op, batch).total() * sb;
+    return 3 * lane_bytes_total(op, batch) + geo_pack(op, batch).total() * sb;
 }
 
 bool slab_filter_applies(const cdftb_operator* op) {
@@ -1598,13 +1650,16 @@ bool slab_filter_applies(const cdftb_operator* op) {
 
 int64_t slab_apply_work_bytes(const cdftb_operator* op, int64_t batch) {
     const int64_t sb = op->dtype == CDFTB_F32 ? 4 : 8;
-    return lanes_of(op, batch) * int64_t(op->nx) * op->ny * padded_z(op->nz) * 8 + geo_pack(op, batch).total() * sb;
+    return lane_bytes_total(op, batch) + geo_pack(op, batch).total() * sb;
 }
 
 int slab_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
                           void* work, int64_t batch, const double* coefficients, int degree, cudaStream_t stream) {
-    if (wide_applies(op, batch))
-        return slab_filter_wide(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
+    if (wide_applies(op, batch)) {
+        if (op->dtype == CDFTB_F32)
+            return slab_filter<WideF4>(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
+        return slab_filter<WideD2>(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
+    }
     if (op->dtype == CDFTB_F32)
         return slab_filter<LaneF2>(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
     return slab_filter<LaneD>(op, block, in_dtype, out, out_dtype, work, batch, coefficients, degree, stream);
@@ -1704,6 +1759,11 @@ extern "C" int cdftb_cusp_apply(const cdftb_operator* op, const void* phi, int i
         return cdftb::generic_cusp_apply(op, phi, in_dtype, out, out_dtype, batch, kinetic_only, stream);
     }
     cudaStream_t s = cdftb::as_stream(stream);
+    if (cdftb::wide_applies(op, batch)) {
+        if (op->dtype == CDFTB_F32)
+            return cdftb::slab_apply<cdftb::WideF4>(op, phi, in_dtype, out, out_dtype, work, batch, kinetic_only, s);
+        return cdftb::slab_apply<cdftb::WideD2>(op, phi, in_dtype, out, out_dtype, work, batch, kinetic_only, s);
+    }
     if (op->dtype == CDFTB_F32)
         return cdftb::slab_apply<cdftb::LaneF2>(op, phi, in_dtype, out, out_dtype, work, batch, kinetic_only, s);
     return cdftb::slab_apply<cdftb::LaneD>(op, phi, in_dtype, out, out_dtype, work, batch, kinetic_only, s);

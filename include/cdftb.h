@@ -31,6 +31,9 @@ enum cdftb_status {
 
 enum cdftb_dtype { CDFTB_F64 = 0, CDFTB_F32 = 1 };
 
+/* Added to a dtype in the tuned-tile query (cdftb_filter_tuned_tile) for the wide-lane kernels. */
+enum { CDFTB_WIDE_LANES = 16 };
+
 /* Library version (major*10000 + minor*100 + patch) and the status text. */
 int cdftb_version(void);
 const char* cdftb_status_string(int status);
@@ -109,15 +112,17 @@ int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_d
  * default in the C library), heuristics choose the tiling. cdftb_filter_tuned_tile reports the
  * table's entry for a key (tile_z 32 or 36, x_chunk in planes; both 0 when the key is not tuned);
  * dtype is CDFTB_F32 or CDFTB_F64 and lanes is the launch's lane count (cdftb_operator orbitals in
- * pairs for float32, one each for float64). */
+ * pairs for float32, one each for float64); for the wide-lane kernels (cdftb_filter_wide) dtype is
+ * CDFTB_F32 + CDFTB_WIDE_LANES or CDFTB_F64 + CDFTB_WIDE_LANES and lanes counts four float32 or two
+ * float64 orbitals each. */
 int cdftb_filter_autotune(int enable);
 int cdftb_filter_tuned_tile(int nx, int ny, int nz, int dtype, int64_t lanes, int* tile_z, int* x_chunk);
 
-/* No reference counterpart: wide float32 lanes for cdftb_chebyshev_filter. Enabled (the default),
- * a float32 filter with one shared geometry (no per-system geometry) and at least 16 lanes of four
- * orbitals runs a kernel that holds four orbitals per 16-byte lane point instead of two: the same
- * operator and recurrence, its sums in another order (float32 rounding differs from the two-orbital
- * kernel). cdftb_chebyshev_filter_work_bytes covers both layouts. */
+/* No reference counterpart: wide lanes for cdftb_chebyshev_filter and cdftb_cusp_apply. Enabled
+ * (the default), an order-8 call with one shared geometry (no per-system geometry) and at least 16
+ * wide lanes runs a kernel that holds 16 bytes per lane point -- four float32 or two float64
+ * orbitals -- instead of 8: the same operator and recurrence, its sums in another order (results
+ * differ from the 8-byte-lane kernel by rounding). The work-size queries cover both layouts. */
 int cdftb_filter_wide(int enable);
 
 /* No reference counterpart: the error flags the library's kernels set on the device (bit 0: a

@@ -183,11 +183,12 @@ def test_autotuned_apply_is_bit_identical(pkg, cuda):
     assert _device_status(pkg) == (0, 0)
 
 
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
 @pytest.mark.parametrize("shape", [(14, 13, 29), (21, 9, 65)])
-def test_wide_lanes_many_systems(pkg, cuda, shape):
-    """Four float32 orbitals per lane: 23 systems x 3 orbitals (lanes that mix systems, an empty last
-    slot), both z tiles (nz 29 -> 32 columns, nz 65 -> 36), against the oracle and against the
-    two-orbital lanes."""
+def test_wide_lanes_many_systems(pkg, cuda, shape, dtype):
+    """16-byte lane points (four float32 or two float64 orbitals): 23 systems x 3 orbitals (lanes
+    that mix systems, an empty last slot), both z tiles (nz 29 -> 32 columns, nz 65 -> 36), against
+    the oracle and against the 8-byte lanes."""
     from importlib import import_module
 
     eigen = import_module(pkg.__name__ + ".eigen")
@@ -201,8 +202,9 @@ def test_wide_lanes_many_systems(pkg, cuda, shape):
     degree = 5
     table = torch.tensor([eigen.chebyshev_coefficients(degree, *b) for b in bounds], dtype=torch.float64,
                          device=cuda)
-    _, ham = _pair(pkg, cuda, shape, 0.25, faces, inv, q, pots[0], dtype=torch.float32)
+    _, ham = _pair(pkg, cuda, shape, 0.25, faces, inv, q, pots[0], dtype=dtype)
     lib = pkg._lib.library()
+    tol = 2e-5 if dtype == torch.float32 else 1e-12
 
     def run():
         return eigen.filter_with_table(ham, _t(blocks, cuda), table, degree, orbitals_per_group=per,
@@ -218,7 +220,33 @@ def test_wide_lanes_many_systems(pkg, cuda, shape):
     for s in (0, 7, 22):
         ham_o, _ = _pair(pkg, cuda, shape, 0.25, faces, inv, q, pots[s])
         want = oeigen.chebyshev_filter(ham_o, blocks[s], degree, *bounds[s])
-        np.testing.assert_allclose(wide[s], want, rtol=0, atol=2e-5 * np.abs(want).max())
-    np.testing.assert_allclose(wide, narrow, rtol=0, atol=2e-5 * np.abs(narrow).max())
+        np.testing.assert_allclose(wide[s], want, rtol=0, atol=tol * np.abs(want).max())
+    np.testing.assert_allclose(wide, narrow, rtol=0, atol=tol * np.abs(narrow).max())
     assert not np.array_equal(wide, narrow)  # the wide kernel ran (its sums run in another order)
+    assert _device_status(pkg) == (0, 0)
+
+
+@pytest.mark.parametrize("kinetic", [False, True])
+def test_wide_lanes_apply(pkg, cuda, kinetic):
+    """The one-launch apply on 40 float64 orbitals (20 wide lanes) against the oracle and against the
+    8-byte lanes, with and without the potential."""
+    shape = (17, 15, 37)
+    n = int(np.prod(shape))
+    faces, inv, q = _random_operator(shape, seed=41)
+    pot = np.random.default_rng(42).standard_normal(n)
+    ham_o, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot)
+    block = np.random.default_rng(43).standard_normal((40, n))
+    lib = pkg._lib.library()
+    run = ham.kinetic_apply if kinetic else ham.apply
+    try:
+        lib.cdftb_filter_wide(1)
+        wide = run(_t(block, cuda)).cpu().numpy()
+        lib.cdftb_filter_wide(0)
+        narrow = run(_t(block, cuda)).cpu().numpy()
+    finally:
+        lib.cdftb_filter_wide(1)
+    want = np.stack([ham_o.kinetic_apply(b) if kinetic else ham_o.apply(b) for b in block[:3]])
+    np.testing.assert_allclose(wide[:3], want, rtol=0, atol=1e-12 * np.abs(want).max())
+    np.testing.assert_allclose(wide, narrow, rtol=0, atol=1e-13 * np.abs(narrow).max())
+    assert not np.array_equal(wide, narrow)
     assert _device_status(pkg) == (0, 0)

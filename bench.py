@@ -122,16 +122,17 @@ def _peaks():
 
 
 def _profile_traffic(kernel_tag: str):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if present."""
-    path = ROOT / "profiles" / "slab_filter_he65.txt"
-    if not path.exists():
-        return None
-    for line in path.read_text().splitlines():
-        if line.startswith(f"traffic_bytes_per_launch[{kernel_tag}]"):
-            try:
-                return float(line.rsplit("=", 1)[1].strip())
-            except ValueError:
-                return None
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summaries, if present."""
+    for name in ("slab_filter_wide_he65.txt", "slab_filter_he65.txt"):
+        path = ROOT / "profiles" / name
+        if not path.exists():
+            continue
+        for line in path.read_text().splitlines():
+            if line.startswith(f"traffic_bytes_per_launch[{kernel_tag}]"):
+                try:
+                    return float(line.rsplit("=", 1)[1].strip())
+                except ValueError:
+                    return None
     return None
 
 
@@ -217,7 +218,7 @@ def run_kernel_only(args) -> None:
                                                          reps=args.steps)
     peak, kind = _peaks()
     achieved = algorithmic / per_launch_s / 1e9
-    print(json.dumps({"kernel": "slab_filter_kernel (one Chebyshev step)", "grid": grid.shape, "systems": batch,
+    print(json.dumps({"kernel": "slab filter (one Chebyshev step)", "grid": grid.shape, "systems": batch,
                       "orbitals": args.orbitals, "form": args.form, "us_per_launch": per_launch_s * 1e6,
                       "algorithmic_bytes": algorithmic, "achieved_gbs": achieved, "peak_gbs": peak,
                       "peak_kind": kind, "frac": achieved / peak}), flush=True)
@@ -586,7 +587,8 @@ def main() -> None:
         per_launch_s, algorithmic = batched_filter_roofline(pkg, dev, grid, bham, 5, precision)
     achieved = algorithmic / per_launch_s / 1e9
     peak, peak_kind = _peaks()
-    tag = "f32" if precision == torch.float32 else "f64"
+    # one shared geometry: the wide-lane kernel (four float32 or two float64 orbitals per lane point)
+    tag = "f32x4" if precision == torch.float32 else "f64x2"
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -601,7 +603,7 @@ def main() -> None:
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": _profile_traffic(f"{tag},batch={batch}"),
-                     "kernel": f"slab_filter_kernel<{tag}> (one Chebyshev step, {batch} systems x 5 orbitals)",
+                     "kernel": f"slab_filter_wide_kernel<{tag}> (one Chebyshev step, {batch} systems x 5 orbitals)",
                      "algorithmic_bytes_per_launch": algorithmic, "us_per_launch": per_launch_s * 1e6,
                      "peak_kind": peak_kind},
         "clocks": clocks,

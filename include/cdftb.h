@@ -119,10 +119,11 @@ int cdftb_filter_autotune(int enable);
 int cdftb_filter_tuned_tile(int nx, int ny, int nz, int dtype, int64_t lanes, int* tile_z, int* x_chunk);
 
 /* No reference counterpart: wide lanes for cdftb_chebyshev_filter and cdftb_cusp_apply. Enabled
- * (the default), an order-8 call with one shared geometry (no per-system geometry) and at least 16
- * wide lanes runs a kernel that holds 16 bytes per lane point -- four float32 or two float64
- * orbitals -- instead of 8: the same operator and recurrence, its sums in another order (results
- * differ from the 8-byte-lane kernel by rounding). The work-size queries cover both layouts. */
+ * (the default), every order-8 call with one shared geometry (no per-system geometry) runs a
+ * kernel that holds 16 bytes per lane point -- four float32 or two float64 orbitals -- instead of
+ * 8: the same operator and recurrence, its sums in another order (results differ from the
+ * 8-byte-lane kernel by rounding). Calls with per-system geometry, or all calls when disabled, use
+ * the 8-byte lanes. The work-size queries cover both layouts. */
 int cdftb_filter_wide(int enable);
 
 /* No reference counterpart: the error flags the library's kernels set on the device (bit 0: a

@@ -56,9 +56,18 @@ def _device_status(pkg):
 SHAPES = [(9, 11, 13), (12, 17, 24), (5, 9, 40), (33, 20, 70), (21, 8, 65)]
 
 
+@pytest.fixture(params=[1, 0], ids=["wide", "narrow"])
+def lanes(request, pkg):
+    """The lane layout: 16-byte lane points (the default) or 8-byte ones."""
+    lib = pkg._lib.library()
+    lib.cdftb_filter_wide(request.param)
+    yield request.param
+    lib.cdftb_filter_wide(1)
+
+
 @pytest.mark.parametrize("shape", SHAPES)
 @pytest.mark.parametrize("batch", [1, 3, 4])
-def test_slab_filter_float64(pkg, cuda, shape, batch):
+def test_slab_filter_float64(pkg, cuda, shape, batch, lanes):
     faces, inv, q = _random_operator(shape, seed=sum(shape) + batch)
     pot = np.random.default_rng(7).standard_normal(int(np.prod(shape)))
     ham_o, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot)
@@ -72,7 +81,7 @@ def test_slab_filter_float64(pkg, cuda, shape, batch):
 
 @pytest.mark.parametrize("shape", SHAPES)
 @pytest.mark.parametrize("batch", [1, 3, 4])
-def test_slab_filter_float32(pkg, cuda, shape, batch):
+def test_slab_filter_float32(pkg, cuda, shape, batch, lanes):
     faces, inv, q = _random_operator(shape, seed=sum(shape) + batch)
     pot = np.random.default_rng(7).standard_normal(int(np.prod(shape)))
     ham_o, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot, dtype=torch.float32)
@@ -85,7 +94,7 @@ def test_slab_filter_float32(pkg, cuda, shape, batch):
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
-def test_slab_filter_many_systems(pkg, cuda, dtype):
+def test_slab_filter_many_systems(pkg, cuda, dtype, lanes):
     """Three systems x three orbitals: per-system potentials and coefficient tables in one call."""
     from importlib import import_module
 
@@ -142,8 +151,9 @@ def test_autotuned_tiling_is_bit_identical(pkg, cuda, dtype):
     _, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot, dtype=dtype)
     block = _t(np.random.default_rng(13).standard_normal((5, int(np.prod(shape)))), cuda)
     lib = pkg._lib.library()
-    code = 1 if dtype == torch.float32 else 0  # CDFTB_F32 / CDFTB_F64
-    lanes = 3 if dtype == torch.float32 else 5
+    # CDFTB_F32 / CDFTB_F64 plus CDFTB_WIDE_LANES: 5 orbitals in 2 float32 or 3 float64 wide lanes
+    code = (1 if dtype == torch.float32 else 0) + 16
+    lanes = 2 if dtype == torch.float32 else 3
     tz, xc = ctypes.c_int(-1), ctypes.c_int(-1)
     try:
         lib.cdftb_filter_autotune(0)
@@ -175,7 +185,7 @@ def test_autotuned_apply_is_bit_identical(pkg, cuda):
         heuristic = ham.apply(block)
         lib.cdftb_filter_autotune(1)
         tuned = ham.apply(block)
-        assert lib.cdftb_filter_tuned_tile(*shape, 0, 3, ctypes.byref(tz), ctypes.byref(xc)) == 0
+        assert lib.cdftb_filter_tuned_tile(*shape, 0 + 16, 2, ctypes.byref(tz), ctypes.byref(xc)) == 0
         assert tz.value in (32, 36) and 1 <= xc.value <= shape[0]
     finally:
         lib.cdftb_filter_autotune(1)

@@ -632,8 +632,10 @@ struct WideShape {
     static constexpr int PW = NG * PWG;
     static constexpr int WARPS = MW + PW + 1;
     static constexpr int T = WARPS * 32;
-    static constexpr int BW = TZ + 18;
-    static constexpr int ZROW = TZ + 2;
+    // odd row pitches (in 16-byte points): the 8 rows of a warp's z items then fall on 8 different
+    // groups of 4 banks (an even pitch such as TZ + 18 puts them on 4)
+    static constexpr int BW = TZ + 19;  // phi box: z0-8 .. z0+TZ+10
+    static constexpr int ZROW = TZ + 3;
     static constexpr unsigned TX_PHI = NROW * BW * EB;
     static constexpr unsigned TX_PREV = TY * TZ * EB;
     static constexpr unsigned TX_W0 = TY * TZ * SB;
@@ -657,6 +659,8 @@ struct WideShape {
     static constexpr size_t BYTES = O_BAR + (2 * RW + 2 * RY) * 8;
     static_assert(TY * TZ % 32 == 0, "march warps cover the tile");
     static_assert(TZ >= 8 && TZ % 2 == 0, "z segments of 8 inside the tile");
+    static_assert(BW % 2 == 1 && ZROW % 2 == 1, "odd row pitches");
+    static_assert((TZ - 8) + 22 <= BW - 1, "the last z segment's nodes lie inside the phi box");
     static_assert(BYTES <= 232448, "fits the opt-in shared memory of one CTA");
 };
 
@@ -1352,7 +1356,7 @@ int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_
 int encode_wide_lane_maps(void* buf, int nzp, int ny, int nx, int64_t lanes, int tz, CUtensorMap* phi,
                           CUtensorMap* prev) {
     const int64_t lane_dims[4] = {2 * int64_t(nzp), ny, nx, lanes};
-    const unsigned phi_box[4] = {unsigned(2 * (tz + 18)), unsigned(NROW), 1, 1};
+    const unsigned phi_box[4] = {unsigned(2 * (tz + 19)), unsigned(NROW), 1, 1};  // WideShape::BW points
     const unsigned prev_box[4] = {unsigned(2 * tz), unsigned(TY), 1, 1};
     int st = encode_map(phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, phi_box);
     if (st == CDFTB_OK) st = encode_map(prev, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, prev_box);

@@ -294,16 +294,17 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
     dev = h.potentials.device
     extra = max(config.n_extra_states, int(config.extra_states_fraction * n_states))
     m = min(n_states + extra, n)
-    blocks = []
+    # the start block, written once in place: the carried vectors, then each system's fresh draws
+    block = torch.empty((b, m, n), dtype=torch.float64, device=dev)
     for s in range(b):
         if initial is None:
-            blocks.append(streams[s].randn((m, n)))
+            block[s] = streams[s].randn((m, n))
         else:
-            blk = initial[s].to(torch.float64).reshape(-1, n)
-            if blk.shape[0] < m:
-                blk = torch.cat([blk, streams[s].randn((m - blk.shape[0], n))], dim=0)
-            blocks.append(blk)
-    block = torch.stack(blocks)
+            blk = initial[s].reshape(-1, n)
+            k = min(blk.shape[0], m)
+            block[s, :k] = blk[:k]
+            if k < m:
+                block[s, k:] = streams[s].randn((m - k, n))
     states = [_EigenState(float_filter=h32 is not None and (float_mask is None or bool(float_mask[s])))
               for s in range(b)]
     need = [s for s in range(b) if bounds[s] is None]
@@ -326,9 +327,10 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
             st.source = "reused"
             st.shift = shift
     previous = evals.clone()
-    out_evals = evals.clone()
-    out_vectors = vectors.clone()
-    out_res = residual.clone()
+    # results per system, kept for the n_states wanted rows only (the others are never returned)
+    out_evals = evals[:, :n_states].clone()
+    out_vectors = vectors[:, :n_states].clone()
+    out_res = residual[:, :n_states].clone()
     active = list(range(b))
     for iteration in range(1, max_iterations + 1):
         # per-system filter intervals (and a fresh Lanczos where a carried bound is rejected)
@@ -388,9 +390,9 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
         if full:
             vectors, evals, residual = vec, ev, res
         else:
-            vectors = vectors.index_copy(0, sel, vec)
-            evals = evals.index_copy(0, sel, ev)
-            residual = residual.index_copy(0, sel, res)
+            vectors.index_copy_(0, sel, vec)
+            evals.index_copy_(0, sel, ev)
+            residual.index_copy_(0, sel, res)
         previous = evals.clone()
         still = []
         done = []
@@ -416,20 +418,26 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
                     done.append(s)
                     still.remove(s)
         if done:
-            idx = torch.tensor(done, dtype=torch.long, device=dev)
-            out_evals = out_evals.index_copy(0, idx, evals.index_select(0, idx))
-            out_vectors = out_vectors.index_copy(0, idx, vectors.index_select(0, idx))
-            out_res = out_res.index_copy(0, idx, residual.index_select(0, idx))
+            _keep(out_evals, out_vectors, out_res, done, evals, vectors, residual, n_states, dev)
         active = still
         if not active:
             break
     if active:
-        idx = torch.tensor(active, dtype=torch.long, device=dev)
-        out_evals = out_evals.index_copy(0, idx, evals.index_select(0, idx))
-        out_vectors = out_vectors.index_copy(0, idx, vectors.index_select(0, idx))
-        out_res = out_res.index_copy(0, idx, residual.index_select(0, idx))
-    return (out_evals[:, :n_states].contiguous(), out_vectors[:, :n_states].contiguous(),
-            out_res[:, :n_states].contiguous(), states)
+        _keep(out_evals, out_vectors, out_res, active, evals, vectors, residual, n_states, dev)
+    return out_evals, out_vectors, out_res, states
+
+
+def _keep(out_evals, out_vectors, out_res, systems, evals, vectors, residual, n_states, dev):
+    """Copy the wanted rows of these systems' current results into the outputs, in place."""
+    if len(systems) == out_vectors.shape[0]:
+        out_evals.copy_(evals[:, :n_states])
+        out_vectors.copy_(vectors[:, :n_states])
+        out_res.copy_(residual[:, :n_states])
+        return
+    idx = torch.tensor(systems, dtype=torch.long, device=dev)
+    out_evals.index_copy_(0, idx, evals[:, :n_states].index_select(0, idx))
+    out_vectors.index_copy_(0, idx, vectors[:, :n_states].index_select(0, idx))
+    out_res.index_copy_(0, idx, residual[:, :n_states].index_select(0, idx))
 
 
 @dataclass
@@ -734,9 +742,10 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
             alpha = torch.tensor([systems[s].mixer.alpha for s in active], dtype=torch.float64, device=dev)
             a2 = alpha[:, None]
             n_next = nin + a2 * (n_out - nin)
-            lin_next = (p_in.v_smooth + a2 * (p_out.v_smooth - p_in.v_smooth),
-                        p_in.node + alpha[None, :, None] * (p_out.node - p_in.node),
-                        p_in.lifted_h + a2 * (p_out.lifted_h - p_in.lifted_h))
+            # the carried linear parts need no element-for-element match: one lerp pass each
+            lin_next = (torch.lerp(p_in.v_smooth, p_out.v_smooth, a2),
+                        torch.lerp(p_in.node, p_out.node, alpha[None, :, None]),
+                        torch.lerp(p_in.lifted_h, p_out.lifted_h, a2))
         else:
             for j, s in enumerate(active):
                 n_next[j] = systems[s].mixer.mix(nin[j:j + 1], n_out[j:j + 1], iteration)[0]

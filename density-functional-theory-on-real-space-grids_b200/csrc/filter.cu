@@ -691,18 +691,11 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
     const bool has_prev = a.has_prev != 0;
 
     // the lane's orbitals (an empty slot borrows the first orbital's group for its lookups)
-    int64_t orb[ORB];
-    int grp[ORB];
-#pragma unroll
-    for (int h = 0; h < ORB; ++h) {
-        const int64_t o = int64_t(ORB) * lane + h;
-        orb[h] = o < a.batch ? o : -1;
-    }
-#pragma unroll
-    for (int h = 0; h < ORB; ++h) {
-        const int64_t o = orb[h] >= 0 ? orb[h] : orb[0];
-        grp[h] = a.shared_potential ? 0 : static_cast<int>(o / a.orb_per_group);
-    }
+    // the lane's orbitals: ORB lane + h, present when below the batch (an empty slot borrows the
+    // first orbital's group for its lookups); formed where they are used, so that no role keeps them
+    // in registers through its loop
+    const int64_t orb0 = int64_t(ORB) * lane;
+    auto orbital_of = [&](int h) -> int64_t { return orb0 + h < a.batch ? orb0 + h : orb0; };
 
     if (t == 0) {
         for (int s = 0; s < RW; ++s) {
@@ -727,6 +720,10 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
         if ((t & 31) != 0) return;
         const unsigned tx = SH::TX_PHI + (has_prev ? SH::TX_PREV : 0) + SH::TX_W0 + SH::TX_W1 + SH::TX_W2 +
                             SH::TX_INV + ORB * SH::TX_POT;
+        int grp[ORB];
+#pragma unroll
+        for (int h = 0; h < ORB; ++h)
+            grp[h] = a.shared_potential ? 0 : static_cast<int>(orbital_of(h) / a.orb_per_group);
         int issued = 0;
         int s = 0, ph = 1;
         for (int n = 0; n < npl; ++n) {
@@ -857,7 +854,7 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
         S c3[3][ORB];
 #pragma unroll
         for (int h = 0; h < ORB; ++h) {
-            const int64_t o = orb[h] >= 0 ? orb[h] : orb[0];
+            const int64_t o = orbital_of(h);
             const double* r = a.coef + ((o / a.orb_per_group) * a.degree + a.step) * 3;
 #pragma unroll
             for (int k = 0; k < 3; ++k) c3[k][h] = static_cast<S>(r[k]);
@@ -939,7 +936,8 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
                         W::parts(res, rv);
 #pragma unroll
                         for (int h = 0; h < ORB; ++h)
-                            if (orb[h] >= 0) store_as<S>(a.out, a.out_dtype, orb[h] * (plane_n * nx) + pt, rv[h]);
+                            if (orb0 + h < a.batch)
+                                store_as<S>(a.out, a.out_dtype, (orb0 + h) * (plane_n * nx) + pt, rv[h]);
                     }
                 } else {
                     E* out = static_cast<E*>(a.out);

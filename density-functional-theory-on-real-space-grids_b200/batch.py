@@ -553,8 +553,25 @@ class BatchedKohnShamStep:
         rho_out = (self.occ[None, :, None] * vectors.pow(2)).sum(dim=1)  # (B, N)
         return rho_out * self.f2[None, :], rho_out
 
+    def output_density_residual(self, vectors: torch.Tensor, n_in: torch.Tensor):
+        """:meth:`output_density` and the integrand of the density residual norm in one pass.
+
+        Returns ``(n_out, rho_out, terms)`` with ``terms = mass |n_out - n_in| / f^2`` per point, whose
+        row sums are the residual norms (``src/cdft/scf/loop.py:298-301, 375-376``).
+        """
+        v = vectors.to(torch.float64).contiguous()
+        b, k, n = v.shape
+        x = n_in.to(torch.float64).contiguous()
+        f = dict(dtype=torch.float64, device=v.device)
+        rho_out, n_out, terms = torch.empty((b, n), **f), torch.empty((b, n), **f), torch.empty((b, n), **f)
+        occ = self.occ.to(torch.float64).contiguous()
+        call("cdftb_density_residual_f64", ptr(v), ptr(occ), k, n, b, ptr(self.f2),
+             ptr(self.quadrature.mass_weights.contiguous()), ptr(x), ptr(rho_out), ptr(n_out), ptr(terms),
+             stream_handle(v.device))
+        return n_out, rho_out, terms
+
     def external_parts(self, rho: torch.Tensor, rho_node: torch.Tensor | None = None):
-        """``((1/2)Q[f^2 grad rho . grad u], Q[f^2 rho W])`` per system (hamiltonian.py:557-574).
+        """``((1/2)Q[f^2 grad rho . grad u], Q[f^2 rho W])`` per system (hamiltonian.py:360-378).
 
         ``rho_node`` (B, M): ``L rho`` when the caller already holds it (the output potentials
         interpolate the same density), so that only the gradient is interpolated here.
@@ -570,10 +587,15 @@ class BatchedKohnShamStep:
         else:
             grad_node = q.interpolate(grad.contiguous())  # (B, 3, M)
         cross_node = q.f2[None] * (grad_node * q.grad_u[None]).sum(dim=1)
-        cross_grid = factor.weight[None] * (grad * factor.grad_u[None]).sum(dim=1)
-        cross = 0.5 * (row_sums(q.weights[None] * cross_node) + row_sums(q.far_weights[None] * cross_grid))
-        pot = (row_sums(q.weights[None] * (q.f2[None] * rho_node * q.transformed_potential[None]))
-               + row_sums(q.far_weights[None] * (factor.weight[None] * rho * factor.transformed_potential[None])))
+        # the grid halves of both integrals in one pass: (far_w weight grad rho . grad u, far_w weight rho W)
+        grid_terms = torch.empty((b, 2, n), dtype=torch.float64, device=rho.device)
+        call("cdftb_external_grid_terms_f64", ptr(grad.contiguous()), ptr(rho.contiguous()),
+             ptr(factor.weight.contiguous()), ptr(factor.grad_u.contiguous()),
+             ptr(factor.transformed_potential.contiguous()), ptr(q.far_weights.contiguous()), n, b, ptr(grid_terms),
+             stream_handle(rho.device))
+        grid_sums = row_sums(grid_terms)  # (B, 2)
+        cross = 0.5 * (row_sums(q.weights[None] * cross_node) + grid_sums[:, 0])
+        pot = row_sums(q.weights[None] * (q.f2[None] * rho_node * q.transformed_potential[None])) + grid_sums[:, 1]
         return cross, pot
 
     def energy_terms(self, evals, vectors, rho_out, p_in: BatchedPotentials, p_out: BatchedPotentials):
@@ -725,11 +747,10 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
                     "eigen_bounds_source": es.source, "eigen_bounds_shift": es.shift}
             st.policy.observe(st.policy._pending_reason, info)
             st.rung_changed = False
-        n_out, rho_out = step.output_density(vectors)
+        n_out, rho_out, res_terms = step.output_density_residual(vectors, nin)
         p_out = step.potentials(n_out)
         terms = step.energy_terms(evals, vectors, rho_out, p_in, p_out)
-        residual = n_out - nin
-        res_norm = row_sums(mass[None] * (residual.abs() / f2[None]))
+        res_norm = row_sums(res_terms)
         keys = list(terms)
         host = torch.stack([*terms.values(), res_norm]).cpu().numpy()  # (len(keys)+1, S)
         # mixing (per system: linear in one batched expression when all are linear)
@@ -779,7 +800,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
                 st.fallback_events.append(f"iteration {iteration}: stepping down to rung {st.rung}")
                 st.worsened = 0
                 st.rung_changed = True
-                n_next[j] = nin[j] + 0.5 * mixing.alpha * residual[j]
+                n_next[j] = nin[j] + 0.5 * mixing.alpha * (n_out[j] - nin[j])
                 if lin_next is not None:
                     a = 0.5 * mixing.alpha
                     lin_next[0][j] = p_in.v_smooth[j] + a * (p_out.v_smooth[j] - p_in.v_smooth[j])

@@ -260,6 +260,52 @@ __global__ void fd_derivative_kernel(const double* __restrict__ in, double* __re
     }
 }
 
+// The output density and the density residual of one SCF iteration, per system g and point i
+// (src/cdft/scf/step.py:366-370 output_density; src/cdft/scf/loop.py:298-301 and 375-376, the
+// residual norm):
+//   rho_out = sum_k occ_k v_k^2,  n_out = rho_out f^2,  res = mass |n_out - n_in| / f^2.
+// Products and sums are rounded one at a time (no contraction), in the order of those lines.
+__global__ void density_residual_kernel(const double* __restrict__ vectors, const double* __restrict__ occ, int k,
+                                        int64_t np, int batch, const double* __restrict__ f2,
+                                        const double* __restrict__ mass, const double* __restrict__ n_in,
+                                        double* __restrict__ rho_out, double* __restrict__ n_out,
+                                        double* __restrict__ res) {
+    const bool narrow = np * batch <= 0xffffffffll;
+    GRID_STRIDE(idx, np * batch) {
+        int64_t g, i;
+        split_index(idx, np, narrow, g, i);
+        const double* v = vectors + g * k * np + i;
+        double r = __dmul_rn(occ[0], __dmul_rn(v[0], v[0]));
+        for (int j = 1; j < k; ++j) r = __dadd_rn(r, __dmul_rn(occ[j], __dmul_rn(v[j * np], v[j * np])));
+        const double f = f2[i];
+        const double n = __dmul_rn(r, f);
+        rho_out[idx] = r;
+        n_out[idx] = n;
+        res[idx] = __dmul_rn(mass[i], __ddiv_rn(fabs(__dsub_rn(n, n_in[idx])), f));
+    }
+}
+
+// Grid half of the external energy parts (hamiltonian.py:360-378), per system g and point i:
+//   out[g][0][i] = far_w (weight ((g0 u0 + g1 u1) + g2 u2)),  out[g][1][i] = far_w ((weight rho) W),
+// with grad (batch, 3, np) the density gradient, u the cusp exponent's gradient (3, np) and W the
+// transformed potential; rounded one operation at a time in that order.
+__global__ void external_grid_kernel(const double* __restrict__ grad, const double* __restrict__ rho,
+                                     const double* __restrict__ weight, const double* __restrict__ grad_u,
+                                     const double* __restrict__ tpot, const double* __restrict__ far_w, int64_t np,
+                                     int batch, double* __restrict__ out) {
+    const bool narrow = np * batch <= 0xffffffffll;
+    GRID_STRIDE(idx, np * batch) {
+        int64_t g, i;
+        split_index(idx, np, narrow, g, i);
+        const double* gr = grad + g * 3 * np + i;
+        const double dot = __dadd_rn(__dadd_rn(__dmul_rn(gr[0], grad_u[i]), __dmul_rn(gr[np], grad_u[np + i])),
+                                     __dmul_rn(gr[2 * np], grad_u[2 * np + i]));
+        const double w = weight[i], fw = far_w[i];
+        out[g * 2 * np + i] = __dmul_rn(fw, __dmul_rn(w, dot));
+        out[g * 2 * np + np + i] = __dmul_rn(fw, __dmul_rn(__dmul_rn(w, rho[idx]), tpot[i]));
+    }
+}
+
 }  // namespace
 
 }  // namespace cdftb
@@ -336,6 +382,30 @@ extern "C" int64_t cdftb_row_sums_scratch_bytes(int rows, int64_t len) {
     int chunks;
     row_shape(rows, len, chunk, chunks);
     return static_cast<int64_t>(rows) * chunks * 8;
+}
+
+extern "C" int cdftb_density_residual_f64(const double* vectors, const double* occupations, int k, int64_t n_points,
+                                          int batch, const double* f2, const double* mass_weights,
+                                          const double* n_in, double* rho_out, double* n_out, double* residual_terms,
+                                          cdftb_stream_t stream) {
+    if (!vectors || !occupations || !f2 || !mass_weights || !n_in || !rho_out || !n_out || !residual_terms || k < 1 ||
+        n_points <= 0 || batch < 1)
+        return CDFTB_ERR_ARGUMENT;
+    density_residual_kernel<<<blocks_for(n_points * batch, 256), 256, 0, as_stream(stream)>>>(
+        vectors, occupations, k, n_points, batch, f2, mass_weights, n_in, rho_out, n_out, residual_terms);
+    return check_launch();
+}
+
+extern "C" int cdftb_external_grid_terms_f64(const double* grad, const double* rho, const double* weight,
+                                             const double* grad_u, const double* transformed_potential,
+                                             const double* far_weights, int64_t n_points, int batch, double* out,
+                                             cdftb_stream_t stream) {
+    if (!grad || !rho || !weight || !grad_u || !transformed_potential || !far_weights || !out || n_points <= 0 ||
+        batch < 1)
+        return CDFTB_ERR_ARGUMENT;
+    external_grid_kernel<<<blocks_for(n_points * batch, 256), 256, 0, as_stream(stream)>>>(
+        grad, rho, weight, grad_u, transformed_potential, far_weights, n_points, batch, out);
+    return check_launch();
 }
 
 extern "C" int cdftb_row_sums_f64(const double* a, int rows, int64_t len, double* out, void* scratch,

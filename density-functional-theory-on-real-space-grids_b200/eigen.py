@@ -50,7 +50,7 @@ def chebyshev_filter(hamiltonian, block: torch.Tensor, degree: int, lower: float
     if upper <= lower:
         raise ValueError(f"filter interval is empty: lower={lower}, upper={upper}")
     rows = chebyshev_coefficients(degree, lower, upper, spectrum_min)
-    # pinned + non-blocking: a pageable copy would synchronise the stream (as chefsi.py:758-771 notes)
+    # pinned + non-blocking: a pageable copy would synchronise the stream (as chefsi.py:316-321 notes)
     table = torch.tensor(rows, dtype=torch.float64).pin_memory().to(block.device, non_blocking=True)
     return filter_with_table(hamiltonian, block, table, degree, orbitals_per_group=block.numel() // block.shape[-1],
                              precision=precision)

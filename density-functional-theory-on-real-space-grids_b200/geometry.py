@@ -425,7 +425,7 @@ class CuspQuadrature:
         return n, grad_n
 
     def external_energy_parts(self, rho: torch.Tensor, factor: CuspFactor):
-        """``((1/2) Q[f^2 grad rho . grad u], Q[f^2 rho W])`` (hamiltonian.py:557-574)."""
+        """``((1/2) Q[f^2 grad rho . grad u], Q[f^2 rho W])`` (hamiltonian.py:360-378)."""
         grad_rho = gradient(self.grid, rho)
         both = self.interpolate(torch.cat([rho.reshape(1, -1), grad_rho]))
         rho_node, grad_rho_node = both[0], both[1:]

@@ -65,7 +65,7 @@ def rowwise_inner(a: torch.Tensor, b: torch.Tensor, q: torch.Tensor | None) -> t
 
 
 class Measure:
-    """``<a,b> = sum_r q(r) a(r) b(r)`` (``src/cdft/eigen/measure.py:155``), q = the quadrature weight."""
+    """``<a,b> = sum_r q(r) a(r) b(r)`` (``src/cdft/eigen/measure.py:18-82``), q = the quadrature weight."""
 
     def __init__(self, grid: UniformGrid, quadrature: torch.Tensor) -> None:
         if quadrature.shape[-1] != grid.n_points:
@@ -230,7 +230,7 @@ class CuspFactoredHamiltonian:
         start = seeded_randn(self.grid.n_points, generator, device=self.grid.device)
         return lanczos_bounds(self, start, steps, safety)
 
-    # -- energies (hamiltonian.py:541-583) --
+    # -- energies (hamiltonian.py:331-390) --
     def kinetic_energy_tensor(self, phi: torch.Tensor, occupations: torch.Tensor) -> torch.Tensor:
         occ = occupations.to(torch.float64)
         kinetic_form = self.measure.inner(phi, self.kinetic_apply(phi))

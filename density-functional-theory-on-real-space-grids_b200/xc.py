@@ -71,7 +71,7 @@ class PBE(_Functional):
 
 
 def functional_by_name(name: str) -> _Functional:
-    """The native functionals (``src/cdft/xc/dispatch.py:231``); others raise ``KeyError``."""
+    """The native functionals (``src/cdft/xc/dispatch.py:26-62``); others raise ``KeyError``."""
     table = {"lda_vwn": LDA, "pbe": PBE}
     key = name.lower()
     if key not in table:

@@ -304,6 +304,19 @@ int cdftb_potentials_grid_lda_f64(const double* density, const double* rho, cons
                                   const double* v1s_grid, const double* coefficients, int n_atoms,
                                   const double* lifted, int64_t n_points, int batch, double* effective,
                                   double* v_hartree, double* terms, double* v_xc, cdftb_stream_t stream);
+/* One SCF iteration's output density and density residual (src/cdft/scf/step.py:366-370,
+ * src/cdft/scf/loop.py:298-301 and 375-376):
+ * rho_out = sum_k occ_k v_k^2 over the k orbitals (batch, k, n_points) of each system, n_out =
+ * rho_out f2, residual_terms = mass |n_out - n_in| / f2 (its row sums are the residual norms). */
+int cdftb_density_residual_f64(const double* vectors, const double* occupations, int k, int64_t n_points, int batch,
+                               const double* f2, const double* mass_weights, const double* n_in, double* rho_out,
+                               double* n_out, double* residual_terms, cdftb_stream_t stream);
+/* Grid half of the external energy parts (hamiltonian.py:360-378): out (batch, 2, n_points) =
+ * (far_w weight (grad rho . grad u), far_w weight rho W); their row sums enter (1/2) Q[f^2 grad rho .
+ * grad u] and Q[f^2 rho W]. grad is (batch, 3, n_points), grad_u (3, n_points). */
+int cdftb_external_grid_terms_f64(const double* grad, const double* rho, const double* weight, const double* grad_u,
+                                  const double* transformed_potential, const double* far_weights, int64_t n_points,
+                                  int batch, double* out, cdftb_stream_t stream);
 /* Deterministic row sums of a rows x len array (the energy integrals). */
 int64_t cdftb_row_sums_scratch_bytes(int rows, int64_t len);
 int cdftb_row_sums_f64(const double* a, int rows, int64_t len, double* out, void* scratch, int64_t scratch_bytes,

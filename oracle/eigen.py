@@ -98,7 +98,7 @@ def _fraction(value, low, high):
 
 
 class ChebyshevFilteredSubspace:
-    """CheFSI (``src/cdft/eigen/chefsi.py:850-1027`` of the listing, class at chefsi.py:408-585)."""
+    """CheFSI (``src/cdft/eigen/chefsi.py:408-585``)."""
 
     def __init__(self, n_points, *, degree, n_extra_states, extra_states_fraction=0.2, lanczos_steps=12,
                  bound_safety=1.02, max_iterations=300, residual_tol=1e-8, cross_check_tol=1e-8, ritz_stop=True):

@@ -16,7 +16,7 @@ from .rng import seeded_randn
 
 
 class Measure:
-    """``<a,b> = sum_r q(r) a(r) b(r)`` (``src/cdft/eigen/measure.py:155-233``)."""
+    """``<a,b> = sum_r q(r) a(r) b(r)`` (``src/cdft/eigen/measure.py:18-82``)."""
 
     def __init__(self, grid: Grid, quadrature: np.ndarray) -> None:
         self.grid = grid
@@ -39,14 +39,14 @@ class Measure:
 
 
 class CuspHamiltonian:
-    """``A = f^-1 H f`` in staggered divergence form (``src/cdft/operators/hamiltonian.py:375-593``)."""
+    """``A = f^-1 H f`` in staggered divergence form (``src/cdft/operators/hamiltonian.py:178-396``)."""
 
     def __init__(self, grid: Grid, factor: CuspFactor, quadrature: CuspQuadrature, extra_potential=None, bare=None):
         self.grid = grid
         self.factor = factor
         self.quadrature = quadrature
         if bare is None and quadrature is None:
-            # No quadrature: W pointwise, measure f^2 h^3 (hamiltonian.py:425-428).
+            # No quadrature: W pointwise, measure f^2 h^3 (hamiltonian.py:228-231).
             bare = (factor.transformed_potential, 1.0 / factor.weight, factor.weight * grid.volume_element)
         elif bare is None:
             bare = quadrature.bare_operator_terms()
@@ -75,7 +75,7 @@ class CuspHamiltonian:
         return lanczos_bounds(self.apply, start, self.measure.inner, self.measure.norm, steps, safety)
 
     def external_energy_parts(self, rho):
-        """``((1/2)Q[f^2 grad rho.grad u], Q[f^2 rho W])`` (hamiltonian.py:557-574)."""
+        """``((1/2)Q[f^2 grad rho.grad u], Q[f^2 rho W])`` (hamiltonian.py:360-378)."""
         q = self.quadrature
         rho_node = q.interpolate(rho)
         grad_rho_node = q.interpolate_gradient(rho)
@@ -87,7 +87,7 @@ class CuspHamiltonian:
         return cross, potential
 
     def kinetic_energy(self, phi, occupations):
-        """(hamiltonian.py:541-555)"""
+        """(hamiltonian.py:331-358)"""
         kinetic_form = self.measure.inner(phi, self.kinetic_apply(phi))
         first = (occupations * kinetic_form).sum()
         rho = (occupations[..., None] * phi ** 2).sum(axis=-2)

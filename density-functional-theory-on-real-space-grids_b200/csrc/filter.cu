@@ -3,10 +3,12 @@
 // order-8 staggered divergence-form operator (src/cdft/operators/divergence.py:99-197, epilogue of
 // src/cdft/operators/hamiltonian.py:303-318) and the recurrence update in one pass.
 //
-// Layout in HBM. The filter keeps its iterates in an internal layout: "lanes" of 8-byte elements,
-// each lane (nx, ny, nzp) with nzp = nz rounded up to even and the padding column held at zero. In
-// float32 a lane interleaves two orbitals (a float2 per point, so that the packed f32x2 FMA of sm_100
-// does two orbitals per instruction); in float64 a lane is one orbital. The block is packed into
+// Layout in HBM. The filter keeps its iterates in an internal layout: "lanes", each lane
+// (nx, ny, nzp) with nzp = nz rounded up to even and the padding column held at zero. This kernel
+// takes 8-byte lane points: in float32 a lane interleaves two orbitals (a float2 per point, so that
+// the packed f32x2 FMA of sm_100 does two orbitals per instruction); in float64 a lane is one
+// orbital. slab_filter_wide_kernel (below) takes 16-byte points -- four float32 or two float64
+// orbitals -- and serves every call with one shared geometry. The block is packed into
 // this layout once per filter call and the last step writes the caller's layout. The geometry (face
 // weights, h^3/omega, potentials) is copied once per call into rows padded to 16 bytes so that TMA
 // can read it.
@@ -554,8 +556,8 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
 // Wide lanes: 16 bytes per lane point -- four float32 orbitals (two packed f32x2 instructions per
 // element operation) or two float64 orbitals. The instructions that do not scale with the orbitals
 // (addressing, barrier waits, loads and stores of a point, the weights) are shared by twice as many
-// orbitals as in slab_filter_kernel. The roles and rings are those of slab_filter_kernel; two
-// forms keep the registers within one CTA per SM:
+// orbitals as in slab_filter_kernel. The roles and rings are those of slab_filter_kernel; two parts
+// are restructured so that a thread stays within 128 registers (one CTA of 512 threads per SM):
 //   pass item   streams its 22 nodes through a window of 8, forming each face as soon as its 8
 //               nodes are in and adding it at once to the 8 outputs it reaches (8 accumulators);
 //   march       keeps the last 8 nodes and the 8 outputs still open: each new x face is added to all

@@ -257,3 +257,44 @@ def test_config3_h2_pbe_81x81x91(pkg, cuda, golden_values, precision):
         assert out.scf_iterations == ref["iterations"]
     else:
         assert abs(out.energies["total"] - ref["total"]) < 1e-8
+
+
+@pytest.mark.parametrize("k", [1, 3])
+def test_fused_density_residual_and_external_terms(pkg, cuda, k):
+    """The two fused per-point kernels against the torch expressions they replace: the output density,
+    n_out and the residual integrand (step.py:366-370, loop.py:298-301); the grid halves of the
+    external energy parts (hamiltonian.py:360-378). With one orbital per system the rounding order
+    is the same, so the results are bit for bit; with three, the orbital sum may be ordered
+    differently by torch's reduction."""
+    call, ptr, stream_handle = pkg._lib.call, pkg._lib.ptr, pkg._lib.stream_handle
+    gen = torch.Generator(device="cpu").manual_seed(17 + k)
+    b, n = 5, 4099
+
+    def rnd(*shape, lo=0.5, hi=1.5):
+        return (lo + (hi - lo) * torch.rand(*shape, generator=gen, dtype=torch.float64)).to(cuda)
+
+    vectors = torch.randn(b, k, n, generator=gen, dtype=torch.float64).to(cuda)
+    occ = rnd(k, lo=0.0, hi=2.0)
+    f2, mass, n_in = rnd(n), rnd(n), rnd(b, n)
+    rho_out, n_out, terms = (torch.empty(b, n, dtype=torch.float64, device=cuda) for _ in range(3))
+    call("cdftb_density_residual_f64", ptr(vectors), ptr(occ), k, n, b, ptr(f2), ptr(mass), ptr(n_in), ptr(rho_out),
+         ptr(n_out), ptr(terms), stream_handle(cuda))
+    want_rho = (occ[None, :, None] * vectors.pow(2)).sum(dim=1)
+    want_n = want_rho * f2[None]
+    want_terms = mass[None] * ((want_n - n_in).abs() / f2[None])
+    if k == 1:
+        assert torch.equal(rho_out, want_rho) and torch.equal(n_out, want_n) and torch.equal(terms, want_terms)
+    else:
+        for got, want in ((rho_out, want_rho), (n_out, want_n), (terms, want_terms)):
+            torch.testing.assert_close(got, want, rtol=1e-15, atol=0)
+
+    grad = torch.randn(b, 3, n, generator=gen, dtype=torch.float64).to(cuda)
+    rho = rnd(b, n)
+    weight, tpot, far = rnd(n), rnd(n, lo=-1.0, hi=1.0), rnd(n)
+    grad_u = torch.randn(3, n, generator=gen, dtype=torch.float64).to(cuda)
+    out = torch.empty(b, 2, n, dtype=torch.float64, device=cuda)
+    call("cdftb_external_grid_terms_f64", ptr(grad), ptr(rho), ptr(weight), ptr(grad_u), ptr(tpot), ptr(far), n, b,
+         ptr(out), stream_handle(cuda))
+    dot = (grad[:, 0] * grad_u[0] + grad[:, 1] * grad_u[1]) + grad[:, 2] * grad_u[2]
+    assert torch.equal(out[:, 0], far[None] * (weight[None] * dot))
+    assert torch.equal(out[:, 1], far[None] * ((weight[None] * rho) * tpot[None]))

@@ -260,3 +260,22 @@ def test_wide_lanes_apply(pkg, cuda, kinetic):
     np.testing.assert_allclose(wide, narrow, rtol=0, atol=1e-13 * np.abs(narrow).max())
     assert not np.array_equal(wide, narrow)
     assert _device_status(pkg) == (0, 0)
+
+
+def test_more_than_65535_lanes(pkg, cuda, lanes):
+    """131075 float64 orbitals on a 2 x 2 x 2 grid: more than 65535 lanes in either layout (65538
+    wide, 131075 narrow), so the filter splits into launches with a lane offset. Sampled orbitals
+    from every launch against the oracle."""
+    shape = (2, 2, 2)
+    n = int(np.prod(shape))
+    faces, inv, q = _random_operator(shape, seed=51)
+    pot = np.random.default_rng(52).standard_normal(n)
+    ham_o, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot)
+    batch = 131075
+    block = np.random.default_rng(53).standard_normal((batch, n))
+    got = pkg.chebyshev_filter(ham, _t(block, cuda), 3, 0.5, 3.0, -1.0).cpu().numpy()
+    rows = np.array([0, 1, 2, 3, 65534, 65535, 65536, 65537, 131069, 131070, 131071, 131072, 131073, 131074])
+    want = oeigen.chebyshev_filter(ham_o, block[rows], 3, 0.5, 3.0, -1.0)
+    np.testing.assert_allclose(got[rows], want, rtol=0, atol=1e-12 * np.abs(want).max())
+    assert np.isfinite(got).all()
+    assert _device_status(pkg) == (0, 0)

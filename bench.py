@@ -348,6 +348,87 @@ def run_scan(args) -> None:
         "data": "synthetic (the H2+ systems themselves)"}), flush=True)
 
 
+def _axis_term(ham, box, axis: int):
+    """One axis's part ``D_d^T [w_d D_d phi]`` of the oracle's ``weighted_divergence`` for one orbital
+    ``box`` (nx, ny, nz): the same element-wise operations in the same order as its loop body."""
+    from oracle.grid import _pad_axis, _slice_along, staggered_coefficients
+
+    acc = ham.grid.fd_order
+    half = acc // 2
+    coeffs = staggered_coefficients(acc)
+    scale = 1.0 / ham.grid.spacing
+    shape = box.shape
+    padded = _pad_axis(box, axis, acc)
+    faces = None
+    for index, c in enumerate(coeffs):
+        term = _slice_along(padded, axis, acc - half + 1 + (index - half), shape[axis] + acc)
+        faces = term * (c * scale) if faces is None else faces + term * (c * scale)
+    faces = faces * ham.faces[axis]
+    term_sum = None
+    for index, c in enumerate(coeffs):
+        term = _slice_along(faces, axis, half - 1 - (index - half), shape[axis])
+        term_sum = term * (c * scale) if term_sum is None else term_sum + term * (c * scale)
+    return term_sum
+
+
+def _orbital_filter(axis_pool, ham, row, degree: int, lower: float, upper: float, spectrum_min: float):
+    """The oracle's ``chebyshev_filter`` for one orbital ``row`` (n,), the y and z axis terms of each
+    application on ``axis_pool`` (or inline when it is None) while the calling thread forms the x
+    term. The terms are added in the oracle's order ((x + y) + z), and h^3/omega and the potential
+    are applied as in ``apply_with_potential``. The recurrence is the oracle's."""
+    grid = ham.grid
+    n = grid.n_points
+
+    def apply(x):
+        box = x.reshape(grid.shape)
+        if axis_pool is None:
+            terms = [_axis_term(ham, box, d) for d in range(3)]
+        else:
+            pending = [axis_pool.submit(_axis_term, ham, box, d) for d in (1, 2)]
+            terms = [_axis_term(ham, box, 0)] + [f.result() for f in pending]
+        div = (terms[0] + terms[1]) + terms[2]
+        return div.reshape(n) * 0.5 * ham.inverse_weight + x * ham.potential
+
+    e = 0.5 * (upper - lower)
+    c = 0.5 * (upper + lower)
+    sigma = e / (spectrum_min - c)
+    sigma1 = sigma
+    y = (apply(row) - c * row) * (sigma1 / e)
+    previous = row
+    for _ in range(2, degree + 1):
+        sigma2 = 1.0 / (2.0 / sigma1 - sigma)
+        y_new = (apply(y) - c * y) * (2.0 * sigma2 / e) - (sigma * sigma2) * previous
+        previous, y = y, y_new
+        sigma = sigma2
+    return y
+
+
+def _threaded_filter(ham, block, degree: int, lower: float, upper: float, spectrum_min: float, threads: int):
+    """The oracle's ``chebyshev_filter`` of a block on up to ``threads`` host threads: one thread per
+    orbital (the orbitals are independent until Rayleigh--Ritz) and, with at least three threads per
+    orbital, the y and z axis terms of each application on a second pool (numpy releases the GIL in
+    its array operations). Bit-identical to ``oracle.eigen.chebyshev_filter``. Returns (result,
+    threads used)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+
+    k = block.shape[0]
+    outer = max(1, min(k, threads))
+    # the axis pool only when every orbital's y and z terms can run at once: with fewer threads the
+    # extra synchronisation per application cost more than it gained (measured on 8 and 16 cores)
+    inner = 2 * k if threads >= 3 * k else 0
+    axis_pool = ThreadPoolExecutor(inner) if inner else None
+    try:
+        with ThreadPoolExecutor(outer) as pool:
+            rows = list(pool.map(lambda o: _orbital_filter(axis_pool, ham, block[o], degree, lower, upper,
+                                                           spectrum_min), range(k)))
+    finally:
+        if axis_pool is not None:
+            axis_pool.shutdown()
+    return np.stack(rows), outer + inner
+
+
 def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     """Seconds for one full solve of the CPU restatement, from a bounded, measured sample.
 
@@ -356,17 +437,15 @@ def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     block applications and 72 potential evaluations (two per SCF iteration, 35 iterations plus the
     final one), so the estimate is the sum of those counts times the measured unit costs.
 
-    The filter runs one orbital per host thread (numpy releases the GIL in its array operations; the
-    orbitals of a block are independent until Rayleigh--Ritz), as many threads as there are orbitals
-    and cores. The potential evaluations depend on each other in a solve; within one, the Poisson
-    FFTs run on every host thread (scipy's FFT of the same transforms) and the rest on one.
+    The filter runs one orbital per host thread, with the y and z axis terms of each application on
+    further threads when the host has them (``_threaded_filter``: bit-identical to the oracle's
+    filter; up to 15 threads for 5 orbitals). The potential evaluations depend on each other in a
+    solve; within one, the Poisson FFTs run on every host thread (scipy's FFT of the same
+    transforms) and the rest on one.
     Returns (seconds, description, host threads used).
     """
-    from concurrent.futures import ThreadPoolExecutor
-
     import numpy as np
 
-    from oracle import eigen as oeigen
     from oracle import scf as oscf
     from oracle.operators import CuspHamiltonian
 
@@ -381,18 +460,15 @@ def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     t_pot = (time.perf_counter() - t) / 2
     ham = CuspHamiltonian(grid, factor, quad, extra_potential=p["effective"], bare=step.bare)
     block = np.random.default_rng(0).standard_normal((5, grid.n_points))
-    threads = max(1, min(block.shape[0], cores))
-    rows = np.array_split(np.arange(block.shape[0]), threads)
-    with ThreadPoolExecutor(threads) as pool:
-        t = time.perf_counter()
-        list(pool.map(lambda r: oeigen.chebyshev_filter(ham, block[r], 20, 1.0, 100.0, -3.0), rows))
-        t_apply = (time.perf_counter() - t) / 20
+    t = time.perf_counter()
+    _, threads = _threaded_filter(ham, block, 20, 1.0, 100.0, -3.0, cores)
+    t_apply = (time.perf_counter() - t) / 20
     n_pot = 2 * (golden["iterations"] + 1)
     full = golden["applications"] * t_apply + n_pot * t_pot
-    text = (f"numpy restatement: one degree-20 filter of 5 orbitals on {threads} host threads ({t_apply * 1e3:.0f} ms "
-            f"per block application) and two potential evaluations with the Poisson FFTs on {cores} threads "
-            f"({t_pot * 1e3:.0f} ms each), scaled to a full solve's {golden['applications']:.0f} applications and "
-            f"{n_pot} evaluations; geometry build excluded")
+    text = (f"numpy restatement: one degree-20 filter of 5 orbitals, one thread per orbital plus threads for the "
+            f"y and z axis terms ({threads} host threads, {t_apply * 1e3:.0f} ms per block application), and two "
+            f"potential evaluations with the Poisson FFTs on {cores} threads ({t_pot * 1e3:.0f} ms each), scaled to "
+            f"a full solve's {golden['applications']:.0f} applications and {n_pot} evaluations; geometry build excluded")
     return full, text, max(threads, cores)
 
 

@@ -429,6 +429,22 @@ def _threaded_filter(ham, block, degree: int, lower: float, upper: float, spectr
     return np.stack(rows), outer + inner
 
 
+def _chunked_xc(evaluate, pool, parts: int):
+    """``oracle.xc.evaluate`` on ``parts`` slices of the points at once (the functionals are
+    point-wise, so the result is bit-identical to one call on all points)."""
+    import numpy as np
+
+    def run(name, density, sigma=None):
+        density = np.asarray(density, dtype=np.float64)
+        sig = None if sigma is None else np.asarray(sigma, dtype=np.float64)
+        cuts = [c for c in np.array_split(np.arange(density.shape[0]), parts) if c.size]
+        res = list(pool.map(lambda c: evaluate(name, density[c], None if sig is None else sig[c]), cuts))
+        v_sigma = None if res[0][2] is None else np.concatenate([r[2] for r in res])
+        return np.concatenate([r[0] for r in res]), np.concatenate([r[1] for r in res]), v_sigma
+
+    return run
+
+
 def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     """Seconds for one full solve of the CPU restatement, from a bounded, measured sample.
 
@@ -440,8 +456,8 @@ def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     The filter runs one orbital per host thread, with the y and z axis terms of each application on
     further threads when the host has them (``_threaded_filter``: bit-identical to the oracle's
     filter; up to 15 threads for 5 orbitals). The potential evaluations depend on each other in a
-    solve; within one, the Poisson FFTs run on every host thread (scipy's FFT of the same
-    transforms) and the rest on one.
+    solve; within one, the Poisson FFTs (scipy's FFT of the same transforms) and the point-wise XC
+    evaluations run on every host thread, the rest on one.
     Returns (seconds, description, host threads used).
     """
     import numpy as np
@@ -454,10 +470,20 @@ def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     cores = os.cpu_count() or 1
     step.poisson.fft_workers = cores  # the Poisson FFTs on every host thread
     n0 = oscf.initial_density(step)
-    t = time.perf_counter()
-    p = step.potentials(n0)
-    p = step.potentials(n0)
-    t_pot = (time.perf_counter() - t) / 2
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import xc as oxc
+
+    serial_xc = oxc.evaluate
+    with ThreadPoolExecutor(cores) as pool:
+        oxc.evaluate = _chunked_xc(serial_xc, pool, cores)  # the XC points on every host thread
+        try:
+            t = time.perf_counter()
+            p = step.potentials(n0)
+            p = step.potentials(n0)
+            t_pot = (time.perf_counter() - t) / 2
+        finally:
+            oxc.evaluate = serial_xc
     ham = CuspHamiltonian(grid, factor, quad, extra_potential=p["effective"], bare=step.bare)
     block = np.random.default_rng(0).standard_normal((5, grid.n_points))
     t = time.perf_counter()
@@ -467,7 +493,7 @@ def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     full = golden["applications"] * t_apply + n_pot * t_pot
     text = (f"numpy restatement: one degree-20 filter of 5 orbitals, one thread per orbital plus threads for the "
             f"y and z axis terms ({threads} host threads, {t_apply * 1e3:.0f} ms per block application), and two "
-            f"potential evaluations with the Poisson FFTs on {cores} threads ({t_pot * 1e3:.0f} ms each), scaled to "
+            f"potential evaluations with the Poisson FFTs and the XC points on {cores} threads ({t_pot * 1e3:.0f} ms each), scaled to "
             f"a full solve's {golden['applications']:.0f} applications and {n_pot} evaluations; geometry build excluded")
     return full, text, max(threads, cores)
 

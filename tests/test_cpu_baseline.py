@@ -21,3 +21,20 @@ def test_threaded_filter_is_the_oracle_filter(threads):
     got, used = bench._threaded_filter(ham, block, 6, 0.5, 30.0, -1.0, threads)
     assert np.array_equal(got, want)
     assert used == (min(threads, 5) if threads < 15 else 15)
+
+
+@pytest.mark.parametrize("name", ["lda_vwn", "pbe"])
+def test_chunked_xc_is_the_oracle_xc(name):
+    from concurrent.futures import ThreadPoolExecutor
+
+    import bench
+    from oracle import xc as oxc
+
+    rng = np.random.default_rng(9)
+    density = rng.uniform(1e-6, 2.0, 1001)
+    sigma = rng.uniform(0.0, 1.0, 1001) if name == "pbe" else None
+    want = oxc.evaluate(name, density, sigma)
+    with ThreadPoolExecutor(4) as pool:
+        got = bench._chunked_xc(oxc.evaluate, pool, 7)(name, density, sigma)
+    for g, w in zip(got, want):
+        assert (g is None and w is None) or np.array_equal(g, w)

@@ -95,9 +95,10 @@ int cdftb_stencil_set_tile(int tile_y, int min_chunk, int ctas_per_sm);
  * chebyshev_coefficients, one table per potential group. block and out are in_dtype/out_dtype
  * (a double block with a float operator is cast once); work is device scratch of at least
  * cdftb_chebyshev_filter_work_bytes(op, batch) bytes, given as work_bytes. The input block is never
- * written. Order 8 runs the slab filter (internal layout: float32 orbitals interleaved in pairs, z
- * padded to even; TMA-staged tiles, bounded waits reported by cdftb_device_status); other orders
- * run one stencil launch per step on the caller's layout. */
+ * written. Order 8 runs the slab filter (internal layout: lanes of 16-byte points holding four
+ * float32 or two float64 orbitals, or with per-system geometry 8-byte points of two float32 or one
+ * float64; z padded to even; TMA-staged tiles, bounded waits reported by cdftb_device_status); other
+ * orders run one stencil launch per step on the caller's layout. */
 int64_t cdftb_chebyshev_filter_work_bytes(const cdftb_operator* op, int64_t batch);
 int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_dtype, void* out, int out_dtype,
                            void* work, int64_t work_bytes, int64_t batch, const double* coefficients, int degree,

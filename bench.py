@@ -45,7 +45,7 @@ def _args():
     p.add_argument("--impl", choices=("native", "reference"), default="native")
     p.add_argument("--form", choices=("mixed", "fp64"), default="mixed")
     p.add_argument("--batch", type=int, default=None,
-                   help="systems solved together per GPU (default 64 for the mixed form, 1 for fp64)")
+                   help="systems solved together per GPU (default 128 for the mixed form, 1 for fp64)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--kernel-only", action="store_true",
                    help="time only the fused Chebyshev step on a He grid of --edge points (for profiling)")
@@ -615,7 +615,7 @@ def main() -> None:
     grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev)
     geometry = pkg.build_cusp_geometry(grid, system.charges, system.positions)
     precision = torch.float32 if args.form == "mixed" else torch.float64
-    batch = args.batch if args.batch is not None else (64 if args.form == "mixed" else 1)
+    batch = args.batch if args.batch is not None else (128 if args.form == "mixed" else 1)
     mixing = pkg.MixingConfig(scheme="linear", alpha=0.3)
     golden = _golden()
     flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)

@@ -66,7 +66,7 @@ def test_profile_traffic_reads_the_committed_summary():
     """The bench's roofline traffic comes from the committed ncu summary (keys hold an '=' themselves)."""
     import bench
 
-    for key in ("f32x4,batch=64", "f32x4,batch=32", "f64x2,batch=1", "f32,batch=32", "f64,batch=1"):
+    for key in ("f32x4,batch=128", "f32x4,batch=64", "f32x4,batch=32", "f64x2,batch=1", "f32,batch=32", "f64,batch=1"):
         value = bench._profile_traffic(key)
         assert value is not None and value > 1e6, key
     assert bench._profile_traffic("f32,batch=7") is None

@@ -445,6 +445,26 @@ def _chunked_xc(evaluate, pool, parts: int):
     return run
 
 
+class _RowBlocks:
+    """A sparse matrix split into row blocks whose products with a vector or an (n, k) array run on a
+    thread pool (scipy releases the GIL in its sparse products). Rows are independent, so the
+    product is bit-identical to the whole matrix's."""
+
+    def __init__(self, matrix, pool, parts: int):
+        import numpy as np
+
+        m = matrix.tocsr()
+        cuts = np.linspace(0, m.shape[0], max(1, parts) + 1).round().astype(int)
+        self.blocks = [m[a:b] for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
+        self.pool = pool
+        self.shape = m.shape
+
+    def __matmul__(self, v):
+        import numpy as np
+
+        return np.concatenate(list(self.pool.map(lambda block: block @ v, self.blocks)), axis=0)
+
+
 def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     """Seconds for one full solve of the CPU restatement, from a bounded, measured sample.
 
@@ -456,8 +476,9 @@ def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     The filter runs one orbital per host thread, with the y and z axis terms of each application on
     further threads when the host has them (``_threaded_filter``: bit-identical to the oracle's
     filter; up to 15 threads for 5 orbitals). The potential evaluations depend on each other in a
-    solve; within one, the Poisson FFTs (scipy's FFT of the same transforms) and the point-wise XC
-    evaluations run on every host thread, the rest on one.
+    solve; within one, the Poisson FFTs (scipy's FFT of the same transforms), the point-wise XC
+    evaluations and the interpolant and lift products (row blocks) run on every host thread, the
+    rest on one.
     Returns (seconds, description, host threads used).
     """
     import numpy as np
@@ -475,8 +496,10 @@ def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     from oracle import xc as oxc
 
     serial_xc = oxc.evaluate
+    serial_l, serial_lt = quad.L, quad.LT
     with ThreadPoolExecutor(cores) as pool:
         oxc.evaluate = _chunked_xc(serial_xc, pool, cores)  # the XC points on every host thread
+        quad.L, quad.LT = _RowBlocks(serial_l, pool, cores), _RowBlocks(serial_lt, pool, cores)  # L and L^T too
         try:
             t = time.perf_counter()
             p = step.potentials(n0)
@@ -484,6 +507,7 @@ def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
             t_pot = (time.perf_counter() - t) / 2
         finally:
             oxc.evaluate = serial_xc
+            quad.L, quad.LT = serial_l, serial_lt
     ham = CuspHamiltonian(grid, factor, quad, extra_potential=p["effective"], bare=step.bare)
     block = np.random.default_rng(0).standard_normal((5, grid.n_points))
     t = time.perf_counter()
@@ -493,7 +517,7 @@ def oracle_solve_estimate(system, geometry, golden) -> tuple[float, str, int]:
     full = golden["applications"] * t_apply + n_pot * t_pot
     text = (f"numpy restatement: one degree-20 filter of 5 orbitals, one thread per orbital plus threads for the "
             f"y and z axis terms ({threads} host threads, {t_apply * 1e3:.0f} ms per block application), and two "
-            f"potential evaluations with the Poisson FFTs and the XC points on {cores} threads ({t_pot * 1e3:.0f} ms each), scaled to "
+            f"potential evaluations with the Poisson FFTs, the XC points and the interpolant/lift rows on {cores} threads ({t_pot * 1e3:.0f} ms each), scaled to "
             f"a full solve's {golden['applications']:.0f} applications and {n_pot} evaluations; geometry build excluded")
     return full, text, max(threads, cores)
 

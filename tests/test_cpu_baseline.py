@@ -38,3 +38,26 @@ def test_chunked_xc_is_the_oracle_xc(name):
         got = bench._chunked_xc(oxc.evaluate, pool, 7)(name, density, sigma)
     for g, w in zip(got, want):
         assert (g is None and w is None) or np.array_equal(g, w)
+
+
+def test_row_block_products_keep_the_potentials():
+    """The interpolant and lift as threaded row blocks leave the oracle's potentials bit for bit."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import bench
+    from oracle import scf as oscf
+
+    system = oscf.he_lda(spacing=0.5, edge=8.0)
+    grid, factor, quad = oscf.build_geometry(system)
+    step = oscf.KohnShamStep(system, grid, factor, quad)
+    n0 = oscf.initial_density(step)
+    want = step.potentials(n0)
+    serial = quad.L, quad.LT
+    with ThreadPoolExecutor(3) as pool:
+        quad.L, quad.LT = bench._RowBlocks(serial[0], pool, 5), bench._RowBlocks(serial[1], pool, 5)
+        try:
+            got = step.potentials(n0)
+        finally:
+            quad.L, quad.LT = serial
+    for key, value in want.items():
+        assert np.array_equal(np.asarray(got[key]), np.asarray(value)), key

@@ -74,6 +74,7 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_stencil_set_tile": (c_int, [c_int, c_int, c_int]),
     "cdftb_filter_autotune": (c_int, [c_int]),
     "cdftb_filter_wide": (c_int, [c_int]),
+    "cdftb_filter_test_withhold": (c_int, [c_int]),
     "cdftb_density_residual_f64": (c_int, [c_void_p, c_void_p, c_int, c_int64, c_int, c_void_p, c_void_p, c_void_p,
                                            c_void_p, c_void_p, c_void_p, c_void_p]),
     "cdftb_external_grid_terms_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
@@ -188,6 +189,29 @@ def call(name: str, *args) -> None:
         text = lib.cdftb_status_string(status).decode()
         cuda = lib.cdftb_last_cuda_error()
         raise CdftbError(f"{name}: {text} (status {status}, last CUDA error {cuda})")
+
+
+class DeviceTimeout(CdftbError):
+    """A kernel's bounded wait gave up (``CDFTB_ERR_TIMEOUT``): its outputs are not valid."""
+
+
+def check_device_status(where: str = "") -> None:
+    """Read and clear the library's device error flags; raise :class:`DeviceTimeout` if any was set.
+
+    Synchronises the device. The drivers call it once per SCF or eigensolver iteration, where they
+    already wait for the device to read their scalars, so that a timed-out launch stops the solve
+    instead of feeding unwritten outputs into the next step.
+    """
+    lib = library()
+    flags = c_int(0)
+    status = lib.cdftb_device_status(ctypes.byref(flags))
+    if status == 0:
+        return
+    text = lib.cdftb_status_string(status).decode()
+    if flags.value:
+        raise DeviceTimeout(f"{where or 'cdftb'}: a kernel gave up waiting ({text}, flags {flags.value}); "
+                            "its results were discarded")
+    raise CdftbError(f"cdftb_device_status: {text} (status {status})")
 
 
 def ptr(t: torch.Tensor | None):

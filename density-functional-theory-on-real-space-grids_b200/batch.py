@@ -223,6 +223,7 @@ def batched_lanczos(h: BatchedHamiltonian, starts: torch.Tensor, steps: int, saf
         v_prev, v = v, w
         beta_prev = beta
     values = torch.stack([*alphas, *betas]).cpu().numpy()  # (2 steps, b)
+    _lib.check_device_status("batched_lanczos")
     out = []
     for s in range(b):
         a = list(values[:steps, s])
@@ -258,6 +259,7 @@ class _EigenState:
     stop_reason: str = "iteration limit"
     float_filter: bool = False
     stable: int = 0
+    applications: int = 0  # block applications of this system's operator (Lanczos, filter, Ritz)
 
 
 def _stable(state, drift: float, tol: float) -> bool:
@@ -314,8 +316,11 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
         for s, bb in zip(need, batched_lanczos(sub, starts, config.lanczos_steps, config.bound_safety)):
             states[s].spectrum = bb
             states[s].source = "lanczos"
+            states[s].applications += config.lanczos_steps
         h.applications += sub.applications if sub is not h else 0
     evals, vectors, residual, _, _ = batched_rayleigh_ritz(h, block, check_orthonormality=False)
+    for st in states:
+        st.applications += 1
     top = m - 1
     tops = evals[:, top].tolist()
     for s in range(b):
@@ -348,6 +353,7 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
             for s, bb in zip(redo, batched_lanczos(sub, starts, config.lanczos_steps, config.bound_safety)):
                 states[s].spectrum = bb
                 states[s].source = "lanczos (reuse rejected)"
+                states[s].applications += config.lanczos_steps
             h.applications += sub.applications
         rows = []
         use_float = []
@@ -384,6 +390,7 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
         drift = (ev[:, :n_states] - prev[:, :n_states]).abs().amax(dim=1)
         worst = res[:, :n_states].amax(dim=1)
         host = torch.stack([worst, drift, ev[:, top], info.to(torch.float64)]).cpu().numpy()
+        _lib.check_device_status(f"batched CheFSI iteration {iteration}")
         if (host[3] != 0).any():
             raise RuntimeError("a filtered block lost rank (Cholesky failed) in the batched solver; "
                                "solve that system with the single-system driver")
@@ -399,6 +406,7 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
         for j, s in enumerate(active):
             st = states[s]
             st.iterations = iteration
+            st.applications += config.chebyshev_degree + 1  # the filter and the Rayleigh--Ritz apply
             st.next_lower = float(host[2, j])
             if host[0, j] < config.residual_tol:
                 st.converged = True
@@ -753,6 +761,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         res_norm = row_sums(res_terms)
         keys = list(terms)
         host = torch.stack([*terms.values(), res_norm]).cpu().numpy()  # (len(keys)+1, S)
+        _lib.check_device_status(f"batched SCF iteration {iteration}")
         # mixing (per system: linear in one batched expression when all are linear)
         n_next = torch.empty_like(nin)
         linear = all(isinstance(systems[s].mixer, LinearMixer) for s in active)
@@ -774,7 +783,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         for j, s in enumerate(active):
             st = systems[s]
             st.iterations = iteration
-            st.applications += h.applications
+            st.applications += estates[j].applications
             total = float(host[keys.index("total"), j])
             rn = float(host[-1, j])
             st.energies.append(total)
@@ -846,11 +855,13 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
     keys = list(terms)
     host = torch.stack([*terms.values(), charge]).cpu().numpy()
     ev = evals.cpu().numpy()
+    _lib.check_device_status("batched final diagonalisation")
     energies = [{k: float(host[i, s]) for i, k in enumerate(keys)} for s in range(b)]
     final_converged = [bool(es.converged) for es in estates]
-    apps = sum(st.applications for st in systems) + h.applications
+    apps = sum(st.applications for st in systems) + sum(es.applications for es in estates)
     measurements = {
         "batch": b,
+        "applications_per_system": [st.applications + es.applications for st, es in zip(systems, estates)],
         "charge_error": [abs(float(host[-1, s]) - step.n_electrons) for s in range(b)],
         "fp64_refinement_from_iteration": [st.refinement_from for st in systems],
         "filter_precision": "float32" if mixed else "float64",
@@ -1031,6 +1042,7 @@ def solve_noninteracting_batch(geometries, n_electrons: float, *, seeds=None, ei
         BatchedKohnShamStep.FLOAT_FILTER_SWITCH_RESIDUAL if h32 is not None else None, ritz_stop=True)
     occ = aufbau_occupations(n_states, float(n_electrons))[0]
     values = evals.cpu().numpy()
+    _lib.check_device_status("batched non-interacting solve")
     out = []
     for s, g in enumerate(geometries):
         band = float((occ * values[s]).sum())

@@ -33,6 +33,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -149,6 +150,8 @@ struct FilterArgs {
     int per_system_geometry;  // face weights and h^3/omega per orbital group (systems on their own grids)
     int lanes_per_group;      // > 0: lanes aligned to orbital groups (lane l holds group l / lanes_per_group)
     int kinetic_only;      // with apply_only: out = 0.5 (h^3/omega) div phi (no potential)
+    int stop_after_planes;  // > 0 only in the timeout test: the producer issues this many planes' copies
+                            // and no more, so the consumers' bounded waits run out with no copy in flight
     const double* coef;
     int degree;
     int step;
@@ -319,6 +322,7 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
         int issued = 0;
         int s = 0, ph = 1;  // slot; parity of its previous use (the first R fills wait for nothing)
         for (int n = 0; n < npl; ++n) {
+            if (a.stop_after_planes > 0 && n >= a.stop_after_planes) break;
             if (n >= R && !wait_full(bar_empty + 8 * s, ph, a.token)) break;
             const unsigned full = bar_full + 8 * s;
             unsigned char* slot = smem + s * SH::SLOT;
@@ -729,6 +733,7 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
         int issued = 0;
         int s = 0, ph = 1;
         for (int n = 0; n < npl; ++n) {
+            if (a.stop_after_planes > 0 && n >= a.stop_after_planes) break;
             if (n >= RW && !wait_full(bar_empty + 8 * s, ph, a.token)) break;
             const unsigned full = bar_full + 8 * s;
             unsigned char* slot = smem + s * SH::SLOT;
@@ -1182,6 +1187,22 @@ int sm_count() {
     return count;
 }
 
+// Abort tokens: never 0, distinct between the two kernels (8-byte lanes 1 .. 2^30 - 1, wide lanes
+// 2^30 .. 2^31 - 1), taken atomically so that launches from several host threads never share one.
+std::atomic<unsigned> g_next_token{0};
+
+unsigned next_launch_token(bool wide) {
+    unsigned v = g_next_token.fetch_add(1u, std::memory_order_relaxed) & 0x3fffffffu;
+    if (v == 0) v = g_next_token.fetch_add(1u, std::memory_order_relaxed) & 0x3fffffffu;
+    return wide ? (0x40000000u | v) : v;
+}
+
+// The timeout test's one-shot setting (cdftb_filter_test_withhold): the next slab launch stops
+// issuing copies after this many planes. 0: off.
+std::atomic<int> g_test_stop_after{0};
+
+int take_test_stop() { return g_test_stop_after.exchange(0, std::memory_order_relaxed); }
+
 template <typename Lane, int TZ>
 int launch_slab(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
     using SH = Shape<TZ, sizeof(typename Lane::S)>;
@@ -1197,13 +1218,11 @@ int launch_slab(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_
     const int64_t tiles = int64_t(tiles_y) * a.tiles_z;
     a.xchunk = xchunk > 0 ? (xchunk < a.nx ? xchunk : a.nx) : choose_chunk(a.nx, tiles * lanes, sm_count());
     const int chunks = static_cast<int>(ceil_div(a.nx, a.xchunk));
-    static unsigned next_token = 0;
     for (int64_t first = 0; first < lanes; first += 65535) {
         const int64_t count = (lanes - first) < 65535 ? (lanes - first) : 65535;
         a.lane_first = first;
-        next_token = (next_token + 1) & 0x7fffffffu;
-        if (next_token == 0) next_token = 1;
-        a.token = next_token;
+        a.token = next_launch_token(false);
+        a.stop_after_planes = take_test_stop();
         dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(chunks), static_cast<unsigned>(count));
         slab_filter_kernel<Lane, TZ><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
         int st = check_launch();
@@ -1338,12 +1357,11 @@ int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_
     a.xchunk = xchunk > 0 ? (xchunk < a.nx ? xchunk : a.nx) : choose_chunk(a.nx, tiles * lanes, sm_count());
     a.lanes_per_group = 0;
     const int chunks = static_cast<int>(ceil_div(a.nx, a.xchunk));
-    static unsigned next_token = 0x40000000u;
     for (int64_t first = 0; first < lanes; first += 65535) {
         const int64_t count = (lanes - first) < 65535 ? (lanes - first) : 65535;
         a.lane_first = first;
-        next_token = 0x40000000u | ((next_token + 1) & 0x3fffffffu);
-        a.token = next_token;
+        a.token = next_launch_token(true);
+        a.stop_after_planes = take_test_stop();
         dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(chunks), static_cast<unsigned>(count));
         slab_filter_wide_kernel<W, TZ><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
         int st = check_launch();
@@ -1696,6 +1714,12 @@ extern "C" int cdftb_filter_tuned_tile(int nx, int ny, int nz, int dtype, int64_
     }
     *tile_z = c.tz;
     *x_chunk = c.xchunk;
+    return CDFTB_OK;
+}
+
+extern "C" int cdftb_filter_test_withhold(int planes) {
+    if (planes < 0) return CDFTB_ERR_ARGUMENT;
+    cdftb::g_test_stop_after.store(planes, std::memory_order_relaxed);
     return CDFTB_OK;
 }
 

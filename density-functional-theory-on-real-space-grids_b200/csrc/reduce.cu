@@ -4,6 +4,11 @@
 // columns for a tile of (i, j) pairs into a partial, and a second kernel sums the partials of each
 // pair in chunk order, so the result does not depend on scheduling.
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "common.cuh"
 
 namespace cdftb {
@@ -221,8 +226,10 @@ extern "C" int cdftb_measure_cross_grouped_f64(const double* a, int ma, int64_t 
 // ---------------------------------------------------------------------------------------------
 // cdftb_measure_cross_static_f64: the same product with its partials in a fixed device array of
 // this library instead of caller scratch, for callers that cannot allocate device memory. The
-// array lives once per device (each device's copy of this module); its address is looked up with
-// cudaGetSymbolAddress on the first call on that device and kept. The first pass writes every
+// array lives once per device (each device's copy of this module). Its address is looked up with
+// cudaGetSymbolAddress on the first call in each CUDA context and kept with that context's ID: a
+// device reset destroys the primary context, the module is loaded again (possibly elsewhere), and
+// the next call, seeing a new context ID, looks the address up again. The first pass writes every
 // partial that the second pass reads, so nothing in the array has to start at zero. Two calls whose
 // work overlaps on the GPU (other streams, other host threads) share the array and race.
 
@@ -234,19 +241,55 @@ constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) static unsigned char g_static_cross_scratch[kStaticCrossScratchBytes];
 
-void* g_static_cross_address[kMaxDevices] = {};
+struct StaticScratchEntry {
+    unsigned long long context_id = 0;  // 0: not looked up yet (CUDA context IDs start at 1)
+    void* address = nullptr;
+};
+StaticScratchEntry g_static_cross[kMaxDevices];
+std::mutex g_static_cross_mutex;
+
+// The ID of the calling thread's current CUDA context, through the driver entry points the runtime
+// hands out (no link against the driver library); 0 when there is none yet or the lookup failed.
+unsigned long long current_context_id() {
+    static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 4000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return 0;
+        get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return 0;
+        get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    unsigned long long id = 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 int static_cross_scratch(void** out) {
     int dev = -1;
     int rc = check(cudaGetDevice(&dev));
     if (rc != CDFTB_OK) return rc;
     if (dev < 0 || dev >= kMaxDevices) return CDFTB_ERR_CAPACITY;
-    void* p = __atomic_load_n(&g_static_cross_address[dev], __ATOMIC_ACQUIRE);
-    if (!p) {
-        rc = check(cudaGetSymbolAddress(&p, g_static_cross_scratch));
-        if (rc != CDFTB_OK) return rc;
-        __atomic_store_n(&g_static_cross_address[dev], p, __ATOMIC_RELEASE);
+    std::lock_guard<std::mutex> lock(g_static_cross_mutex);
+    StaticScratchEntry& entry = g_static_cross[dev];
+    unsigned long long id = current_context_id();
+    if (id != 0 && id == entry.context_id) {
+        *out = entry.address;
+        return CDFTB_OK;
     }
+    void* p = nullptr;
+    rc = check(cudaGetSymbolAddress(&p, g_static_cross_scratch));  // makes the runtime's context current
+    if (rc != CDFTB_OK) return rc;
+    if (id == 0) id = current_context_id();
+    entry.context_id = id;  // still 0 if the driver gave no ID: then the next call looks it up again
+    entry.address = p;
     *out = p;
     return CDFTB_OK;
 }

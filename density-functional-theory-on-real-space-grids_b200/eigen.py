@@ -325,6 +325,7 @@ class ChebyshevFilteredSubspace:
             worst, drift, orth, next_lower, chol = torch.stack([
                 residual[:n_states].max(), (evals[:n_states] - previous[:n_states]).abs().max(), orth_error,
                 evals[top], info[0].to(torch.float64)]).tolist()
+            _lib.check_device_status(f"CheFSI iteration {iteration}")
             if chol != 0.0:
                 # rank-deficient filtered block: redo this step with the eigh fallback (rayleigh_ritz.py:64-70)
                 evals, vectors, orth_error = rayleigh_ritz(hamiltonian, filtered, measure, host=False)
@@ -351,4 +352,5 @@ class ChebyshevFilteredSubspace:
                 break
         self.spectral_bounds = (spectrum_min, spectrum_max)
         self.top_ritz_fraction = top_fraction
+        _lib.check_device_status("ChebyshevFilteredSubspace.solve")
         return EigenResult(evals[:n_states], vectors[:n_states], residual[:n_states], iteration, converged)

@@ -299,6 +299,7 @@ def lanczos_bounds(hamiltonian: CuspFactoredHamiltonian, start: torch.Tensor, st
         v_prev, v = v, w
         beta_prev = beta
     values = torch.cat([*alphas, *betas]).tolist()
+    _lib.check_device_status("lanczos_bounds")
     a = values[:steps]
     b = values[steps:]
     for index, value in enumerate(b):

@@ -558,6 +558,7 @@ def solve_self_consistent(step: KohnShamStep, mixing: MixingConfig | None = None
         n_next = mixer.mix(n_in, n_out, iteration)
         change_d = norm_l1(n_next - n_in)
         host = torch.stack([*terms.values(), res_norm_d, change_d]).tolist()
+        _lib.check_device_status(f"SCF iteration {iteration}")
         nt = len(terms)
         values = dict(zip(terms, host[:nt]))
         res_norm, change = host[nt], host[nt + 1]
@@ -598,6 +599,7 @@ def solve_self_consistent(step: KohnShamStep, mixing: MixingConfig | None = None
     terms = step.energy_terms(eigen, occupations, rho_out, p_in, p_out)
     charge = row_sums((mass * rho_out)[None])[0]
     host = torch.stack([*terms.values(), charge, *eigen.eigenvalues]).tolist()
+    _lib.check_device_status("final diagonalisation")
     nt = len(terms)
     final = dict(zip(terms, host[:nt]))
     measurements = {

@@ -132,6 +132,13 @@ int cdftb_filter_wide(int enable);
  * clears them; status CDFTB_ERR_TIMEOUT when any flag was set. */
 int cdftb_device_status(int* flags);
 
+/* No reference counterpart: a test of the bounded waits above. The next slab-filter launch (filter
+ * step or one-launch apply, order 8) issues the TMA copies of its first `planes` planes in x and no
+ * more, so its consumers' waits run out (2 s) with no copy in flight; the launch then records the
+ * timeout (cdftb_device_status returns CDFTB_ERR_TIMEOUT once) and its outputs are not written. One
+ * launch only: the setting clears itself. 0 turns a pending setting off. */
+int cdftb_filter_test_withhold(int planes);
+
 /* (e1) out[g][i][j] = sum_p q[p] a[g][i][p] b[g][j][p] (src/cdft/eigen/measure.py:72-96,
  * Measure.inner/gram/cross), f64, deterministic two-pass reduction. a and b hold `groups`
  * blocks of ma and mb rows, group_stride_a/b elements apart. q may be NULL (plain sum). */
@@ -152,8 +159,10 @@ int cdftb_measure_cross_grouped_f64(const double* a, int ma, int64_t group_strid
  * caller scratch. This call allocates nothing (no cudaMalloc, no cudaFree).
  * - Returns CDFTB_ERR_CAPACITY when cdftb_measure_cross_scratch_bytes(ma, mb, n, groups) exceeds
  *   that capacity.
- * - The first call on a device looks up the array's address (cudaGetSymbolAddress, checked;
- *   CDFTB_ERR_LAUNCH on failure). That set-up call must come before any stream capture.
+ * - The first call in each CUDA context on a device looks up the array's address
+ *   (cudaGetSymbolAddress, checked; CDFTB_ERR_LAUNCH on failure) and keeps it with the context's ID,
+ *   so after a device reset (a new primary context) the next call looks it up again. That set-up
+ *   call must come before any stream capture.
  * - Calls whose work overlaps on the GPU (several streams or host threads on one device) share the
  *   array and race; the caller orders them.
  * - Nothing in the array has to start at zero: the first pass writes every partial the second

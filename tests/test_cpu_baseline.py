@@ -61,3 +61,28 @@ def test_row_block_products_keep_the_potentials():
             quad.L, quad.LT = serial
     for key, value in want.items():
         assert np.array_equal(np.asarray(got[key]), np.asarray(value)), key
+
+
+def test_threaded_whole_solve_is_the_oracle_solve():
+    """The timed CPU solve (the oracle's own solve with its parts on host threads) gives the oracle's
+    energies and density bit for bit, and the patched functions are restored afterwards."""
+    import bench
+    from oracle import operators as oops
+    from oracle import scf as oscf
+    from oracle import xc as oxc
+
+    system = oscf.he_lda(spacing=0.5, edge=8.0)
+    geometry = oscf.build_geometry(system)
+    want = oscf.solve_self_consistent(system, geometry)
+    saved = (oxc.evaluate, oops.CuspHamiltonian.kinetic_apply, oops.CoulombCutoffPoisson.solve,
+             oscf.KohnShamStep.potentials, geometry[2].L, geometry[2].LT)
+    got, seconds, breakdown = bench.oracle_solve(system, geometry, 4)
+    assert (oxc.evaluate, oops.CuspHamiltonian.kinetic_apply, oops.CoulombCutoffPoisson.solve,
+            oscf.KohnShamStep.potentials, geometry[2].L, geometry[2].LT) == saved
+    assert got["scf_iterations"] == want["scf_iterations"]
+    # the FFTs differ (scipy on threads vs numpy): the Poisson solution agrees to rounding only
+    assert abs(got["energies"]["total"] - want["energies"]["total"]) < 1e-12
+    assert np.abs(got["density"] - want["density"]).max() < 1e-10
+    # the operator applications plus one kinetic application per energy evaluation
+    assert breakdown["block_applications"] == want["applications"] + want["scf_iterations"] + 1
+    assert seconds > 0.0

@@ -470,9 +470,12 @@ class HostThreads:
 
     Inside the context, for the geometry ``(grid, factor, quadrature)``:
 
-    - every block application's axis terms ``D_d^T[w_d D_d phi]`` run one task per (orbital, axis)
-      on a pool of ``cores`` threads (``_axis_term``: the oracle's element-wise operations in its
-      order; the terms are added ``(x + y) + z`` as the oracle's ``weighted_divergence`` does);
+    - the Chebyshev filter runs one orbital per thread, with each application's y and z axis terms
+      on further threads when the host has them (``_threaded_filter``: the recurrence of every
+      orbital is independent until Rayleigh--Ritz);
+    - every other block application's axis terms ``D_d^T[w_d D_d phi]`` run one task per (orbital,
+      axis) (``_axis_term``: the oracle's element-wise operations in its order; the terms are added
+      ``(x + y) + z`` as the oracle's ``weighted_divergence`` does);
     - the point-wise XC evaluations run as slices of the points (``_chunked_xc``);
     - the interpolant and the lift run as row blocks of the sparse matrices (``_RowBlocks``);
     - the Poisson FFTs use scipy's FFT of the same transforms on every thread.
@@ -497,12 +500,26 @@ class HostThreads:
         from oracle import scf as oscf
         from oracle import xc as oxc
 
+        from oracle import eigen as oeigen
+
         self._pool = ThreadPoolExecutor(self.cores)
         pool, cores, box_shape = self._pool, self.cores, self.grid.shape
         self._saved = (oxc.evaluate, self.quadrature.L, self.quadrature.LT, oops.CoulombCutoffPoisson.solve,
-                       oops.CuspHamiltonian.kinetic_apply, oscf.KohnShamStep.potentials)
-        serial_xc, _, _, serial_poisson, _, serial_potentials = self._saved
+                       oops.CuspHamiltonian.kinetic_apply, oscf.KohnShamStep.potentials, oeigen.chebyshev_filter)
+        serial_xc, _, _, serial_poisson, _, serial_potentials, serial_filter = self._saved
         seconds, counts = self.seconds, self.counts
+
+        def chebyshev_filter(ham, block, degree, lower, upper, spectrum_min):
+            if type(ham) is not oops.CuspHamiltonian:  # e.g. a level-shifted operator: the serial filter
+                return serial_filter(ham, block, degree, lower, upper, spectrum_min)
+            if upper <= lower:
+                raise ValueError(f"filter interval is empty: lower={lower}, upper={upper}")
+            t = time.perf_counter()
+            out, _ = _threaded_filter(ham, block, degree, lower, upper, spectrum_min, cores)
+            ham.apply_count += degree
+            seconds["applications"] += time.perf_counter() - t
+            counts["applications"] += degree
+            return out
 
         def kinetic_apply(ham, phi):
             t = time.perf_counter()
@@ -535,15 +552,17 @@ class HostThreads:
         oops.CoulombCutoffPoisson.solve = poisson_solve
         oops.CuspHamiltonian.kinetic_apply = kinetic_apply
         oscf.KohnShamStep.potentials = potentials
+        oeigen.chebyshev_filter = chebyshev_filter
         return self
 
     def __exit__(self, *exc):
+        from oracle import eigen as oeigen
         from oracle import operators as oops
         from oracle import scf as oscf
         from oracle import xc as oxc
 
         (oxc.evaluate, self.quadrature.L, self.quadrature.LT, oops.CoulombCutoffPoisson.solve,
-         oops.CuspHamiltonian.kinetic_apply, oscf.KohnShamStep.potentials) = self._saved
+         oops.CuspHamiltonian.kinetic_apply, oscf.KohnShamStep.potentials, oeigen.chebyshev_filter) = self._saved
         self._pool.shutdown()
         return False
 

@@ -108,8 +108,8 @@ class KohnShamStep:
     def potentials(self, density: torch.Tensor) -> Potentials:
         if density.shape[0] != 1:
             raise NotImplementedError("the self-consistent path is spin-restricted (n_spin = 1)")
-        if self.functional.rung >= 2:
-            return self._potentials_gga(density)
+        if self.functional.name != "lda_vwn":
+            return self._potentials_generic(density)
         g = self.geometry
         q = self.quadrature
         grid = self.grid
@@ -153,8 +153,11 @@ class KohnShamStep:
         return Potentials(v_hartree=v_hartree, v_xc=v_xc[None, :], effective=effective, hartree_energy=0.5 * sums[0],
                           xc_energy=node_sum + sums[2], xc_double_counting=sums[1], hartree_coefficients=coef)
 
-    def _potentials_gga(self, density: torch.Tensor) -> Potentials:
-        """GGA potentials (step.py:252-280): the gradient term in weak form, by lift and FD transpose."""
+    def _potentials_generic(self, density: torch.Tensor) -> Potentials:
+        """Potentials for any native functional (step.py:224-313) through ``functional.evaluate``;
+        a GGA adds the gradient term in weak form, by lift and FD transpose (step.py:252-280). The
+        spin-restricted VWN LDA takes the fused kernels of :meth:`potentials` instead."""
+        gga = self.functional.rung >= 2
         g = self.geometry
         q = self.quadrature
         grid = self.grid
@@ -179,6 +182,25 @@ class KohnShamStep:
              ptr(n_smooth), stream)
         v_smooth = self.poisson.solve(n_smooth)
         v_h_grid = (coef[:, None] * g.step.v1s_grid).sum(dim=0) + v_smooth
+        if not gga:
+            node = q.interpolate(torch.cat([rho[None], v_smooth[None]]))
+            rho_node, vs_node = node[0], node[1]
+            v_h_node = (coef[:, None] * g.step.v1s_node).sum(dim=0) + vs_node
+            n_node = q.f2 * rho_node
+            out_grid = self.functional.evaluate(n_grid[None, :])
+            out_node = self.functional.evaluate(n_node[None, :])
+            e_n_node, e_n_grid = out_node.v_xc[0], out_grid.v_xc[0]
+            lift_in = torch.cat([(q.weights * (q.f2 * v_h_node))[None], (q.weights * (q.f2 * e_n_node))[None]])
+            lifted = q.lift(lift_in.contiguous())
+            hartree_w = lifted[0] + q.far_weights * (f2 * v_h_grid)
+            xc_w = lifted[1] + q.far_weights * (f2 * e_n_grid)
+            hartree_energy = 0.5 * row_sums((hartree_w * rho)[None])[0]
+            xc_energy = q.integrate(out_node.e_xc, out_grid.e_xc)
+            xc_dc = row_sums((xc_w * rho)[None])[0]
+            effective = (hartree_w + xc_w) / q.mass_weights
+            return Potentials(v_hartree=v_h_grid, v_xc=e_n_grid[None, :].clone(), effective=effective,
+                              hartree_energy=hartree_energy, xc_energy=xc_energy, xc_double_counting=xc_dc,
+                              hartree_coefficients=coef)
         grad_rho = gradient(grid, rho)
         node = q.interpolate(torch.cat([rho[None], grad_rho, v_smooth[None]]))
         rho_node, grad_rho_node, vs_node = node[0], node[1:4], node[4]

@@ -249,6 +249,40 @@ int cdftb_xc_lda_vwn_f64(const double* density, int64_t points, double* e, doubl
 int cdftb_xc_pbe_f64(const double* density, const double* sigma, int64_t points, double* e, double* v, double* vs,
                      cdftb_stream_t stream);
 
+/* ---- (d) every native functional, spin-restricted or spin-polarised (src/cdft/xc/base.py:45-189) ---- */
+
+/* The functional names of src/cdft/xc/dispatch.py:26-44 (_builders). */
+typedef enum cdftb_xc_id {
+    CDFTB_XC_LDA_VWN = 0,      /* lda_vwn: Slater + VWN5 */
+    CDFTB_XC_LDA_PW92 = 1,     /* lda_pw92: Slater + PW92 (original parameters) */
+    CDFTB_XC_LDA_PW92_MOD = 2, /* lda_pw92_mod: Slater + PW92 (modified parameters, as inside PBE) */
+    CDFTB_XC_LDA_PZ81 = 3,     /* lda_pz81: Slater + PZ81 */
+    CDFTB_XC_PBE = 4,          /* pbe: PBE exchange + PBE correlation */
+    CDFTB_XC_BLYP = 5,         /* blyp: B88 exchange + LYP correlation */
+    CDFTB_XC_LDA_X = 6,        /* lda_x: Slater exchange alone */
+    CDFTB_XC_LDA_C_VWN = 7,    /* lda_c_vwn */
+    CDFTB_XC_LDA_C_PW = 8,     /* lda_c_pw */
+    CDFTB_XC_LDA_C_PW_MOD = 9, /* lda_c_pw_mod */
+    CDFTB_XC_LDA_C_PZ = 10,    /* lda_c_pz */
+    CDFTB_XC_GGA_X_PBE = 11,   /* gga_x_pbe */
+    CDFTB_XC_GGA_C_PBE = 12,   /* gga_c_pbe */
+    CDFTB_XC_GGA_X_B88 = 13,   /* gga_x_b88 */
+    CDFTB_XC_GGA_C_LYP = 14    /* gga_c_lyp */
+} cdftb_xc_id;
+
+/* 1 if `functional` (a cdftb_xc_id) needs sigma, 0 if not, -1 for an unknown id. */
+int cdftb_xc_is_gga(int functional);
+
+/* SemiLocalFunctional.evaluate (xc/base.py:115-156) for one functional on `points` points:
+ * density (n_spin, points) with n_spin 1 (total density) or 2 (n_up, n_dn rows); for a GGA, sigma
+ * (1, points) or (3, points) = (uu, ud, dd) rows. Writes e (points,) the energy per volume,
+ * v (n_spin, points) = de/dn per channel and, for a GGA, v_sigma (1 or 3, points) = de/dsigma per
+ * component. Spin split, thresholds, clamps and empty points as base.py:45-80, 171-189; the
+ * derivatives are exact derivatives of the energy density (forward-mode dual numbers), as the
+ * reference's autograd gives them. sigma and v_sigma may be NULL for an LDA. */
+int cdftb_xc_eval_f64(int functional, int n_spin, const double* density, const double* sigma, int64_t points,
+                      double* e, double* v, double* v_sigma, cdftb_stream_t stream);
+
 /* ---- (d4) cusp-aware quadrature interpolant (src/cdft/operators/quadrature.py:506-650) ---- */
 
 /* Stencil corner (m x 3 ints) and the three 8-point Lagrange weight vectors (m x 24) of every point

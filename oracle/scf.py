@@ -121,7 +121,7 @@ class KohnShamStep:
         n_node, grad_n_node = q.density_gradient_at_nodes(rho)
         hartree_weights = q.lumped_weights(q.f2 * v_h_node, f2 * v_h_grid)
         hartree_energy = 0.5 * (hartree_weights * rho).sum()
-        gga = self.functional == "pbe"
+        gga = xc_mod.RUNG[self.functional] >= 2
         grad_n_grid = q.density_gradient_on_grid(rho) if gga else None
         sigma_grid = (grad_n_grid * grad_n_grid).sum(axis=0) if gga else None
         sigma_node = (grad_n_node * grad_n_node).sum(axis=0) if gga else None

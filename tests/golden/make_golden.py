@@ -1,6 +1,6 @@
 """Generate the golden fixtures by running the reference solver ``cdft`` itself.
 
-Run in the build container, where the reference is mounted read-only at ``/root/reference``:
+Run where the reference checkout is readable (``CDFT_REFERENCE``, default ``/root/reference``):
 
     PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [--with-65]
 
@@ -20,7 +20,7 @@ import sys
 import time
 from pathlib import Path
 
-REFERENCE = Path("/root/reference")
+REFERENCE = Path(os.environ.get("CDFT_REFERENCE", "/root/reference"))  # the reference checkout (read only)
 OUT = Path(__file__).resolve().parent
 
 os.environ.setdefault("PYTHONDONTWRITEBYTECODE", "1")

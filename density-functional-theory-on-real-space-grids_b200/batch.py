@@ -32,8 +32,8 @@ from .grid import UniformGrid
 from .operators import apply_workspace, cast, measure_cross, rowwise_inner
 from .poisson import CoulombCutoffPoisson
 from .rng import SeededStream
-from .scf import (FILTER_STEPS_PER_ITERATION, BoundReusePolicy, LinearMixer, MixingConfig, PulayMixer, SCFConfig,
-                  aufbau_occupations, nuclear_repulsion)
+from .scf import (FILTER_STEPS_PER_ITERATION, BoundReusePolicy, LinearMixer, MixingConfig, SCFConfig,
+                  aufbau_occupations, make_mixer, nuclear_repulsion)
 from .xc import functional_by_name
 
 
@@ -693,11 +693,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
     mixed = step.filter_precision == torch.float32
 
     def make(alpha, scheme=None):
-        scheme = scheme or mixing.scheme
-        if scheme == "linear":
-            return LinearMixer(alpha)
-        period = mixing.pulay_period if scheme == "periodic_pulay" else 1
-        return PulayMixer(alpha, mixing.history, period, inner_weights)
+        return make_mixer(mixing, alpha, inner_weights, scheme, grid=step.grid)
 
     systems = [_SystemState(mixer=make(mixing.alpha), policy=BoundReusePolicy(), float_phase=mixed) for _ in range(b)]
     n_in = (initial_density if initial_density is not None else step.initial_density()).to(torch.float64).clone()
@@ -764,7 +760,9 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         _lib.check_device_status(f"batched SCF iteration {iteration}")
         # mixing (per system: linear in one batched expression when all are linear)
         n_next = torch.empty_like(nin)
-        linear = all(isinstance(systems[s].mixer, LinearMixer) for s in active)
+        # a preconditioned residual is not the difference of the two densities' linear parts
+        linear = all(isinstance(systems[s].mixer, LinearMixer) and systems[s].mixer.preconditioner is None
+                     for s in active)
         lin_next = None
         if linear:
             # x_in + alpha (x_out - x_in) per system (LinearMixer.mix, element for element) in one expression per

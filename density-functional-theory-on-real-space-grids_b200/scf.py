@@ -316,35 +316,64 @@ def initial_density(step: KohnShamStep, kind: str = "hydrogenic") -> torch.Tenso
     return total[None, :].clone()
 
 
+class KerkerPreconditioner:
+    """``F(q) q^2 / (q^2 + q0^2)`` on the box (``src/cdft/scf/mixing.py:35-56``), one library call
+    (``cdftb_kerker_precondition_f64``) for every spin row of a ``(n_spin, N)`` residual."""
+
+    def __init__(self, grid, q0: float) -> None:
+        self.grid = grid
+        self.q0 = float(q0)
+
+    def __call__(self, residual: torch.Tensor) -> torch.Tensor:
+        _lib.require_cuda(residual, "residual")
+        x = residual.to(torch.float64).contiguous()
+        rows = x.numel() // self.grid.n_points
+        nbytes = _lib.library().cdftb_kerker_work_bytes(*self.grid.shape, rows)
+        work = torch.empty(nbytes, dtype=torch.uint8, device=x.device)
+        out = torch.empty_like(x)
+        call("cdftb_kerker_precondition_f64", ptr(x), rows, *self.grid.shape, self.grid.spacing, self.q0, ptr(out),
+             ptr(work), nbytes, stream_handle(x.device))
+        return out
+
+
 class LinearMixer:
     """(``src/cdft/scf/mixing.py:59-83``)"""
 
-    def __init__(self, alpha: float):
+    def __init__(self, alpha: float, preconditioner=None):
         if not 0.0 < alpha <= 1.0:
             raise ValueError("mixing alpha must lie in (0, 1]")
         self.alpha = alpha
-        self.name = f"linear(alpha={alpha:g})"
-        self.last_event = "linear step"
+        self.preconditioner = preconditioner
+        self.name = f"linear mixing, alpha {alpha:g}"
+        self.last_event = "damped step"
 
     def mix(self, n_in, n_out, iteration):
-        return n_in + self.alpha * (n_out - n_in)
+        residual = n_out - n_in
+        if self.preconditioner is not None:
+            residual = self.preconditioner(residual)
+        return n_in + self.alpha * residual
 
 
 class PulayMixer:
     """Periodic Pulay / DIIS (``src/cdft/scf/mixing.py:86-162``); residual products on the device."""
 
-    def __init__(self, alpha: float, history: int, period: int, inner_weights: torch.Tensor):
+    def __init__(self, alpha: float, history: int, period: int, inner_weights: torch.Tensor, preconditioner=None):
         if history < 2:
-            raise ValueError("Pulay mixing needs a history of at least 2")
+            raise ValueError("a Pulay history holds at least 2 pairs")
+        if period < 1:
+            raise ValueError("the Pulay period is at least 1")
         self.alpha, self.history, self.period = alpha, history, period
         self.inner_weights = inner_weights
+        self.preconditioner = preconditioner
         self._inputs, self._residuals = [], []
-        self.name = (f"periodic_pulay(alpha={alpha:g}, history={history}, period={period})" if period > 1
-                     else f"pulay(alpha={alpha:g}, history={history})")
+        self.name = (f"DIIS every {period} iterations, alpha {alpha:g}, {history} pairs" if period > 1
+                     else f"DIIS, alpha {alpha:g}, {history} pairs")
         self.last_event = ""
 
     def mix(self, n_in, n_out, iteration):
         residual = n_out - n_in
+        if self.preconditioner is not None:
+            residual = self.preconditioner(residual)
         self._inputs.append(n_in.clone())
         self._residuals.append(residual.clone())
         if len(self._inputs) > self.history:
@@ -352,7 +381,7 @@ class PulayMixer:
             self._residuals.pop(0)
         m = len(self._inputs)
         if m < 2 or iteration % self.period != 0:
-            self.last_event = "linear step"
+            self.last_event = "damped step"
             return n_in + self.alpha * residual
         stack = torch.stack([r.reshape(-1) for r in self._residuals])
         gram = measure_cross(stack, stack, self.inner_weights)[0].cpu().numpy()
@@ -365,7 +394,7 @@ class PulayMixer:
         rhs = np.zeros(m + 1)
         rhs[m] = 1.0
         coefficients = np.linalg.solve(system, rhs)[:m]
-        self.last_event = f"Pulay extrapolation over {m} vectors"
+        self.last_event = f"DIIS combination of {m} pairs"
         mixed = torch.zeros_like(n_in)
         for c, stored_in, stored_res in zip(coefficients, self._inputs, self._residuals):
             mixed = mixed + float(c) * (stored_in + self.alpha * stored_res)
@@ -374,12 +403,14 @@ class PulayMixer:
 
 @dataclass
 class MixingConfig:
-    """``contract.MixingConfig`` (contract.py:452-460)."""
+    """``contract.MixingConfig`` (contract.py:466-474)."""
 
-    scheme: str = "periodic_pulay"  # linear | pulay | periodic_pulay
+    scheme: str = "periodic_pulay"  # linear | anderson | pulay | periodic_pulay | kerker
     alpha: float = 0.30
     history: int = 8
     pulay_period: int = 3
+    kerker: bool = False
+    kerker_q0: float = 1.5
 
 
 @dataclass
@@ -393,12 +424,21 @@ class SCFConfig:
     fallback_ladder: bool = True
 
 
-def make_mixer(cfg: MixingConfig, alpha: float, inner_weights, scheme: str | None = None):
-    scheme = scheme or cfg.scheme
+def make_mixer(cfg: MixingConfig, alpha: float, inner_weights, scheme: str | None = None, grid=None):
+    """The mixer a mixing configuration asks for (``src/cdft/scf/mixing.py:160-177``): ``kerker``
+    as a scheme is periodic Pulay with the Kerker preconditioner; ``kerker=True`` adds the
+    preconditioner to any scheme; ``anderson`` and ``pulay`` are Pulay with period 1."""
+    scheme = str(getattr(scheme or cfg.scheme, "value", scheme or cfg.scheme)).lower()
+    if scheme not in ("linear", "anderson", "pulay", "periodic_pulay", "kerker"):
+        raise ValueError(f"unknown mixing scheme {scheme!r}")
+    kerker = cfg.kerker or scheme == "kerker"
+    if kerker and grid is None:
+        raise ValueError("the Kerker preconditioner needs the grid")
+    pre = KerkerPreconditioner(grid, cfg.kerker_q0) if kerker else None
     if scheme == "linear":
-        return LinearMixer(alpha)
-    period = cfg.pulay_period if scheme == "periodic_pulay" else 1
-    return PulayMixer(alpha, cfg.history, period, inner_weights)
+        return LinearMixer(alpha, pre)
+    period = cfg.pulay_period if scheme in ("periodic_pulay", "kerker") else 1
+    return PulayMixer(alpha, cfg.history, period, inner_weights, pre)
 
 
 class BoundReusePolicy:
@@ -416,22 +456,22 @@ class BoundReusePolicy:
 
     def decide(self, *, residual_rose: bool, rung_changed: bool, level_shift: bool):
         if not self.enabled:
-            return "reuse off"
+            return "carrying bounds is switched off"
         if self.bounds is None:
-            return "no carried interval"
+            return "nothing carried yet"
         if level_shift:
-            return "level-shift rung active"
+            return "the operator is level-shifted"
         if rung_changed:
-            return "fallback rung taken"
+            return "the mixer was just replaced"
         if residual_rose:
-            return "SCF residual rose"
+            return "the density residual grew"
         if self.since_estimate >= LANCZOS_REUSE_BACKSTOP:
-            return f"backstop ({LANCZOS_REUSE_BACKSTOP} iterations)"
+            return f"{LANCZOS_REUSE_BACKSTOP} iterations since the last estimate"
         low, high = self.bounds
         if self.widening > LANCZOS_REUSE_MAX_WIDENING * (high - low):
-            return "accumulated shift"
+            return "the carried interval has widened too far"
         if not self.top_fraction < BOUND_REUSE_RITZ_FRACTION:
-            return "top Ritz fraction near the upper bound"
+            return "the top Ritz value came close to the upper bound"
         return None
 
     def hint(self, shift):
@@ -526,10 +566,10 @@ def solve_self_consistent(step: KohnShamStep, mixing: MixingConfig | None = None
         n_in = initial_density_override.to(device=step.grid.device, dtype=torch.float64).reshape(1, -1).clone()
     else:
         n_in = initial_density(step, initial_guess)
-    mixer = make_mixer(mixing, mixing.alpha, inner_weights)
+    mixer = make_mixer(mixing, mixing.alpha, inner_weights, grid=step.grid)
     ladder = [
-        ("pulay", lambda: make_mixer(mixing, mixing.alpha, inner_weights)),
-        ("damped pulay", lambda: make_mixer(mixing, 0.5 * mixing.alpha, inner_weights)),
+        ("pulay", lambda: make_mixer(mixing, mixing.alpha, inner_weights, grid=step.grid)),
+        ("damped pulay", lambda: make_mixer(mixing, 0.5 * mixing.alpha, inner_weights, grid=step.grid)),
         ("linear", lambda: LinearMixer(0.5 * mixing.alpha)),
         ("linear, level shift 0.5 Ha", lambda: LinearMixer(0.5 * mixing.alpha)),
     ]

@@ -283,6 +283,17 @@ int cdftb_xc_is_gga(int functional);
 int cdftb_xc_eval_f64(int functional, int n_spin, const double* density, const double* sigma, int64_t points,
                       double* e, double* v, double* v_sigma, cdftb_stream_t stream);
 
+/* ---- (s2) density mixing ---- */
+
+/* The Kerker preconditioner (src/cdft/scf/mixing.py:35-56, KerkerPreconditioner.__call__): for each
+ * of `channels` residual rows of the box (nx, ny, nz), out = irfftn(rfftn(F) q^2 / (q^2 + q0^2)),
+ * q from 2 pi fftfreq(n, spacing) per axis, a periodic transform of the box (not zero-padded).
+ * Any edge up to 1024 (direct axis sums, not FFTs). work: device scratch of at least
+ * cdftb_kerker_work_bytes(nx, ny, nz, channels) bytes. residual and out may not overlap. */
+int64_t cdftb_kerker_work_bytes(int nx, int ny, int nz, int channels);
+int cdftb_kerker_precondition_f64(const double* residual, int channels, int nx, int ny, int nz, double spacing,
+                                  double q0, double* out, void* work, int64_t work_bytes, cdftb_stream_t stream);
+
 /* ---- (d4) cusp-aware quadrature interpolant (src/cdft/operators/quadrature.py:506-650) ---- */
 
 /* Stencil corner (m x 3 ints) and the three 8-point Lagrange weight vectors (m x 24) of every point

@@ -202,6 +202,27 @@ def initial_density(step: KohnShamStep):
     return total[None, :].copy()
 
 
+class KerkerPreconditioner:
+    """``F(q) q^2 / (q^2 + q0^2)`` by a periodic FFT of the box (``src/cdft/scf/mixing.py:35-56``)."""
+
+    def __init__(self, shape, spacing: float, q0: float) -> None:
+        self.shape = tuple(int(n) for n in shape)
+        two_pi = 2.0 * math.pi
+        kx = two_pi * np.fft.fftfreq(self.shape[0], d=spacing)
+        ky = two_pi * np.fft.fftfreq(self.shape[1], d=spacing)
+        kz = two_pi * np.fft.rfftfreq(self.shape[2], d=spacing)
+        q2 = kx[:, None, None] ** 2 + ky[None, :, None] ** 2 + kz[None, None, :] ** 2
+        self.filter = q2 / (q2 + q0 * q0)
+
+    def __call__(self, residual):
+        rows = np.atleast_2d(residual)
+        out = np.empty_like(rows)
+        for s, row in enumerate(rows):
+            box = row.reshape(self.shape)
+            out[s] = np.fft.irfftn(np.fft.rfftn(box) * self.filter, s=self.shape).reshape(-1)
+        return out.reshape(np.shape(residual))
+
+
 class LinearMixer:
     """(``src/cdft/scf/mixing.py:59-83``)"""
 

@@ -11,8 +11,9 @@ active set: later launches run on the compacted remainder, so its result is the 
 system alone gives. The host reads a handful of scalars per system once per eigensolver iteration
 and once per SCF iteration, in one transfer for the whole batch.
 
-Spin-restricted LDA; the GGA potentials and the level-shift rung of the fallback ladder run in the
-single-system driver (:mod:`.scf`).
+Spin-restricted, any native functional (the VWN LDA on fused kernels, every other LDA and GGA on the
+generic batched path); the level-shift rung of the fallback ladder runs in the single-system driver
+(:mod:`.scf`).
 """
 
 from __future__ import annotations
@@ -27,7 +28,7 @@ import torch
 from . import _lib
 from ._lib import F32, F64, call, ptr, stream_handle
 from .eigen import BOUND_REUSE_RITZ_FRACTION, EigenConfig, chebyshev_coefficients, filter_workspace
-from .geometry import CuspGeometry, gradient, row_sums
+from .geometry import CuspGeometry, gradient, partial_derivative, row_sums
 from .grid import UniformGrid
 from .operators import apply_workspace, cast, measure_cross, rowwise_inner
 from .poisson import CoulombCutoffPoisson
@@ -473,8 +474,6 @@ class BatchedKohnShamStep:
         self.factor = geometry.factor
         self.quadrature = geometry.quadrature
         self.functional = functional_by_name(functional)
-        if self.functional.rung != 1:
-            raise NotImplementedError("the batched driver runs LDA; use the single-system driver for a GGA")
         self.batch = int(batch)
         self.n_electrons = float(n_electrons)
         self.n_states = max(1, int(-(-self.n_electrons // 2.0)))
@@ -500,6 +499,8 @@ class BatchedKohnShamStep:
         is of earlier densities -- passes them, and the Poisson solve, the interpolation and the
         Hartree half of the lift are skipped (the XC half is not linear and is always lifted).
         """
+        if self.functional.name != "lda_vwn":
+            return self._potentials_generic(density)
         g = self.geometry
         q = self.quadrature
         grid = self.grid
@@ -552,6 +553,86 @@ class BatchedKohnShamStep:
         return BatchedPotentials(effective=effective, v_hartree=v_hartree, hartree_energy=0.5 * sums[:, 0],
                                  xc_energy=node_sum + sums[:, 2], xc_double_counting=sums[:, 1], v_smooth=fields[1],
                                  node=node, lifted_h=lifted[:, 0])
+
+    def _potentials_generic(self, density: torch.Tensor) -> BatchedPotentials:
+        """Potentials for any native functional (``src/cdft/scf/step.py:224-313``) for ``(B, N)``
+        densities: the single-system generic path (``scf.KohnShamStep._potentials_generic``) with a
+        system axis on every array, the functional evaluated on all systems' points in one call and a
+        GGA's gradient term in weak form (lift and FD transpose, step.py:252-280). No linear parts are
+        returned, so the driver solves the Poisson problem of every input density."""
+        g = self.geometry
+        q = self.quadrature
+        grid = self.grid
+        factor = self.factor
+        n = grid.n_points
+        m = q.n_nodes
+        na = len(g.charges)
+        b = density.shape[0]
+        dev = grid.device
+        stream = stream_handle(dev)
+        f = dict(dtype=torch.float64, device=dev)
+        gga = self.functional.rung >= 2
+        f2 = self.f2
+        n_grid = density.to(torch.float64).contiguous()
+        rho = torch.empty((b, n), **f)
+        n_smooth = torch.empty((b, n), **f)
+        call("cdftb_hartree_split_f64", ptr(n_grid), ptr(f2), None, None, 0, n, b, ptr(rho), ptr(n_smooth), stream)
+        rho_nuc = torch.empty((b, na), **f)
+        call("cdftb_quadrature_interpolate_f64", ptr(g.step.nuclei_base), ptr(g.step.nuclei_w1d), na, *grid.shape,
+             ptr(rho), b, n, ptr(rho_nuc), na, stream)
+        coef = torch.empty((b, na), **f)
+        call("cdftb_cusp_coefficients_f64", ptr(rho_nuc), ptr(g.step.nucleus_f2), ptr(g.step.overlap), na, b,
+             ptr(coef), stream)
+        call("cdftb_hartree_split_f64", ptr(n_grid), ptr(f2), ptr(g.step.cusp_grid), ptr(coef), na, n, b, ptr(rho),
+             ptr(n_smooth), stream)
+        v_smooth = self.poisson.solve_batch(n_smooth)
+        v_h_grid = (coef[:, :, None] * g.step.v1s_grid[None]).sum(dim=1) + v_smooth
+        if gga:
+            grad_rho = gradient(grid, rho)  # (B, 3, N)
+            node = q.interpolate(torch.cat([rho[:, None], grad_rho, v_smooth[:, None]], dim=1))  # (B, 5, M)
+            rho_node, grad_rho_node, vs_node = node[:, 0], node[:, 1:4], node[:, 4]
+        else:
+            node = q.interpolate(torch.stack([rho, v_smooth], dim=1))  # (B, 2, M)
+            rho_node, vs_node = node[:, 0], node[:, 1]
+        v_h_node = (coef[:, :, None] * g.step.v1s_node[None]).sum(dim=1) + vs_node
+        n_node = q.f2[None] * rho_node
+        if gga:
+            grad_n_node = q.f2[None, None] * (grad_rho_node - 2.0 * rho_node[:, None] * q.grad_u[None])
+            grad_n_grid = f2[None, None] * (grad_rho - 2.0 * rho[:, None] * factor.grad_u[None])
+            sigma_grid = (grad_n_grid * grad_n_grid).sum(dim=1)
+            sigma_node = (grad_n_node * grad_n_node).sum(dim=1)
+            out_grid = self.functional.evaluate(n_grid.reshape(1, b * n), sigma_grid.reshape(1, b * n))
+            out_node = self.functional.evaluate(n_node.reshape(1, b * m), sigma_node.reshape(1, b * m))
+        else:
+            out_grid = self.functional.evaluate(n_grid.reshape(1, b * n))
+            out_node = self.functional.evaluate(n_node.reshape(1, b * m))
+        e_n_node, e_n_grid = out_node.v_xc.reshape(b, m), out_grid.v_xc.reshape(b, n)
+        parts = [(q.weights[None] * (q.f2[None] * v_h_node))[:, None], (q.weights[None] * (q.f2[None] * e_n_node))[:, None]]
+        if gga:
+            e_s_node, e_s_grid = out_node.v_sigma.reshape(b, m), out_grid.v_sigma.reshape(b, n)
+            flux_node = 2.0 * e_s_node[:, None] * q.f2[None, None] * grad_n_node
+            flux_grid = 2.0 * e_s_grid[:, None] * f2[None, None] * grad_n_grid
+            cross_node = -2.0 * (flux_node * q.grad_u[None]).sum(dim=1)
+            cross_grid = -2.0 * (flux_grid * factor.grad_u[None]).sum(dim=1)
+            parts += [q.weights[None, None] * flux_node, (q.weights[None] * cross_node)[:, None]]
+        lifted = q.lift(torch.cat(parts, dim=1).contiguous())  # (B, 2 or 6, N)
+        hartree_w = lifted[:, 0] + q.far_weights[None] * (f2[None] * v_h_grid)
+        xc_w = lifted[:, 1] + q.far_weights[None] * (f2[None] * e_n_grid)
+        if gga:
+            # lumped_gradient_weights: -sum_d D_d [L^T(w flux_d) + h^3 far flux_grid_d]
+            pre = lifted[:, 2:5] + grid.volume_element * (q.far[None, None] * flux_grid)
+            div = torch.zeros((b, n), **f)
+            for d in range(3):
+                partial_derivative(grid, pre[:, d].contiguous(), d, out=div, accumulate=True, sign=-1.0)
+            xc_w = xc_w + div
+            xc_w = xc_w + (lifted[:, 5] + q.far_weights[None] * cross_grid)
+        hartree_energy = 0.5 * row_sums(hartree_w * rho)
+        xc_energy = row_sums(q.weights[None] * out_node.e_xc.reshape(b, m)) + \
+            row_sums(q.far_weights[None] * out_grid.e_xc.reshape(b, n))
+        xc_dc = row_sums(xc_w * rho)
+        effective = (hartree_w + xc_w) / q.mass_weights[None]
+        return BatchedPotentials(effective=effective, v_hartree=v_h_grid, hartree_energy=hartree_energy,
+                                 xc_energy=xc_energy, xc_double_counting=xc_dc)
 
     def hamiltonian(self, effective: torch.Tensor, dtype=torch.float64) -> BatchedHamiltonian:
         return BatchedHamiltonian(self.grid, self.factor, self.quadrature, self.bare_potential[None, :] + effective,
@@ -762,7 +843,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         n_next = torch.empty_like(nin)
         # a preconditioned residual is not the difference of the two densities' linear parts
         linear = all(isinstance(systems[s].mixer, LinearMixer) and systems[s].mixer.preconditioner is None
-                     for s in active)
+                     for s in active) and p_in.v_smooth is not None
         lin_next = None
         if linear:
             # x_in + alpha (x_out - x_in) per system (LinearMixer.mix, element for element) in one expression per

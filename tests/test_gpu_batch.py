@@ -107,3 +107,48 @@ def test_batched_scan_matches_the_reference(pkg, cuda, golden_values, precision)
             assert res["iterations"] == ref["iterations"]
         else:
             assert abs(res["total"] - ref["total"]) < 1e-9
+
+
+# ------------------------------------------------------------------ GGA and the other functionals in the batch
+
+
+def test_batched_pbe_h2(pkg, cuda, golden_values):
+    """H2 PBE (h = 0.4, box 10 x 10 x 11.2, default periodic Pulay, degree 16): two systems of the
+    batched driver each give the reference's energy and iteration count."""
+    system = oscf.h2_pbe(spacing=0.4, box=(10.0, 10.0, 11.2))
+    grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=cuda)
+    geo = pkg.build_cusp_geometry(grid, system.charges, system.positions)
+    step = pkg.batch.BatchedKohnShamStep(geo, "pbe", 2.0, 2, pkg.EigenConfig(chebyshev_degree=16), seeds=[0, 0])
+    out = pkg.batch.solve_self_consistent_batch(step, pkg.MixingConfig())
+    ref = golden_values["h2_pbe_h04"]
+    for s in range(2):
+        assert out.converged[s]
+        assert out.scf_iterations[s] == ref["iterations"]
+        assert abs(out.energies[s]["total"] - ref["total"]) < 1e-10
+
+
+def test_config3_batched_mixed(pkg, cuda, golden_values):
+    """Config 3 (H2 PBE, 81 x 81 x 91, degree 16) batched in the mixed form: float32 filter, float64
+    Rayleigh--Ritz and refinement; within 1e-8 Ha of the reference's float64 energy."""
+    system = oscf.h2_pbe()
+    grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=cuda)
+    geo = pkg.build_cusp_geometry(grid, system.charges, system.positions)
+    step = pkg.batch.BatchedKohnShamStep(geo, "pbe", 2.0, 2, pkg.EigenConfig(chebyshev_degree=16), seeds=[0, 3],
+                                         filter_precision=torch.float32)
+    out = pkg.batch.solve_self_consistent_batch(step, pkg.MixingConfig())
+    ref = golden_values["h2_pbe_h020"]["total"]
+    assert all(out.converged)
+    for e in out.energies:
+        assert abs(e["total"] - ref) < 1e-8
+
+
+def test_batched_blyp_he25(pkg, he25_geometry):
+    """A non-VWN functional in the batch (the generic path) equals the single-system solve."""
+    mixing = pkg.MixingConfig(scheme="linear", alpha=0.3)
+    single = pkg.solve_self_consistent(pkg.KohnShamStep(he25_geometry, "blyp", 2.0), mixing)
+    step = pkg.batch.BatchedKohnShamStep(he25_geometry, "blyp", 2.0, 2, seeds=[0, 0])
+    out = pkg.batch.solve_self_consistent_batch(step, mixing)
+    for s in range(2):
+        assert out.converged[s]
+        assert out.scf_iterations[s] == single.scf_iterations
+        assert abs(out.energies[s]["total"] - single.energies["total"]) < 1e-11

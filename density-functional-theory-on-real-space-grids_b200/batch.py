@@ -117,6 +117,64 @@ class BatchedHamiltonian:
         return sub
 
 
+class LevelShiftedBatch:
+    """``H + shift (1 - P_occ)`` for every system of a batch (``src/cdft/scf/loop.py:553-589``, the
+    fallback ladder's last rung): ``P_occ`` projects, in the measure, onto each system's occupied
+    orbitals of the previous iteration. Applies as ``H phi + shift (phi - (phi, o) o)``; the filter is
+    the reference's eager scaled recurrence over that apply (one apply launch per step, float64);
+    Lanczos bounds are the inner operator's with the upper bound raised by ``shift``."""
+
+    def __init__(self, inner: BatchedHamiltonian, occupied: torch.Tensor, shift: float) -> None:
+        self.inner = inner
+        self.occupied = occupied.to(torch.float64).contiguous()  # (B, k_occ, N)
+        self.shift = float(shift)
+        self.grid = inner.grid
+        self.q = inner.q
+        self.potentials = inner.potentials
+        self.dtype = torch.float64
+        self.applications = 0
+
+    @property
+    def batch(self) -> int:
+        return self.inner.batch
+
+    def apply(self, phi: torch.Tensor, kinetic_only: bool = False) -> torch.Tensor:
+        if kinetic_only:
+            return self.inner.apply(phi, kinetic_only=True)
+        x = phi.to(torch.float64).contiguous()
+        out = self.inner.apply(x)
+        coefficients = measure_cross(x, self.occupied, self.q, x.shape[0])  # (B, k, k_occ)
+        self.applications += 1
+        return out + self.shift * (x - torch.bmm(coefficients, self.occupied))
+
+    def filter(self, block: torch.Tensor, table: torch.Tensor, degree: int) -> torch.Tensor:
+        """``chefsi.py:81-113`` per system with that system's rows ``(c, a_k, b_k)`` of ``table``."""
+        rows = table.to(torch.float64)
+        c = rows[:, :, 0][:, :, None, None]
+        a = rows[:, :, 1][:, :, None, None]
+        bk = rows[:, :, 2][:, :, None, None]
+        x = block.to(torch.float64)
+        y = (self.apply(x) - c[:, 0] * x) * a[:, 0]
+        previous = x
+        for k in range(1, degree):
+            y_new = (self.apply(y) - c[:, k] * y) * a[:, k] - bk[:, k] * previous
+            previous, y = y, y_new
+        return y
+
+    def subset(self, index: list[int]) -> "LevelShiftedBatch":
+        idx = torch.tensor(index, dtype=torch.long, device=self.occupied.device)
+        return LevelShiftedBatch(self.inner.subset(index), self.occupied.index_select(0, idx), self.shift)
+
+
+def _enclosures(sub, starts: torch.Tensor, config: EigenConfig):
+    """Lanczos bounds for every system of ``sub`` (a level-shifted batch: its inner operator's, with
+    the upper bound raised by the shift, as ``_LevelShifted.spectral_bounds``)."""
+    if isinstance(sub, LevelShiftedBatch):
+        return [(lo, hi + sub.shift) for lo, hi in batched_lanczos(sub.inner, starts, config.lanczos_steps,
+                                                                   config.bound_safety)]
+    return batched_lanczos(sub, starts, config.lanczos_steps, config.bound_safety)
+
+
 class _RitzBuffers:
     def __init__(self):
         self._key = None
@@ -314,7 +372,7 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
     if need:
         starts = torch.stack([streams[s].randn(n) for s in need])
         sub = h if len(need) == b else h.subset(need)
-        for s, bb in zip(need, batched_lanczos(sub, starts, config.lanczos_steps, config.bound_safety)):
+        for s, bb in zip(need, _enclosures(sub, starts, config)):
             states[s].spectrum = bb
             states[s].source = "lanczos"
             states[s].applications += config.lanczos_steps
@@ -351,7 +409,7 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
         if redo:
             starts = torch.stack([streams[s].randn(n) for s in redo])
             sub = h.subset(redo)
-            for s, bb in zip(redo, batched_lanczos(sub, starts, config.lanczos_steps, config.bound_safety)):
+            for s, bb in zip(redo, _enclosures(sub, starts, config)):
                 states[s].spectrum = bb
                 states[s].source = "lanczos (reuse rejected)"
                 states[s].applications += config.lanczos_steps
@@ -741,6 +799,7 @@ class _SystemState:
     refinement_from: int | None = None
     rung_changed: bool = False
     fallback_events: list = field(default_factory=list)
+    level_shift: float = 0.0
 
 
 @dataclass
@@ -809,7 +868,8 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
             shifts = (p_in.effective - prev).abs().amax(dim=1).tolist()
         for j, s in enumerate(active):
             st = systems[s]
-            reason = st.policy.decide(residual_rose=st.worsened > 0, rung_changed=st.rung_changed, level_shift=False)
+            reason = st.policy.decide(residual_rose=st.worsened > 0, rung_changed=st.rung_changed,
+                                      level_shift=bool(st.level_shift))
             if reason is None and shifts is not None:
                 hints.append((st.policy.bounds[0], st.policy.bounds[1], shifts[j]))
             else:
@@ -823,8 +883,38 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
         # The first full diagonalisation of a mixed solve stops at the float switch: the float phase
         # that follows holds float accuracy anyway, and the float64 refinement sweep and the final
         # float64 diagonalisation set the result's.
-        evals, vectors, _, estates = batched_chefsi(h, h32, step.n_states, step.eigen, init, streams, hints, steps_cap,
-                                                    switch, float_mask=float_now, stop_at_switch=mixed)
+        shifted = [j for j, s in enumerate(active) if systems[s].level_shift]
+        if not shifted:
+            evals, vectors, _, estates = batched_chefsi(h, h32, step.n_states, step.eigen, init, streams, hints,
+                                                        steps_cap, switch, float_mask=float_now, stop_at_switch=mixed)
+        else:
+            # systems on the level-shift rung diagonalise H + shift (1 - P_occ), in float64, in a call of
+            # their own (loop.py:353-356: the filter then runs eagerly over the shifted apply)
+            plain = [j for j in range(len(active)) if j not in shifted]
+            n_occ = int((step.occ > 1e-12).sum())
+            evals = torch.empty((len(active), step.n_states), dtype=torch.float64, device=dev)
+            vectors = torch.empty((len(active), step.n_states, n), dtype=torch.float64, device=dev)
+            estates = [None] * len(active)
+            for part, is_shifted in ((plain, False), (shifted, True)):
+                if not part:
+                    continue
+                hp = h.subset(part)
+                sub_init = init.index_select(0, torch.tensor(part, dtype=torch.long, device=dev))
+                if is_shifted:
+                    hp = LevelShiftedBatch(hp, sub_init[:, :n_occ], systems[active[part[0]]].level_shift)
+                    hf, fmask = None, None
+                else:
+                    hf = None if h32 is None else h32.subset(part)
+                    fmask = [float_now[j] for j in part]
+                ev_p, vec_p, _, es_p = batched_chefsi(hp, hf, step.n_states, step.eigen, sub_init,
+                                                      [streams[j] for j in part], [hints[j] for j in part],
+                                                      steps_cap, switch if not is_shifted else None, float_mask=fmask,
+                                                      stop_at_switch=mixed and not is_shifted)
+                idx = torch.tensor(part, dtype=torch.long, device=dev)
+                evals.index_copy_(0, idx, ev_p)
+                vectors.index_copy_(0, idx, vec_p)
+                for j, es in zip(part, es_p):
+                    estates[j] = es
         for j, s in enumerate(active):
             st = systems[s]
             es = estates[j]
@@ -882,8 +972,7 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
             if scf.fallback_ladder and st.worsened >= 3 and st.rung + 1 < 4:
                 st.rung += 1
                 if st.rung == 3:
-                    raise RuntimeError("the level-shift rung is not batched; solve this system with the "
-                                       "single-system driver")
+                    st.level_shift = 0.5  # loop.py:320: the last rung shifts the unoccupied states by 0.5 Ha
                 st.mixer = make(0.5 * mixing.alpha) if st.rung == 1 else LinearMixer(0.5 * mixing.alpha)
                 st.fallback_events.append(f"iteration {iteration}: stepping down to rung {st.rung}")
                 st.worsened = 0

@@ -152,3 +152,27 @@ def test_batched_blyp_he25(pkg, he25_geometry):
         assert out.converged[s]
         assert out.scf_iterations[s] == single.scf_iterations
         assert abs(out.energies[s]["total"] - single.energies["total"]) < 1e-11
+
+
+def test_level_shifted_batch_matches_the_single_system_rung(pkg, he25_geometry):
+    """The ladder's last rung in the batch: CheFSI on H + 0.5 (1 - P_occ) for two systems gives the
+    single-system driver's level-shifted diagonalisation (``loop.py:553-589``)."""
+    step = pkg.KohnShamStep(he25_geometry, "lda_vwn", 2.0)
+    p = step.potentials(pkg.initial_density(step))
+    eigen0, _ = step.diagonalise(step.hamiltonian(p))
+    occ = step.occupy(eigen0.eigenvalues)
+    shifted = pkg.scf._LevelShifted(step.hamiltonian(p), eigen0, occ, 0.5)
+    single, info = step.diagonalise(shifted, initial=eigen0.eigenvectors, max_iterations=4)
+
+    bstep = pkg.batch.BatchedKohnShamStep(he25_geometry, "lda_vwn", 2.0, 2, seeds=[0, 0])
+    bh = bstep.hamiltonian(p.effective[None].expand(2, -1).contiguous())
+    init = eigen0.eigenvectors[None].expand(2, -1, -1).contiguous()
+    op = pkg.batch.LevelShiftedBatch(bh, init[:, :1], 0.5)
+    streams = [pkg.rng.SeededStream(0, he25_geometry.grid.device) for _ in range(2)]
+    evals, vectors, _, states = pkg.batch.batched_chefsi(op, None, step.n_states, step.eigen, init, streams,
+                                                         [None, None], 4, None)
+    want = single.eigenvalues.cpu()
+    for s in range(2):
+        assert states[s].iterations == single.n_iterations
+        torch.testing.assert_close(evals[s].cpu(), want, rtol=0, atol=1e-10)
+        assert abs(states[s].spectrum[1] - info["eigen_spectral_bounds"][1]) < 1e-9

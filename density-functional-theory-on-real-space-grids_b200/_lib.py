@@ -91,6 +91,8 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_kerker_work_bytes": (c_int64, [c_int, c_int, c_int, c_int]),
     "cdftb_kerker_precondition_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_double, c_void_p,
                                               c_void_p, c_int64, c_void_p]),
+    "cdftb_reciprocal_filter_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_int, c_double, c_void_p,
+                                            c_void_p, c_int64, c_void_p]),
     "cdftb_xc_eval_f64": (c_int, [c_int, c_int, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "cdftb_quadrature_stencils": (c_int, [c_void_p, c_int64, c_int, c_int, c_int, c_double, c_double, c_double, c_double,
                                           c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -354,3 +354,185 @@ class ChebyshevFilteredSubspace:
         self.top_ritz_fraction = top_fraction
         _lib.check_device_status("ChebyshevFilteredSubspace.solve")
         return EigenResult(evals[:n_states], vectors[:n_states], residual[:n_states], iteration, converged)
+
+
+# ---------------------------------------------------------------------------------------------
+# LOBPCG: the eigensolver cross-check on the native apply
+
+
+def _combine(matrix: np.ndarray, block: torch.Tensor) -> torch.Tensor:
+    """``matrix @ block`` for a small host matrix ``(a, b)`` and a device block ``(b, N)``, one
+    ``cdftb_block_rotate_f64`` launch."""
+    mat = np.ascontiguousarray(np.asarray(matrix, dtype=np.float64))
+    a, b = mat.shape
+    x = block.to(torch.float64).contiguous()
+    n = x.shape[-1]
+    out = torch.empty((a, n), dtype=torch.float64, device=x.device)
+    if a == 0:
+        return out
+    r = torch.from_numpy(mat).to(x.device, non_blocking=True)
+    call("cdftb_block_rotate_f64", ptr(r), ptr(x), 0, ptr(out), F64, 0, a, b, n, 1, stream_handle(x.device))
+    return out
+
+
+def _symmetrise(m: np.ndarray) -> np.ndarray:
+    return 0.5 * (m + m.T)
+
+
+def _stable_basis(block: torch.Tensor, measure: Measure, threshold: float = 1e-12):
+    """An orthonormal basis of ``block`` with near-dependent directions dropped, and how many were
+    dropped (``src/cdft/eigen/lobpcg.py:253-271``)."""
+    if block.shape[0] == 0:
+        return block, 0
+    g = measure.gram(block).cpu().numpy()
+    evals, evecs = np.linalg.eigh(_symmetrise(g))
+    keep = evals > evals[-1] * threshold
+    if evals[-1] <= 0.0:
+        return block[:0], block.shape[0]
+    scaled = evecs[:, keep] / np.sqrt(evals[keep])
+    return _combine(scaled.T, block), int((~keep).sum())
+
+
+def _lobpcg_orthonormalise(block: torch.Tensor, measure: Measure) -> torch.Tensor:
+    """Cholesky in the measure, the stable basis on failure (``lobpcg.py:221-229``): ``L^-1 block``
+    by the native forward substitution."""
+    g = measure.gram(block).cpu().numpy()
+    try:
+        chol = np.linalg.cholesky(g)
+    except np.linalg.LinAlgError:
+        return _stable_basis(block, measure)[0]
+    x = block.to(torch.float64).contiguous()
+    m, n = x.shape
+    lower = torch.from_numpy(np.ascontiguousarray(chol)).to(x.device)
+    out = torch.empty_like(x)
+    call("cdftb_block_trsm_lower_f64", ptr(lower), ptr(x), m * n, ptr(out), F64, m * n, m, n, 1,
+         stream_handle(x.device))
+    return out
+
+
+def _orthogonalise_against(block: torch.Tensor, basis: torch.Tensor, measure: Measure) -> torch.Tensor:
+    """Project ``basis`` out of ``block`` twice, then orthonormalise the rest (``lobpcg.py:232-242``)."""
+    for _ in range(2):
+        block = block - _combine(measure.cross(block, basis).cpu().numpy(), basis)
+    return _stable_basis(block, measure)[0]
+
+
+class LOBPCG:
+    """Locally optimal block preconditioned conjugate gradient (``src/cdft/eigen/lobpcg.py:44-207``),
+    the reference's permanent cross-check of the Chebyshev eigensolver (gate G2.5), on the native
+    apply and measure products.
+
+    The residual is preconditioned in the similarity frame by default: mapped to the wavefunction
+    frame (``r_psi = f r_phi``), filtered with the Teter--Payne--Allan kinetic preconditioner by a
+    periodic transform of the box (``cdftb_reciprocal_filter_f64``, kind 1), and mapped back. The
+    small projected problems (at most three blocks of states) are solved on the host, one read per
+    iteration, as in the reference.
+    """
+
+    FRAMES = ("similarity", "transformed", "none")
+
+    def __init__(self, grid, config: EigenConfig, precondition: bool | str = True) -> None:
+        if precondition is True:
+            precondition = "similarity"
+        elif precondition is False:
+            precondition = "none"
+        if precondition not in self.FRAMES:
+            raise ValueError(f"unknown preconditioner frame {precondition!r}; one of {self.FRAMES}")
+        self.grid = grid
+        self.config = config
+        self.frame = precondition
+        self.history: list[dict] = []
+        self.eigenvalue_tol = 0.1 * config.cross_check_tol
+        self.eigenvalue_drift = float("inf")
+        self._reference_energy = None
+
+    def _kinetic_reference(self) -> float:
+        """The grid's mean kinetic scale: the mean of G^2/2 over the half-spectrum box."""
+        if self._reference_energy is None:
+            import math
+
+            h = self.grid.spacing
+            nx, ny, nz = self.grid.shape
+            kx = 2.0 * math.pi * np.fft.fftfreq(nx, d=h)
+            ky = 2.0 * math.pi * np.fft.fftfreq(ny, d=h)
+            kz = 2.0 * math.pi * np.fft.rfftfreq(nz, d=h)
+            g2 = 0.5 * (kx[:, None, None] ** 2 + ky[None, :, None] ** 2 + kz[None, None, :] ** 2)
+            self._reference_energy = max(float(g2.mean()), 1.0e-6)
+        return self._reference_energy
+
+    def _precondition(self, block: torch.Tensor) -> torch.Tensor:
+        x = block.to(torch.float64).contiguous()
+        rows = x.shape[0]
+        nbytes = _lib.library().cdftb_kerker_work_bytes(*self.grid.shape, rows)
+        work = torch.empty(nbytes, dtype=torch.uint8, device=x.device)
+        out = torch.empty_like(x)
+        call("cdftb_reciprocal_filter_f64", ptr(x), rows, *self.grid.shape, self.grid.spacing, 1,
+             self._kinetic_reference(), ptr(out), ptr(work), nbytes, stream_handle(x.device))
+        return out
+
+    def solve(self, hamiltonian, n_states: int, initial: torch.Tensor | None = None, generator=None) -> EigenResult:
+        grid = self.grid
+        cfg = self.config
+        measure = hamiltonian.measure
+        factor = getattr(hamiltonian, "factor", None)
+        f = None
+        if factor is not None and not getattr(factor, "is_identity", True):
+            f = torch.exp(-factor.u).clamp_min(1.0e-150)
+        if initial is None:
+            x = seeded_randn((n_states, grid.n_points), generator, device=grid.device)
+        else:
+            x = initial.to(torch.float64).reshape(-1, grid.n_points)[:n_states].clone()
+        x = _lobpcg_orthonormalise(x, measure)
+        hx = hamiltonian.apply(x)
+        evals_h, rotation = np.linalg.eigh(_symmetrise(measure.cross(x, hx).cpu().numpy()))
+        x = _combine(rotation.T, x)
+        hx = _combine(rotation.T, hx)
+        evals = torch.from_numpy(evals_h).to(grid.device)
+        p = None
+        converged = False
+        iteration = 0
+        residual = None
+        previous = evals_h.copy()
+        stable = 0
+        self.eigenvalue_drift = float("inf")
+        for iteration in range(1, cfg.max_iterations + 1):
+            r = hx - evals[:, None] * x
+            residual = measure.norm(r)
+            res_h = residual.cpu().numpy()
+            _lib.check_device_status(f"LOBPCG iteration {iteration}")
+            keep = res_h > 0.1 * cfg.residual_tol
+            worst = float(res_h.max())
+            drift = float(np.abs(evals_h - previous).max()) if iteration > 1 else float("inf")
+            previous = evals_h.copy()
+            self.eigenvalue_drift = drift
+            self.history.append({"iteration": float(iteration), "residual": worst, "eigenvalue_drift": drift})
+            if worst < cfg.residual_tol:
+                converged = True
+                break
+            stable = stable + 1 if drift < self.eigenvalue_tol else 0
+            if stable >= 2:
+                converged = True
+                break
+            w = r[torch.from_numpy(keep).to(r.device)] if keep.any() else r
+            if self.frame == "similarity" and f is not None:
+                w = self._precondition(w * f) / f
+            elif self.frame != "none":
+                w = self._precondition(w)
+            w = _orthogonalise_against(w, x, measure)
+            if w.shape[0] == 0:
+                converged = True
+                break
+            blocks = [x, w] if p is None else [x, w, p]
+            basis, dropped = _stable_basis(torch.cat(blocks, dim=0), measure)
+            h_basis = hamiltonian.apply(basis)
+            sub_evals, sub_vectors = np.linalg.eigh(_symmetrise(measure.cross(basis, h_basis).cpu().numpy()))
+            coeff = sub_vectors[:, :n_states]
+            x_new = _combine(coeff.T, basis)
+            hx_new = _combine(coeff.T, h_basis)
+            p = x_new - _combine(measure.cross(x_new, x).cpu().numpy(), x)
+            x, hx = x_new, hx_new
+            evals_h = sub_evals[:n_states]
+            evals = torch.from_numpy(np.ascontiguousarray(evals_h)).to(grid.device)
+            if dropped:
+                self.history[-1]["dropped_directions"] = float(dropped)
+        return EigenResult(evals[:n_states], x[:n_states], residual[:n_states], iteration, converged)

@@ -683,8 +683,22 @@ def solve_self_consistent(step: KohnShamStep, mixing: MixingConfig | None = None
                       energy_history=energies, residual_history=residuals, density=n_out, measurements=measurements)
 
 
+def lobpcg_cross_check(hamiltonian, eigenvalues: torch.Tensor, n_states: int, eigen: EigenConfig, seed: int) -> dict:
+    """The two-solver check of gate G2.5 (``src/cdft/scf/noninteracting.py:182-189``): LOBPCG on the
+    same operator from a start seeded with ``seed + 1``, against the Chebyshev eigenvalues."""
+    from .eigen import LOBPCG
+
+    grid = hamiltonian.grid
+    second = LOBPCG(grid, eigen).solve(hamiltonian, n_states, generator=SeededStream(seed + 1, grid.device))
+    delta = (eigenvalues.to(torch.float64) - second.eigenvalues).abs()
+    return {"two_solver_max_delta": float(delta.max()), "two_solver_converged": bool(second.converged),
+            "lobpcg_iterations": float(second.n_iterations),
+            "lobpcg_eigenvalues": second.eigenvalues.tolist()}
+
+
 def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: int = 0,
-                         eigen: EigenConfig | None = None, external_potential: torch.Tensor | None = None) -> dict:
+                         eigen: EigenConfig | None = None, external_potential: torch.Tensor | None = None,
+                         cross_check: bool = False) -> dict:
     """(``src/cdft/scf/noninteracting.py:118-330``) for the cusp-factorised path, ``ritz_stop=True``.
 
     ``external_potential`` adds a diagonal term to the operator (an external perturbation in the
@@ -705,6 +719,9 @@ def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: in
     kinetic, band = vals[0], vals[1]
     ion_ion = nuclear_repulsion(geometry.charges, geometry.positions)
     external = band - kinetic
-    return {"total": kinetic + external + ion_ion, "kinetic": kinetic, "eigenvalues": vals[2:],
-            "iterations": result.n_iterations, "converged": result.converged, "applications": float(ham.apply_count),
-            "stop_reason": solver.stop_reason, "orbitals": result.eigenvectors, "occupations": occ[0]}
+    out = {"total": kinetic + external + ion_ion, "kinetic": kinetic, "eigenvalues": vals[2:],
+           "iterations": result.n_iterations, "converged": result.converged, "applications": float(ham.apply_count),
+           "stop_reason": solver.stop_reason, "orbitals": result.eigenvectors, "occupations": occ[0]}
+    if cross_check:
+        out.update(lobpcg_cross_check(ham, result.eigenvalues, n_states, eigen or EigenConfig(), seed))
+    return out

@@ -294,6 +294,13 @@ int64_t cdftb_kerker_work_bytes(int nx, int ny, int nz, int channels);
 int cdftb_kerker_precondition_f64(const double* residual, int channels, int nx, int ny, int nz, double spacing,
                                   double q0, double* out, void* work, int64_t work_bytes, cdftb_stream_t stream);
 
+/* The same periodic box transform with a filter chosen by `kind`: 0 the Kerker filter above
+ * (param = q0), 1 the Teter--Payne--Allan kinetic preconditioner of LOBPCG
+ * (src/cdft/eigen/lobpcg.py:160-189, LOBPCG._apply_preconditioner): P(x) / (P(x) + 16 x^4),
+ * P = 27 + 18 x + 12 x^2 + 8 x^3, x = (q^2 / 2) / E_ref with param = E_ref > 0. Same work size. */
+int cdftb_reciprocal_filter_f64(const double* field, int channels, int nx, int ny, int nz, double spacing, int kind,
+                                double param, double* out, void* work, int64_t work_bytes, cdftb_stream_t stream);
+
 /* ---- (d4) cusp-aware quadrature interpolant (src/cdft/operators/quadrature.py:506-650) ---- */
 
 /* Stencil corner (m x 3 ints) and the three 8-point Lagrange weight vectors (m x 24) of every point

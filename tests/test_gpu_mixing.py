@@ -73,3 +73,35 @@ def test_batched_scf_with_kerker(pkg, he25, scf_golden):
         assert out.converged[s]
         assert out.scf_iterations[s] == int(scf_golden["scf_linear_kerker_iterations"])
         assert abs(out.energies[s]["total"] - want) < 1e-10
+
+
+# ------------------------------------------------------------------ LOBPCG, the eigensolver cross-check
+
+
+@pytest.fixture(scope="module")
+def h17(pkg, cuda):
+    system = oscf.h_atom(points_per_edge=17, half_box=4.0)
+    grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=cuda)
+    return pkg.build_cusp_geometry(grid, system.charges, system.positions)
+
+
+@pytest.mark.parametrize("k", [1, 2])
+def test_lobpcg_matches_the_reference(pkg, h17, scf_golden, k):
+    """The bare H atom (box 8, h = 0.5): the reference's LOBPCG eigenvalues, started from the same
+    seeded block, in about the same number of iterations."""
+    ham = pkg.CuspFactoredHamiltonian(h17.grid, h17.factor, quadrature=h17.quadrature)
+    solver = pkg.eigen.LOBPCG(h17.grid, pkg.EigenConfig())
+    out = solver.solve(ham, k, generator=pkg.rng.SeededStream(1, h17.grid.device))
+    want = scf_golden[f"lobpcg_{k}_eigenvalues"]
+    assert out.converged == bool(scf_golden[f"lobpcg_{k}_converged"])
+    np.testing.assert_allclose(out.eigenvalues.cpu().numpy(), want, rtol=0, atol=1e-9)
+    assert abs(out.n_iterations - int(scf_golden[f"lobpcg_{k}_iterations"])) <= 2
+
+
+def test_two_solver_cross_check(pkg, h17, scf_golden):
+    """``solve_noninteracting(cross_check=True)``: CheFSI and LOBPCG agree to the G2.5 tolerance."""
+    out = pkg.solve_noninteracting(h17, 1.0, cross_check=True)
+    assert out["two_solver_converged"]
+    assert out["two_solver_max_delta"] < 1e-8
+    np.testing.assert_allclose(out["eigenvalues"], scf_golden["cross_eigenvalue"], rtol=0, atol=1e-11)
+    assert abs(out["lobpcg_iterations"] - float(scf_golden["cross_lobpcg_iterations"])) <= 2

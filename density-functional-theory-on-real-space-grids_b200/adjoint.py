@@ -20,8 +20,12 @@ the expectation value Q[n g_k] through the cusp-aware quadrature (Hellmann--Feyn
   quadrature the discrete Hartree potential (analytic cusp part plus grid Poisson, lifted to the
   nodes) is not the exact derivative of the discrete Hartree energy, so a first-order term remains:
   0.3% of the gradient for He at h = 0.5.
-The derivative with respect to a nuclear position is taken by central differences of total
-energies on a fixed (unanchored) grid.
+The derivative with respect to a nuclear position (``nuclear_gradient_variational``) follows from
+the stationarity of the Kohn--Sham Lagrangian at the converged orbitals (Hellmann--Feynman plus the
+Pulay terms of the cusp factor, face weights, quadrature and measure that move with the nucleus):
+no orbital response, no re-solve; the explicit geometry derivative is a central difference of the
+device geometry build at fixed orbitals. ``nuclear_gradient`` (central differences of converged
+total energies on a fixed, unanchored grid) is the check.
 """
 
 from __future__ import annotations
@@ -174,4 +178,70 @@ def nuclear_gradient(energy_at, positions, delta: float = 1.0e-4) -> np.ndarray:
             plus[a, d] += delta
             minus[a, d] -= delta
             grad[a, d] = (energy_at(plus) - energy_at(minus)) / (2.0 * delta)
+    return grad
+
+
+# ------------------------------------------------------------------------ nuclear gradient
+
+
+def fixed_orbital_energy(geometry, orbitals: torch.Tensor, occupations: torch.Tensor, eigenvalues: torch.Tensor,
+                         functional: str | None = None, n_electrons: float | None = None) -> float:
+    """The Kohn--Sham Lagrangian at fixed transformed orbitals ``phi`` on ``geometry``:
+
+        L = sum_i f_i <phi_i, A_bare phi_i>_q + E_H[n] + E_xc[n] + E_ion - sum_i f_i eps_i (<phi_i, phi_i>_q - 1)
+
+    with ``n = f^2 sum_i f_i phi_i^2`` and every geometric quantity (face weights, ``h^3/omega``,
+    ``W~/omega``, the measure ``q``, the cusp factor, the quadrature) that of ``geometry``. At the
+    geometry the orbitals were solved on, L is the total energy (``band - double counting + E_H +
+    E_xc + E_ion``, ``src/cdft/scf/step.py:398-439``); ``functional=None`` is the bare-nucleus energy
+    (band + E_ion, ``src/cdft/scf/noninteracting.py``).
+    """
+    from .operators import CuspFactoredHamiltonian
+    from .scf import KohnShamStep, nuclear_repulsion
+
+    phi = orbitals.to(torch.float64).reshape(-1, geometry.grid.n_points)
+    occ = occupations.to(torch.float64).reshape(-1)
+    eps = eigenvalues.to(torch.float64).reshape(-1)
+    ham = CuspFactoredHamiltonian(geometry.grid, geometry.factor, quadrature=geometry.quadrature)
+    q = ham.measure.quadrature
+    a_phi = ham.apply(phi)
+    form = (q[None] * phi * a_phi).sum(dim=1)
+    norm = (q[None] * phi * phi).sum(dim=1)
+    value = (occ * (form - eps * (norm - 1.0))).sum()
+    total = float(value) + nuclear_repulsion(geometry.charges, geometry.positions)
+    if functional is not None:
+        rho = (occ[:, None] * phi * phi).sum(dim=0)
+        n_grid = (rho * geometry.factor.weight)[None]
+        step = KohnShamStep(geometry, functional, float(n_electrons if n_electrons is not None else occ.sum()))
+        p = step.potentials(n_grid)
+        total += float(p.hartree_energy) + float(p.xc_energy)
+    return total
+
+
+def nuclear_gradient_variational(build, positions, orbitals: torch.Tensor, occupations: torch.Tensor,
+                                 eigenvalues: torch.Tensor, functional: str | None = None,
+                                 n_electrons: float | None = None, delta: float = 1.0e-4) -> np.ndarray:
+    """``dE/dR_a`` from the stationarity of the Kohn--Sham Lagrangian (Hellmann--Feynman with the
+    Pulay terms of the moving cusp factor, quadrature and measure): ``dE/dR = dL/dR`` at the
+    converged orbitals, so no orbital response and no re-solve. The explicit geometry derivative of
+    :func:`fixed_orbital_energy` is taken by central differences of the device geometry build
+    (``build(positions) -> CuspGeometry``, 6 builds per nucleus), at fixed orbitals, multipliers and
+    grid (the grid is not re-anchored to the moved nuclei).
+
+    Exact for a bare-nucleus problem (the eigenvalue derivative of an operator self-adjoint in the
+    measure). For the self-consistent energy it carries the first-order error of the discrete
+    Hartree potential's non-stationarity noted in the module docstring, which vanishes as the grid
+    refines.
+    """
+    base = np.asarray(positions, dtype=float)
+    grad = np.zeros_like(base)
+    for a in range(base.shape[0]):
+        for d in range(3):
+            values = []
+            for sign in (+1.0, -1.0):
+                moved = base.copy()
+                moved[a, d] += sign * delta
+                geo = build([tuple(p) for p in moved])
+                values.append(fixed_orbital_energy(geo, orbitals, occupations, eigenvalues, functional, n_electrons))
+            grad[a, d] = (values[0] - values[1]) / (2.0 * delta)
     return grad

@@ -203,3 +203,70 @@ def test_config5_external_gradient_101(pkg, cuda):
              for sign in (+1, -1)]
         fd = (e[0] - e[1]) / (2 * step)
         assert abs(fd - grad[k]) <= 1e-6 * abs(grad[k]), (int(k), fd, grad[k])
+
+
+def _scan_system(bond, spacing=0.4):
+    system = oscf.h2_plus(bond, spacing=spacing, transverse=10.0)
+    system.box_lengths = (10.0, 10.0, 12.6)  # one fixed grid for every displacement
+    return system
+
+
+def test_variational_nuclear_gradient_bare_h2plus(pkg, cuda):
+    """dE/dR_a of H2+ (R = 2.6, h = 0.4) from the stationarity of the Lagrangian at the converged
+    orbital (no re-solve) against central differences of converged energies (step 1e-4), to 1e-6
+    relative; the transverse components vanish by symmetry."""
+    system = _scan_system(2.6)
+    eigen = pkg.EigenConfig(residual_tol=1e-12)
+    geo = _geometry(pkg, system, cuda)
+    out = pkg.solve_noninteracting(geo, n_electrons=1.0, eigen=eigen)
+    assert out["converged"]
+    grid = geo.grid
+
+    def build(positions):
+        return pkg.build_cusp_geometry(grid, system.charges, positions)
+
+    grad = pkg.adjoint.nuclear_gradient_variational(build, system.positions, out["orbitals"], out["occupations"],
+                                                    torch.tensor(out["eigenvalues"][:1], dtype=torch.float64))
+
+    def energy_at(positions):
+        res = pkg.solve_noninteracting(build([tuple(p) for p in positions]), n_electrons=1.0, eigen=eigen)
+        return float(res["total"])
+
+    fd = pkg.adjoint.nuclear_gradient(energy_at, system.positions, delta=1e-4)
+    assert abs(grad[1, 2]) > 1e-3
+    np.testing.assert_allclose(grad[:, 2], fd[:, 2], rtol=1e-6, atol=0)
+    assert np.abs(grad[:, :2]).max() < 1e-9 and np.abs(fd[:, :2]).max() < 1e-7
+    assert abs(grad[0, 2] + grad[1, 2]) < 1e-8  # equal and opposite on the symmetric molecule
+
+
+def test_variational_nuclear_gradient_interacting(pkg, cuda):
+    """The same for the self-consistent He atom displaced from a grid point (h = 0.5, box 12): the
+    Lagrangian gradient against central differences of tightly converged SCF energies. The discrete
+    Hartree potential's non-stationarity leaves a first-order gap at this coarse grid."""
+    system = oscf.he_lda(spacing=0.5, edge=12.0)
+    system.positions = ((0.11, -0.07, 0.19),)
+    geo = _geometry(pkg, system, cuda)
+    grid = geo.grid
+    scf = pkg.SCFConfig(energy_tol=1e-12, density_tol=1e-9, max_iterations=300)
+    mixing = pkg.MixingConfig(scheme="linear", alpha=0.3)
+    eigen = pkg.EigenConfig(residual_tol=1e-11)
+
+    def solve(g):
+        out = pkg.solve_self_consistent(pkg.KohnShamStep(g, "lda_vwn", 2.0, eigen), mixing, scf)
+        assert out.converged
+        return out
+
+    def build(positions):
+        return pkg.build_cusp_geometry(grid, system.charges, positions)
+
+    base = solve(geo)
+    step = pkg.KohnShamStep(geo, "lda_vwn", 2.0, eigen)
+    p_in = step.potentials(base.density)
+    eig, _ = step.diagonalise(step.hamiltonian(p_in))
+    occ = step.occupy(eig.eigenvalues)
+    grad = pkg.adjoint.nuclear_gradient_variational(build, system.positions, eig.eigenvectors, occ[0],
+                                                    eig.eigenvalues, functional="lda_vwn", n_electrons=2.0)
+    fd = pkg.adjoint.nuclear_gradient(lambda pos: float(solve(build([tuple(p) for p in pos])).energies["total"]),
+                                      system.positions, delta=1e-4)
+    assert np.abs(fd).max() > 1e-4
+    np.testing.assert_allclose(grad, fd, rtol=2e-2, atol=2e-6)

@@ -200,8 +200,8 @@ def fixed_orbital_energy(geometry, orbitals: torch.Tensor, occupations: torch.Te
     from .scf import KohnShamStep, nuclear_repulsion
 
     phi = orbitals.to(torch.float64).reshape(-1, geometry.grid.n_points)
-    occ = occupations.to(torch.float64).reshape(-1)
-    eps = eigenvalues.to(torch.float64).reshape(-1)
+    occ = occupations.to(device=phi.device, dtype=torch.float64).reshape(-1)
+    eps = eigenvalues.to(device=phi.device, dtype=torch.float64).reshape(-1)
     ham = CuspFactoredHamiltonian(geometry.grid, geometry.factor, quadrature=geometry.quadrature)
     q = ham.measure.quadrature
     a_phi = ham.apply(phi)
@@ -220,7 +220,8 @@ def fixed_orbital_energy(geometry, orbitals: torch.Tensor, occupations: torch.Te
 
 def nuclear_gradient_variational(build, positions, orbitals: torch.Tensor, occupations: torch.Tensor,
                                  eigenvalues: torch.Tensor, functional: str | None = None,
-                                 n_electrons: float | None = None, delta: float = 1.0e-4) -> np.ndarray:
+                                 n_electrons: float | None = None, delta: float = 1.0e-4,
+                                 components=None) -> np.ndarray:
     """``dE/dR_a`` from the stationarity of the Kohn--Sham Lagrangian (Hellmann--Feynman with the
     Pulay terms of the moving cusp factor, quadrature and measure): ``dE/dR = dL/dR`` at the
     converged orbitals, so no orbital response and no re-solve. The explicit geometry derivative of
@@ -231,17 +232,18 @@ def nuclear_gradient_variational(build, positions, orbitals: torch.Tensor, occup
     Exact for a bare-nucleus problem (the eigenvalue derivative of an operator self-adjoint in the
     measure). For the self-consistent energy it carries the first-order error of the discrete
     Hartree potential's non-stationarity noted in the module docstring, which vanishes as the grid
-    refines.
+    refines. ``components`` (pairs ``(nucleus, axis)``) limits the work to those entries; the
+    others are returned as zero.
     """
     base = np.asarray(positions, dtype=float)
     grad = np.zeros_like(base)
-    for a in range(base.shape[0]):
-        for d in range(3):
-            values = []
-            for sign in (+1.0, -1.0):
-                moved = base.copy()
-                moved[a, d] += sign * delta
-                geo = build([tuple(p) for p in moved])
-                values.append(fixed_orbital_energy(geo, orbitals, occupations, eigenvalues, functional, n_electrons))
-            grad[a, d] = (values[0] - values[1]) / (2.0 * delta)
+    todo = components if components is not None else [(a, d) for a in range(base.shape[0]) for d in range(3)]
+    for a, d in todo:
+        values = []
+        for sign in (+1.0, -1.0):
+            moved = base.copy()
+            moved[a, d] += sign * delta
+            geo = build([tuple(p) for p in moved])
+            values.append(fixed_orbital_energy(geo, orbitals, occupations, eigenvalues, functional, n_electrons))
+        grad[a, d] = (values[0] - values[1]) / (2.0 * delta)
     return grad

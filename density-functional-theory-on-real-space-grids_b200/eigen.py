@@ -49,11 +49,33 @@ def chebyshev_filter(hamiltonian, block: torch.Tensor, degree: int, lower: float
     """
     if upper <= lower:
         raise ValueError(f"filter interval is empty: lower={lower}, upper={upper}")
+    if not hasattr(hamiltonian, "operator"):
+        # an operator that is not one diagonal potential (the level-shifted rung of the fallback
+        # ladder): the scaled recurrence over its own apply, as chefsi.py:99-113 runs it
+        return _eager_filter(hamiltonian, block, degree, lower, upper, spectrum_min)
     rows = chebyshev_coefficients(degree, lower, upper, spectrum_min)
     # pinned + non-blocking: a pageable copy would synchronise the stream (as chefsi.py:316-321 notes)
     table = torch.tensor(rows, dtype=torch.float64).pin_memory().to(block.device, non_blocking=True)
     return filter_with_table(hamiltonian, block, table, degree, orbitals_per_group=block.numel() // block.shape[-1],
                              precision=precision)
+
+
+def _eager_filter(hamiltonian, block: torch.Tensor, degree: int, lower: float, upper: float,
+                  spectrum_min: float) -> torch.Tensor:
+    """The scaled three-term recurrence (``src/cdft/eigen/chefsi.py:99-113``) over ``hamiltonian.apply``."""
+    e = 0.5 * (upper - lower)
+    c = 0.5 * (upper + lower)
+    sigma = e / (spectrum_min - c)
+    sigma1 = sigma
+    x = block.to(torch.float64)
+    y = (hamiltonian.apply(x) - c * x) * (sigma1 / e)
+    previous = x
+    for _ in range(2, degree + 1):
+        sigma2 = 1.0 / (2.0 / sigma1 - sigma)
+        y_new = (hamiltonian.apply(y) - c * y) * (2.0 * sigma2 / e) - (sigma * sigma2) * previous
+        previous, y = y, y_new
+        sigma = sigma2
+    return y
 
 
 def filter_workspace(op, batch: int, device: torch.device) -> torch.Tensor:

@@ -121,19 +121,40 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _profile_traffic(kernel_tag: str):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summaries, if present."""
-    for name in ("slab_filter_wide_he65.txt", "slab_filter_he65.txt"):
-        path = ROOT / "profiles" / name
+def _profile_figure(name: str, kernel_tag: str):
+    """A figure (``name[kernel_tag] = value``) of the dominant kernel from the committed ncu summaries."""
+    for file in ("slab_filter_wide_he65.txt", "slab_filter_he65.txt"):
+        path = ROOT / "profiles" / file
         if not path.exists():
             continue
         for line in path.read_text().splitlines():
-            if line.startswith(f"traffic_bytes_per_launch[{kernel_tag}]"):
+            if line.startswith(f"{name}[{kernel_tag}]"):
                 try:
                     return float(line.rsplit("=", 1)[1].strip())
                 except ValueError:
                     return None
     return None
+
+
+def _profile_traffic(kernel_tag: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summaries, if present."""
+    return _profile_figure("traffic_bytes_per_launch", kernel_tag)
+
+
+def _profile_pipe(tag: str, batch: int):
+    """The arithmetic pipe's active fraction of the dominant kernel (ncu sm__pipe_fma_cycles_active for
+    float32, sm__pipe_fp64_cycles_active for float64, over elapsed cycles), from the committed capture
+    at this batch or, failing that, the largest batch captured (a rate, nearly independent of the
+    batch once the grid fills the GPU)."""
+    name = "fma_pipe_frac" if tag == "f32x4" else "fp64_pipe_frac"
+    exact = _profile_figure(name, f"{tag},batch={batch}")
+    if exact is not None:
+        return exact, batch
+    for b in (64, 32, 16, 8, 1):
+        value = _profile_figure(name, f"{tag},batch={b}")
+        if value is not None:
+            return value, b
+    return None, None
 
 
 def filter_step_roofline(pkg, dev, grid, hamiltonian, m: int, precision, reps: int = 5, degree: int = 20):
@@ -297,22 +318,27 @@ def run_adjoint(args) -> None:
         "grid": list(grid.shape)}), flush=True)
 
 
-def run_scan(args) -> None:
+SCAN_BONDS = [0.8 + k * 5.2 / 47 for k in range(48)]
+
+
+def scan_system(bond: float):
+    from oracle import scf as oscf  # the system definitions only
+
+    return oscf.h2_plus(bond, spacing=0.25, transverse=12.0)
+
+
+def scan_figures(pkg, dev, precision, warmup: int, one_by_one: bool = True, indices=None) -> dict:
     """The bare H2+ bond scan: 48 systems, R = 0.8 + k 5.2 / 47, box (12, 12, R + 12), h = 0.25.
 
     Every system has its own grid (49 x 49 x 52 .. 73) and device geometry; one batched solve runs
-    them together (one filter launch per CheFSI iteration for all 48). Reports systems per second of
-    the batched solve (the geometry builds timed separately) and, for comparison, of one-by-one solves.
+    them together (one filter launch per CheFSI iteration for all of them). Returns systems per second
+    of the batched solve (the geometry builds timed separately) and, if asked, of one-by-one solves.
+    ``indices`` selects a share of the 48 (a rank's, under a cost partition); ``totals`` maps each
+    solved index to its total energy.
     """
     import torch
 
-    import __graft_entry__
-    from oracle import scf as oscf  # the system definitions only
-
-    pkg = __graft_entry__.package()
-    dev = torch.device("cuda:0")
-    bonds = [0.8 + k * 5.2 / 47 for k in range(48)]
-    precision = torch.float32 if args.form == "mixed" else torch.float64
+    indices = list(range(len(SCAN_BONDS))) if indices is None else list(indices)
     stream = torch.cuda.current_stream()
 
     def timed(fn):
@@ -326,26 +352,79 @@ def run_scan(args) -> None:
 
     def build_all():
         geos = []
-        for bond in bonds:
-            system = oscf.h2_plus(bond, spacing=0.25, transverse=12.0)
+        for k in indices:
+            system = scan_system(SCAN_BONDS[k])
             grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev)
             geos.append(pkg.build_cusp_geometry(grid, system.charges, system.positions))
         return geos
 
+    if not indices:
+        return {"value": 0.0, "unit": "solves/s", "batched_solve_s": 0.0, "one_by_one_solve_s": None,
+                "geometry_build_s": 0.0, "grids": [], "totals": {}}
     geos, build_s = timed(build_all)
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         pkg.batch.solve_noninteracting_batch(geos, 1.0, filter_precision=precision)
     batched, batched_s = timed(lambda: pkg.batch.solve_noninteracting_batch(geos, 1.0, filter_precision=precision))
-    _, single_s = timed(lambda: [pkg.solve_noninteracting(g, n_electrons=1.0) for g in geos])
+    single_s = None
+    if one_by_one:
+        _, single_s = timed(lambda: [pkg.solve_noninteracting(g, n_electrons=1.0) for g in geos])
+    return {"metric": "H2+ bond scan (48 systems, own grids) solves/s", "value": len(indices) / batched_s,
+            "unit": "solves/s", "batched_solve_s": batched_s, "one_by_one_solve_s": single_s,
+            "geometry_build_s": build_s, "grids": sorted({g.grid.shape for g in geos}),
+            "totals": {k: float(batched[j]["total"]) for j, k in enumerate(indices)}}
+
+
+def scan_errors(totals: list[float]) -> list[float]:
+    """|E - E_reference| for the scan members the reference fixtures hold."""
     golden = json.loads((ROOT / "tests" / "golden" / "reference_values.json").read_text())
-    errors = [abs(batched[k]["total"] - golden[f"h2plus_scan_R{bonds[k]:.4f}"]["total"])
-              for k in range(48) if f"h2plus_scan_R{bonds[k]:.4f}" in golden]
-    print(json.dumps({
-        "metric": "H2+ bond scan (48 systems, own grids) solves/s", "value": 48 / batched_s, "unit": "solves/s",
-        "n_gpus": 1, "form": args.form, "batched_solve_s": batched_s, "one_by_one_solve_s": single_s,
-        "geometry_build_s": build_s, "grids": sorted({g.grid.shape for g in geos}),
-        "max_energy_error_vs_reference_ha": max(errors) if errors else None, "reference_members_checked": len(errors),
-        "data": "synthetic (the H2+ systems themselves)"}), flush=True)
+    return [abs(totals[k] - golden[f"h2plus_scan_R{SCAN_BONDS[k]:.4f}"]["total"])
+            for k in range(len(SCAN_BONDS)) if f"h2plus_scan_R{SCAN_BONDS[k]:.4f}" in golden]
+
+
+def run_scan(args) -> None:
+    """The H2+ bond scan (``--workload h2plus-scan``) on N GPUs: the 48 systems are partitioned by
+    cost (grid points; every member takes a similar number of applies) with one batched solve per
+    rank and no collective during the solve; the time is the max over ranks and rank 0 gathers the
+    energies on the host."""
+    import torch
+
+    import __graft_entry__
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    pkg = __graft_entry__.package()
+    precision = torch.float32 if args.form == "mixed" else torch.float64
+    shapes = []
+    for bond in SCAN_BONDS:
+        system = scan_system(bond)
+        shapes.append(pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev).shape)
+    costs = [pkg.replicas.system_cost(s) for s in shapes]
+    shares = pkg.replicas.partition_by_cost(costs, world)
+    figures = scan_figures(pkg, dev, precision, args.warmup, one_by_one=world == 1, indices=shares[rank])
+    slowest = max_over_ranks(figures["batched_solve_s"], dist, dev)
+    totals = pkg.replicas.gather_by_index(figures.pop("totals"), len(SCAN_BONDS), dist)
+    if rank == 0:
+        errors = scan_errors(totals)
+        figures.update({"value": len(SCAN_BONDS) / slowest, "batched_solve_s": slowest, "n_gpus": world,
+                        "form": args.form, "partition": "by cost (grid points), longest processing time first",
+                        "share_loads": pkg.replicas.share_loads(costs, shares),
+                        "max_energy_error_vs_reference_ha": max(errors) if errors else None,
+                        "reference_members_checked": len(errors),
+                        "data": "synthetic (the H2+ systems themselves)"})
+        print(json.dumps(figures), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def _axis_term(ham, box, axis: int):
@@ -852,6 +931,7 @@ def main() -> None:
     peak, peak_kind = _peaks()
     # one shared geometry: the wide-lane kernel (four float32 or two float64 orbitals per lane point)
     tag = "f32x4" if precision == torch.float32 else "f64x2"
+    pipe_frac, pipe_batch = _profile_pipe(tag, batch)
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -870,9 +950,21 @@ def main() -> None:
                      "traffic": _profile_traffic(f"{tag},batch={batch}"),
                      "kernel": f"slab_filter_wide_kernel<{tag}> (one Chebyshev step, {batch} systems x 5 orbitals)",
                      "algorithmic_bytes_per_launch": algorithmic, "us_per_launch": per_launch_s * 1e6,
-                     "peak_kind": peak_kind},
+                     "peak_kind": peak_kind,
+                     "fp32_pipe_frac" if tag == "f32x4" else "fp64_pipe_frac": pipe_frac,
+                     "pipe_source": (f"ncu {'sm__pipe_fma' if tag == 'f32x4' else 'sm__pipe_fp64'}_cycles_active / "
+                                     f"elapsed, one launch at {pipe_batch} systems (profiles/slab_filter_wide_he65.txt)"
+                                     if pipe_frac is not None else None)},
         "clocks": clocks,
     }
+    if rank == 0 and world == 1:
+        # config 4 beside the headline: the 48-system bond scan, every system on its own grid
+        scan = scan_figures(pkg, dev, precision, warmup=1, one_by_one=False)
+        errors = scan_errors([scan["totals"][k] for k in range(len(SCAN_BONDS))])
+        result["h2plus_scan"] = {k: scan[k] for k in ("value", "unit", "batched_solve_s", "geometry_build_s")}
+        result["h2plus_scan"].update({"max_energy_error_vs_reference_ha": max(errors) if errors else None,
+                                      "reference_members_checked": len(errors)})
+        result["h2plus_scan"]["workload"] = "bare H2+ bond scan, 48 systems on their own grids (49x49x52..73)"
     if plain is not None:
         result["plain_fp64"] = plain
         result["batched_mixed_over_plain_fp64"] = value / (world * plain["value"])

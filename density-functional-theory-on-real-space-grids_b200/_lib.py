@@ -80,6 +80,7 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_external_grid_terms_f64": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
                                               c_int, c_void_p, c_void_p]),
     "cdftb_filter_tuned_tile": (c_int, [c_int, c_int, c_int, c_int, c_int64, c_void_p, c_void_p]),
+    "cdftb_filter_tuned_tile_rows": (c_int, [c_int, c_int, c_int, c_int, c_int64, c_void_p]),
     "cdftb_poisson_plan_create": (c_int, [c_int, c_int, c_int, c_double, c_double, c_int, ctypes.POINTER(c_void_p),
                                           ctypes.POINTER(c_int), ctypes.POINTER(c_double)]),
     "cdftb_poisson_plan_destroy": (c_int, [c_void_p]),

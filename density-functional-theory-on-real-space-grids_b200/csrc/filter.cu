@@ -59,6 +59,7 @@ constexpr int NG = 2;     // pass warp groups; planes alternate between them
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
 static_assert(R % NG == 0 && RY % NG == 0, "a slot is always served by the same pass group");
 constexpr unsigned kSuspendNs = 20000;  // try_wait suspend hint: a waiting warp sleeps instead of spinning
+constexpr unsigned kNapNs = 256;        // longest sleep between tries of the wide kernel's producer and pass groups
 
 constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
 
@@ -202,12 +203,20 @@ __device__ __forceinline__ void record_failure(unsigned token) {
 }
 
 // Bounded wait for the phase of this parity. False after limit_ns, or as soon as another warp or
-// CTA of the same launch has given up; a timeout itself is recorded.
+// CTA of the same launch has given up; a timeout itself is recorded. With nap_ns > 0 the warp sleeps
+// between tries, 32 ns doubling up to nap_ns: a role that runs ahead of the one it waits for (the
+// producer, the pass groups) then takes few issue slots from the warps doing the work, at the cost
+// of waking up to nap_ns late.
 __device__ __noinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity, unsigned long long limit_ns,
-                                               unsigned token) {
+                                               unsigned token, unsigned nap_ns) {
     const unsigned long long start = globaltimer();
+    unsigned nap = 32;
     for (unsigned it = 0; it < (1u << 30); ++it) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (nap_ns > 0) {
+            __nanosleep(nap);
+            nap = nap * 2 < nap_ns ? nap * 2 : nap_ns;
+        }
         if ((it & 7) == 7) {
             if (*reinterpret_cast<volatile unsigned*>(&g_abort_token) == token) return false;
             if (globaltimer() - start > limit_ns) {
@@ -220,15 +229,15 @@ __device__ __noinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity, un
     return false;
 }
 
-__device__ __forceinline__ bool wait_full(unsigned bar, unsigned parity, unsigned token) {
+__device__ __forceinline__ bool wait_full(unsigned bar, unsigned parity, unsigned token, unsigned nap_ns = 0) {
     if (mbar_try_wait(bar, parity)) return true;
-    return mbar_wait_bounded(bar, parity, kWaitLimitNs, token);
+    return mbar_wait_bounded(bar, parity, kWaitLimitNs, token, nap_ns);
 }
 
 // The same wait by every lane of a warp, with one verdict for the whole warp (a lane that gave up
 // makes the warp leave together, so no lane waits in __syncwarp for an exited one).
-__device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, unsigned token) {
-    return __all_sync(0xffffffffu, wait_full(bar, parity, token)) != 0;
+__device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, unsigned token, unsigned nap_ns = 0) {
+    return __all_sync(0xffffffffu, wait_full(bar, parity, token, nap_ns)) != 0;
 }
 
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
@@ -560,13 +569,18 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
 // Wide lanes: 16 bytes per lane point -- four float32 orbitals (two packed f32x2 instructions per
 // element operation) or two float64 orbitals. The instructions that do not scale with the orbitals
 // (addressing, barrier waits, loads and stores of a point, the weights) are shared by twice as many
-// orbitals as in slab_filter_kernel. The roles and rings are those of slab_filter_kernel; two parts
-// are restructured so that a thread stays within 128 registers (one CTA of 512 threads per SM):
-//   pass item   streams its 22 nodes through a window of 8, forming each face as soon as its 8
-//               nodes are in and adding it at once to the 8 outputs it reaches (8 accumulators);
+// orbitals as in slab_filter_kernel. The roles and rings are those of slab_filter_kernel; three parts
+// are restructured so that a thread stays within its register share (one CTA per SM) and the roles
+// wait on one another less:
+//   tile        TY x TZ with TY = 8 or 13 (13 x 24 covers a 65-row grid in 5 tiles without padding);
+//   pass item   streams its TY + 14 nodes through a window of 8, forming each face as soon as its 8
+//               nodes are in and adding it at once to the TY outputs it reaches (TY accumulators);
+//               the plane slot is released as soon as the outputs are in registers, before they are
+//               stored to a result slot;
 //   march       keeps the last 8 nodes and the 8 outputs still open: each new x face is added to all
-//               of them, the newest output starts from its plane's y+z part, and the oldest one is
-//               complete after its last face.
+//               of them, the newest output opens with its first face, and the oldest one is complete
+//               after its last face, when its plane's y+z part joins it. The pass groups thus have
+//               7 planes of lead on the march, and the result ring is 8 (or 6) slots deep.
 // Lanes run over the orbitals in order (lane l: orbitals ORB l .. ORB l + ORB - 1); lanes aligned to
 // orbital groups (per-system geometry) keep slab_filter_kernel.
 
@@ -581,6 +595,19 @@ struct WideF4 {  // four float32 orbitals
     static __device__ __forceinline__ float2 hi(E v) { return make_float2(v.z, v.w); }
     static __device__ __forceinline__ E join(float2 a, float2 b) { return make_float4(a.x, a.y, b.x, b.y); }
     static __device__ __forceinline__ T splat(S s) { return make_float2(s, s); }
+    // c - t v and -t v (the negation folded into the operand)
+    static __device__ __forceinline__ E fmat_neg(T t, E v, E c) {
+        const T n = make_float2(-t.x, -t.y);
+        return join(__ffma2_rn(n, lo(v), lo(c)), __ffma2_rn(n, hi(v), hi(c)));
+    }
+    static __device__ __forceinline__ E mult_neg(T t, E v) {
+        const T n = make_float2(-t.x, -t.y);
+        return join(__fmul2_rn(n, lo(v)), __fmul2_rn(n, hi(v)));
+    }
+    // c + tap[k] v for the antisymmetric taps held as their lower four (k = 0..7, compile time)
+    static __device__ __forceinline__ E fmat_k(const T* t4, int k, E v, E c) {
+        return k < 4 ? fmat(t4[k], v, c) : fmat_neg(t4[7 - k], v, c);
+    }
     static __device__ __forceinline__ E fmat(T t, E v, E c) {
         return join(__ffma2_rn(t, lo(v), lo(c)), __ffma2_rn(t, hi(v), hi(c)));
     }
@@ -590,6 +617,10 @@ struct WideF4 {  // four float32 orbitals
     }
     static __device__ __forceinline__ E mul(E a, E b) { return join(__fmul2_rn(lo(a), lo(b)), __fmul2_rn(hi(a), hi(b))); }
     static __device__ __forceinline__ E add(E a, E b) { return join(__fadd2_rn(lo(a), lo(b)), __fadd2_rn(hi(a), hi(b))); }
+    // a - b (the negation folded into the add's operand)
+    static __device__ __forceinline__ E sub(E a, E b) {
+        return join(__fadd2_rn(lo(a), make_float2(-b.x, -b.y)), __fadd2_rn(hi(a), make_float2(-b.z, -b.w)));
+    }
     static __device__ __forceinline__ E neg(E a) { return make_float4(-a.x, -a.y, -a.z, -a.w); }
     static __device__ __forceinline__ E zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
     static __device__ __forceinline__ E make(const S* v) { return make_float4(v[0], v[1], v[2], v[3]); }
@@ -609,6 +640,13 @@ struct WideD2 {  // two float64 orbitals
     static constexpr bool WIDE = true;
     static constexpr CUtensorMapDataType GEO_TYPE = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
     static __device__ __forceinline__ T splat(S s) { return s; }
+    static __device__ __forceinline__ E fmat_neg(T t, E v, E c) {
+        return make_double2(::fma(-t, v.x, c.x), ::fma(-t, v.y, c.y));
+    }
+    static __device__ __forceinline__ E mult_neg(T t, E v) { return make_double2(-t * v.x, -t * v.y); }
+    static __device__ __forceinline__ E fmat_k(const T* t4, int k, E v, E c) {
+        return k < 4 ? fmat(t4[k], v, c) : fmat_neg(t4[7 - k], v, c);
+    }
     static __device__ __forceinline__ E fmat(T t, E v, E c) { return make_double2(::fma(t, v.x, c.x), ::fma(t, v.y, c.y)); }
     static __device__ __forceinline__ E mult(T t, E v) { return make_double2(t * v.x, t * v.y); }
     static __device__ __forceinline__ E fma(E a, E b, E c) {
@@ -616,6 +654,7 @@ struct WideD2 {  // two float64 orbitals
     }
     static __device__ __forceinline__ E mul(E a, E b) { return make_double2(a.x * b.x, a.y * b.y); }
     static __device__ __forceinline__ E add(E a, E b) { return make_double2(a.x + b.x, a.y + b.y); }
+    static __device__ __forceinline__ E sub(E a, E b) { return make_double2(a.x - b.x, a.y - b.y); }
     static __device__ __forceinline__ E neg(E a) { return make_double2(-a.x, -a.y); }
     static __device__ __forceinline__ E zero() { return make_double2(0.0, 0.0); }
     static __device__ __forceinline__ E make(const S* v) { return make_double2(v[0], v[1]); }
@@ -628,12 +667,17 @@ struct WideD2 {  // two float64 orbitals
 constexpr int RW = 4;  // plane slots of the wide kernel (16-byte elements: a slot is 34-40 KB)
 static_assert(RW % NG == 0, "a slot is always served by the same pass group");
 
-template <int TZ, int SB, int ORB>  // SB: bytes of a geometry element; ORB: potentials per lane
+template <int TYW, int TZ, int SB, int ORB>  // TYW: tile rows; SB: bytes of a geometry element; ORB: potentials per lane
 struct WideShape {
+    static constexpr int NROWW = TYW + 2 * HALO;  // rows of the phi box
     static constexpr int EB = 16;
-    static constexpr int MW = TY * TZ / 32;
-    static constexpr int NZS = (TZ + 7) / 8;
-    static constexpr int ITEMS = TZ + TY * NZS;
+    // march warps: one thread per tile point (the last warp may have idle threads)
+    static constexpr int MW = (TYW * TZ + 31) / 32;
+    // pass items: TZ columns of TYW outputs (y) and TYW rows x NZS segments of TYW outputs (z); the
+    // last z segment is moved left to end at TZ (it then stores only the outputs the previous one
+    // did not): every item forms TYW outputs from TYW + 14 nodes
+    static constexpr int NZS = (TZ + TYW - 1) / TYW;
+    static constexpr int ITEMS = TZ + TYW * NZS;
     static constexpr int PWG = (ITEMS + 31) / 32;
     static constexpr int PW = NG * PWG;
     static constexpr int WARPS = MW + PW + 1;
@@ -642,13 +686,13 @@ struct WideShape {
     // groups of 4 banks (an even pitch such as TZ + 18 puts them on 4)
     static constexpr int BW = TZ + 19;  // phi box: z0-8 .. z0+TZ+10
     static constexpr int ZROW = TZ + 3;
-    static constexpr unsigned TX_PHI = NROW * BW * EB;
-    static constexpr unsigned TX_PREV = TY * TZ * EB;
-    static constexpr unsigned TX_W0 = TY * TZ * SB;
-    static constexpr unsigned TX_W1 = (TY + 7) * TZ * SB;
-    static constexpr unsigned TX_W2 = TY * (TZ + 8) * SB;
-    static constexpr unsigned TX_INV = TY * TZ * SB;
-    static constexpr unsigned TX_POT = TY * TZ * SB;
+    static constexpr unsigned TX_PHI = NROWW * BW * EB;
+    static constexpr unsigned TX_PREV = TYW * TZ * EB;
+    static constexpr unsigned TX_W0 = TYW * TZ * SB;
+    static constexpr unsigned TX_W1 = (TYW + 7) * TZ * SB;
+    static constexpr unsigned TX_W2 = TYW * (TZ + 8) * SB;
+    static constexpr unsigned TX_INV = TYW * TZ * SB;
+    static constexpr unsigned TX_POT = TYW * TZ * SB;
     static constexpr size_t O_PHI = 0;
     static constexpr size_t O_PREV = O_PHI + align128(TX_PHI);
     static constexpr size_t O_W0 = O_PREV + align128(TX_PREV);
@@ -659,30 +703,47 @@ struct WideShape {
     static constexpr size_t POT_STEP = align128(TX_POT);
     static constexpr size_t SLOT = O_POT + ORB * POT_STEP;
     static constexpr size_t O_YZ = RW * SLOT;
-    static constexpr size_t YZ_Z = size_t(TY) * TZ * EB;
-    static constexpr size_t YZ_SLOT = align128(YZ_Z + size_t(TY) * ZROW * EB);
-    static constexpr size_t O_BAR = O_YZ + RY * YZ_SLOT;
-    static constexpr size_t BYTES = O_BAR + (2 * RW + 2 * RY) * 8;
-    static_assert(TY * TZ % 32 == 0, "march warps cover the tile");
-    static_assert(TZ >= 8 && TZ % 2 == 0, "z segments of 8 inside the tile");
+    static constexpr size_t YZ_Z = size_t(TYW) * TZ * EB;
+    static constexpr size_t YZ_SLOT = align128(YZ_Z + size_t(TYW) * ZROW * EB);
+    // y+z result slots: the march adds a plane's y+z part when that output completes, 7 planes after
+    // the pass formed it, so the ring is as deep as shared memory allows (8, else 6, else 4)
+    static constexpr size_t fits(int ry) { return O_YZ + ry * YZ_SLOT + (2 * RW + 2 * ry) * 8 <= 232448; }
+    static constexpr int RYW = fits(8) ? 8 : fits(6) ? 6 : 4;
+    static constexpr size_t O_BAR = O_YZ + RYW * YZ_SLOT;
+    static constexpr size_t BYTES = O_BAR + (2 * RW + 2 * RYW) * 8;
+    static_assert(RYW % NG == 0, "a result slot is always served by the same pass group");
+    static_assert(TZ >= TYW && TZ % 4 == 0, "z segments of TYW inside the tile; 16-byte float32 geometry rows");
     static_assert(BW % 2 == 1 && ZROW % 2 == 1, "odd row pitches");
-    static_assert((TZ - 8) + 22 <= BW - 1, "the last z segment's nodes lie inside the phi box");
+    static_assert((TZ - TYW) + NROWW <= BW - 1, "the last z segment's nodes lie inside the phi box");
+    // the idle march threads of the last warp read their tile's first point (see the kernel); the
+    // per-point regions of a slot hold at least one warp's worth of points past the tile
+    static_assert(TYW * TZ >= 32, "a tile of at least one warp");
     static_assert(BYTES <= 232448, "fits the opt-in shared memory of one CTA");
 };
 
-template <typename W, int TZ>
-__global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::T, 1)
+// One CTA per SM: the register budget per thread. The SM's 64 K registers are four files of 16 K,
+// one per scheduler, and a CTA's warps are spread over the four, so the scheduler with the most
+// warps (ceil(warps / 4)) bounds it: 128 registers for 13 to 16 warps, 170 for 9 to 12.
+template <int T>
+constexpr int wide_max_registers() {
+    return (16384 / (((T / 32) + 3) / 4 * 32)) / 8 * 8 < 255 ? (16384 / (((T / 32) + 3) / 4 * 32)) / 8 * 8 : 255;
+}
+
+template <typename W, int TYW, int TZ>
+__global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typename W::S), W::ORB>::T>()))
     slab_filter_wide_kernel(const __grid_constant__ FilterMaps maps, const FilterArgs a) {
     using E = typename W::E;
     using S = typename W::S;
     constexpr int ORB = W::ORB;
-    using SH = WideShape<TZ, sizeof(S), ORB>;
+    using SH = WideShape<TYW, TZ, sizeof(S), ORB>;
+    constexpr int TY = TYW;              // this kernel's tile rows (the 8-byte-lane kernel keeps 8)
+    constexpr int NROW = SH::NROWW;
     constexpr int BW = SH::BW;
     extern __shared__ __align__(1024) unsigned char smem[];
     const unsigned bar_full = smem_u32(smem + SH::O_BAR);
     const unsigned bar_empty = bar_full + 8 * RW;
     const unsigned bar_yfull = bar_empty + 8 * RW;
-    const unsigned bar_yempty = bar_yfull + 8 * RY;
+    const unsigned bar_yempty = bar_yfull + 8 * SH::RYW;
 
     const int t = threadIdx.x;
     const int warp = t >> 5;
@@ -708,7 +769,7 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
             mbar_init(bar_full + 8 * s, 1);
             mbar_init(bar_empty + 8 * s, SH::MW + SH::PWG);
         }
-        for (int s = 0; s < RY; ++s) {
+        for (int s = 0; s < SH::RYW; ++s) {
             mbar_init(bar_yfull + 8 * s, SH::PWG);
             mbar_init(bar_yempty + 8 * s, SH::MW);
         }
@@ -717,9 +778,12 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
     }
     __syncthreads();
 
-    typename W::T tap[8];
+    // the taps are antisymmetric (tap[7 - j] = -tap[j]): four registers serve all eight, the upper
+    // four as negated operands (tapk below)
+    typename W::T tap4[4];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) tap[j] = W::splat(static_cast<S>(a.taps[j]));
+    for (int j = 0; j < 4; ++j) tap4[j] = W::splat(static_cast<S>(a.taps[j]));
+#define tap(j) tap4[(j)]
 
     if (warp == SH::MW + SH::PW) {
         // ------------------------------------------------------------------ producer
@@ -734,7 +798,7 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
         int s = 0, ph = 1;
         for (int n = 0; n < npl; ++n) {
             if (a.stop_after_planes > 0 && n >= a.stop_after_planes) break;
-            if (n >= RW && !wait_full(bar_empty + 8 * s, ph, a.token)) break;
+            if (n >= RW && !wait_full(bar_empty + 8 * s, ph, a.token, kNapNs)) break;
             const unsigned full = bar_full + 8 * s;
             unsigned char* slot = smem + s * SH::SLOT;
             const int q = q0 + n;
@@ -785,8 +849,8 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
             const int zi = it - TZ;
             const int ry = zi % TY;
             const int seg = zi / TY;
-            const int zs = min(seg * 8, TZ - 8);
-            first = seg * 8 - zs;
+            const int zs = min(seg * TY, TZ - TY);
+            first = seg * TY - zs;
             active = y0 + ry < ny && z0 + zs < nz;
             nb = (ry + HALO) * BW + zs + 1;
             ns = 1;
@@ -797,36 +861,46 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
         }
         int s = pg, ph = 0;
         for (int n = pg; n < npl; n += NG) {
-            if (!warp_wait(bar_full + 8 * s, ph, a.token)) return;
+            if (!warp_wait(bar_full + 8 * s, ph, a.token, kNapNs)) return;
             const int q = q0 + n;
             if (q >= xa && q <= xe) {
-                const int m = q - xa;
-                const int ys = m & (RY - 1);
-                const unsigned uy = m / RY;
-                if (uy >= 1 && !warp_wait(bar_yempty + 8 * ys, (uy - 1) & 1, a.token)) return;
+                E acc[TY];
                 if (active) {
                     const unsigned char* slot = smem + s * SH::SLOT;
                     const E* nodes = reinterpret_cast<const E*>(slot) + nb;
                     const S* w = reinterpret_cast<const S*>(slot) + wb;
-                    E* out = reinterpret_cast<E*>(smem + SH::O_YZ + ys * SH::YZ_SLOT) + ob;
-                    E win[8], acc[TY];
+                    E win[8];
 #pragma unroll
                     for (int r = 0; r < NROW; ++r) {
                         win[r & 7] = nodes[r * ns];
                         if (r >= 7) {
                             const int rf = r - 7;  // face rf from nodes rf .. rf + 7
-                            E sum = W::zero();
+                            // the taps are antisymmetric (tap[7 - j] = -tap[j]): four independent
+                            // differences, then a chain of four (depth 5 instead of 8)
+                            E sum = W::mult(tap(0), W::sub(win[rf & 7], win[(rf + 7) & 7]));
 #pragma unroll
-                            for (int j = 0; j < 8; ++j) sum = W::fmat(tap[j], win[(rf + j) & 7], sum);
+                            for (int j = 1; j < 4; ++j)
+                                sum = W::fmat(tap(j), W::sub(win[(rf + j) & 7], win[(rf + 7 - j) & 7]), sum);
                             const E f = W::mult(W::splat(w[rf * ws]), sum);
                             // face rf reaches outputs o = rf - 7 .. rf with tap o + 7 - rf
 #pragma unroll
                             for (int o = 0; o < TY; ++o) {
                                 if (o < rf - 7 || o > rf) continue;
-                                acc[o] = (o == rf) ? W::mult(tap[7], f) : W::fmat(tap[o + 7 - rf], f, acc[o]);
+                                acc[o] = (o == rf) ? W::mult_neg(tap(0), f) : W::fmat_k(tap4, o + 7 - rf, f, acc[o]);
                             }
                         }
                     }
+                }
+                // the plane slot is free once the outputs are in registers; the result slot is
+                // reused only after the march has taken its previous plane (7 planes behind)
+                __syncwarp();
+                if ((t & 31) == 0) mbar_arrive(bar_empty + 8 * s);
+                const int m = q - xa;
+                const int ys = m % SH::RYW;
+                const unsigned uy = m / SH::RYW;
+                if (uy >= 1 && !warp_wait(bar_yempty + 8 * ys, (uy - 1) & 1, a.token, kNapNs)) return;
+                if (active) {
+                    E* out = reinterpret_cast<E*>(smem + SH::O_YZ + ys * SH::YZ_SLOT) + ob;
 #pragma unroll
                     for (int o = 0; o < TY; ++o)
                         if (o >= first) out[o * os] = acc[o];
@@ -835,8 +909,8 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
                 if ((t & 31) == 0) mbar_arrive(bar_yfull + 8 * ys);
             } else {
                 __syncwarp();
+                if ((t & 31) == 0) mbar_arrive(bar_empty + 8 * s);
             }
-            if ((t & 31) == 0) mbar_arrive(bar_empty + 8 * s);
             s += NG;
             if (s >= RW) {
                 s -= RW;
@@ -847,12 +921,15 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
     }
 
     // ---------------------------------------------------------------------- march
-    const int ty = t / TZ;
-    const int tz = t - ty * TZ;
+    // Threads past the tile (when TY * TZ is not a multiple of 32) take part in every wait and
+    // arrive, read their tile's first point and store nothing.
+    const bool in_tile = t < TY * TZ;
+    const int ty = in_tile ? t / TZ : 0;
+    const int tz = in_tile ? t - ty * TZ : 0;
     const int y = y0 + ty;
     const int z = z0 + tz;
-    const bool own_in = y < ny && z < nz;
-    const bool own_pad = y < ny && z < nzp;
+    const bool own_in = in_tile && y < ny && z < nz;
+    const bool own_pad = in_tile && y < ny && z < nzp;
     const int64_t plane_n = int64_t(ny) * nz;
     const int own = ty * TZ + tz;
 
@@ -890,29 +967,32 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
             phq[g] = reinterpret_cast<const E*>(slot + SH::O_PHI)[(ty + HALO) * BW + tz + 8];
             E face;
             {
-                E sum = W::zero();
+                // antisymmetric taps: sum_j<4 tap[j] (node q-7+j - node q-j)
+                E sum = W::mult(tap(0), W::sub(phq[(g + 1) & 7], phq[g & 7]));
 #pragma unroll
-                for (int j = 0; j < 8; ++j) sum = W::fmat(tap[j], phq[(g + 1 + j) & 7], sum);
+                for (int j = 1; j < 4; ++j)
+                    sum = W::fmat(tap(j), W::sub(phq[(g + 1 + j) & 7], phq[(g + 8 - j) & 7]), sum);
                 const S wx = own_in ? reinterpret_cast<const S*>(slot + SH::O_W0)[own] : S(0);
                 face = W::mult(W::splat(wx), sum);  // x face q - 4
             }
             // the face reaches the open outputs q - 7 .. q (slot (g - d) & 7 holds output q - d, tap 7 - d)
 #pragma unroll
-            for (int d = 1; d < 8; ++d) acc[(g - d) & 7] = W::fmat(tap[7 - d], face, acc[(g - d) & 7]);
+            for (int d = 1; d < 8; ++d) acc[(g - d) & 7] = W::fmat_k(tap4, 7 - d, face, acc[(g - d) & 7]);
+            const int i = q - HALO;  // output complete at this plane (slot (g + 1) & 7)
             E yz = W::zero();
-            if (q >= xa && q <= xe) {
-                const int m = q - xa;
-                const int ys = m & (RY - 1);
-                if (!warp_wait(bar_yfull + 8 * ys, (m / RY) & 1, a.token)) return;
+            if (i >= xa) {
+                // the y+z part of output i, formed by a pass group 7 planes ago
+                const int m = i - xa;
+                const int ys = m % SH::RYW;
+                if (!warp_wait(bar_yfull + 8 * ys, (m / SH::RYW) & 1, a.token)) return;
                 const unsigned char* yzs = smem + SH::O_YZ + ys * SH::YZ_SLOT;
                 yz = W::add(reinterpret_cast<const E*>(yzs)[own],
-                               reinterpret_cast<const E*>(yzs + SH::YZ_Z)[ty * SH::ZROW + tz]);
+                            reinterpret_cast<const E*>(yzs + SH::YZ_Z)[ty * SH::ZROW + tz]);
                 __syncwarp();
                 if ((t & 31) == 0) mbar_arrive(bar_yempty + 8 * ys);
             }
-            const int i = q - HALO;  // output complete at this plane (slot (g + 1) & 7)
             if (i >= xa && own_pad) {
-                const E div = acc[(g + 1) & 7];
+                const E div = W::add(acc[(g + 1) & 7], yz);
                 const int64_t pt = int64_t(i) * plane_n + (own_in ? int64_t(y) * nz + z : 0);
                 E res = W::zero();
                 if (own_in) {
@@ -951,9 +1031,9 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
                     out[(int64_t(lane) * nx + i) * (int64_t(ny) * nzp) + int64_t(y) * nzp + z] = res;
                 }
             }
-            // the newest output, q, opens from its y+z part and its first face (its slot held output
-            // q - 8, completed on the previous plane)
-            acc[g] = W::fmat(tap[7], face, yz);
+            // the newest output, q, opens with its first face (its slot held output q - 8, completed
+            // on the previous plane); its y+z part joins when it completes
+            acc[g] = W::mult_neg(tap(0), face);
             __syncwarp();
             if ((t & 31) == 0) mbar_arrive(bar_empty + 8 * s);
             if (++s == RW) {
@@ -963,6 +1043,8 @@ __global__ void __launch_bounds__(WideShape<TZ, sizeof(typename W::S), W::ORB>::
         }
     }
 }
+
+#undef tap
 
 // Internal layout from a caller block: lanes of (nx, ny, nzp), padding and missing orbitals zero.
 // blockIdx.y walks the lanes (the lane's orbitals are found once), and each thread writes two
@@ -1151,12 +1233,6 @@ GeoPack geo_pack(const cdftb_operator* op, int64_t batch) {
     return g;
 }
 
-// The z tile (32 or 36 columns) that wastes the fewest columns of the padded row.
-int choose_tz(int nzp) {
-    const int64_t w32 = ceil_div(nzp, 32) * 32;
-    const int64_t w36 = ceil_div(nzp, 36) * 36;
-    return w36 < w32 ? 36 : 32;
-}
 
 // x chunks: one CTA per SM is resident and a CTA's time grows with the planes it marches (its
 // chunk plus 14 halo planes), so pick the chunk count that minimises waves x planes.
@@ -1242,7 +1318,7 @@ int pad_rows(const void* src, int64_t rows, int cols, int cols_pad, S* dst, cuda
 // Copies the geometry into the padded rows TMA reads (at geo, element type S) and encodes the maps
 // of the geometry; kinetic_only zeroes the potential rows instead of copying them.
 template <typename Lane>
-int prepare_geometry(const cdftb_operator* op, int64_t batch, void* geo_base, int tz, bool kinetic_only,
+int prepare_geometry(const cdftb_operator* op, int64_t batch, void* geo_base, int ty, int tz, bool kinetic_only,
                      FilterMaps* maps, cudaStream_t stream) {
     using S = typename Lane::S;
     const int nx = op->nx, ny = op->ny, nz = op->nz;
@@ -1274,15 +1350,15 @@ int prepare_geometry(const cdftb_operator* op, int64_t batch, void* geo_base, in
     }
     const CUtensorMapDataType gt = Lane::GEO_TYPE;
     const int sb = sizeof(S);
-    const unsigned tile_box[4] = {unsigned(tz), unsigned(TY), 1, 1};
+    const unsigned tile_box[4] = {unsigned(tz), unsigned(ty), 1, 1};
     const int64_t d_w0[4] = {gp.nzg, ny, nx + 8, ng};
     const int64_t d_w1[4] = {gp.nzg, ny + 8, nx, ng};
-    const unsigned b_w1[4] = {unsigned(tz), unsigned(TY + 7), 1, 1};
+    const unsigned b_w1[4] = {unsigned(tz), unsigned(ty + 7), 1, 1};
     const int64_t d_w2[4] = {gp.nz8g, ny, nx, ng};
-    const unsigned b_w2[4] = {unsigned(tz + 8), unsigned(TY), 1, 1};
+    const unsigned b_w2[4] = {unsigned(tz + 8), unsigned(ty), 1, 1};
     const int64_t d_inv[4] = {gp.nzg, ny, nx, ng};
     const int64_t d_pot[4] = {gp.nzg, ny, nx, nsys};
-    const unsigned b_pot[4] = {unsigned(tz), unsigned(TY), 1, 1};
+    const unsigned b_pot[4] = {unsigned(tz), unsigned(ty), 1, 1};
     if ((st = encode_map(&maps->w0, gt, sb, 4, w0p, d_w0, tile_box)) != CDFTB_OK) return st;
     if ((st = encode_map(&maps->w1, gt, sb, 4, w1p, d_w1, b_w1)) != CDFTB_OK) return st;
     if ((st = encode_map(&maps->w2, gt, sb, 4, w2p, d_w2, b_w2)) != CDFTB_OK) return st;
@@ -1341,17 +1417,22 @@ int launch_any_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lane
 // ---- wide lanes (slab_filter_wide_kernel): launch, lane maps, packing
 bool g_wide = true;  // guarded by g_tune_mutex (declared below with the tuner)
 
-template <typename W, int TZ>
+template <typename W, int TYW, int TZ>
 int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
-    using SH = WideShape<TZ, sizeof(typename W::S), W::ORB>;
+    using SH = WideShape<TYW, TZ, sizeof(typename W::S), W::ORB>;
     static bool configured = false;
     if (!configured) {
-        int st = check(cudaFuncSetAttribute(slab_filter_wide_kernel<W, TZ>,
+        int st = check(cudaFuncSetAttribute(slab_filter_wide_kernel<W, TYW, TZ>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(SH::BYTES)));
         if (st != CDFTB_OK) return st;
+        // a CTA this kernel's registers cannot hold is refused here, before any launch
+        cudaFuncAttributes attr{};
+        st = check(cudaFuncGetAttributes(&attr, slab_filter_wide_kernel<W, TYW, TZ>));
+        if (st != CDFTB_OK) return st;
+        if (attr.maxThreadsPerBlock < SH::T) return CDFTB_ERR_CAPACITY;
         configured = true;
     }
-    const int tiles_y = static_cast<int>(ceil_div(a.ny, TY));
+    const int tiles_y = static_cast<int>(ceil_div(a.ny, TYW));
     a.tiles_z = static_cast<int>(ceil_div(a.nzp, TZ));
     const int64_t tiles = int64_t(tiles_y) * a.tiles_z;
     a.xchunk = xchunk > 0 ? (xchunk < a.nx ? xchunk : a.nx) : choose_chunk(a.nx, tiles * lanes, sm_count());
@@ -1363,7 +1444,7 @@ int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_
         a.token = next_launch_token(true);
         a.stop_after_planes = take_test_stop();
         dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(chunks), static_cast<unsigned>(count));
-        slab_filter_wide_kernel<W, TZ><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
+        slab_filter_wide_kernel<W, TYW, TZ><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
         int st = check_launch();
         if (st != CDFTB_OK) return st;
     }
@@ -1371,11 +1452,11 @@ int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_
 }
 
 // Lane buffers of 16-byte points described as 8-byte elements, two per point.
-int encode_wide_lane_maps(void* buf, int nzp, int ny, int nx, int64_t lanes, int tz, CUtensorMap* phi,
+int encode_wide_lane_maps(void* buf, int nzp, int ny, int nx, int64_t lanes, int ty, int tz, CUtensorMap* phi,
                           CUtensorMap* prev) {
     const int64_t lane_dims[4] = {2 * int64_t(nzp), ny, nx, lanes};
-    const unsigned phi_box[4] = {unsigned(2 * (tz + 19)), unsigned(NROW), 1, 1};  // WideShape::BW points
-    const unsigned prev_box[4] = {unsigned(2 * tz), unsigned(TY), 1, 1};
+    const unsigned phi_box[4] = {unsigned(2 * (tz + 19)), unsigned(ty + 2 * HALO), 1, 1};  // WideShape::BW points
+    const unsigned prev_box[4] = {unsigned(2 * tz), unsigned(ty), 1, 1};
     int st = encode_map(phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, phi_box);
     if (st == CDFTB_OK) st = encode_map(prev, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 4, buf, lane_dims, prev_box);
     return st;
@@ -1410,9 +1491,10 @@ constexpr int64_t lane_point_bytes() {
 }
 
 template <typename L>
-int encode_lanes(void* buf, int nzp, int ny, int nx, int64_t lanes, int tz, CUtensorMap* phi, CUtensorMap* prev) {
+int encode_lanes(void* buf, int nzp, int ny, int nx, int64_t lanes, int ty, int tz, CUtensorMap* phi,
+                 CUtensorMap* prev) {
     if constexpr (L::WIDE)
-        return encode_wide_lane_maps(buf, nzp, ny, nx, lanes, tz, phi, prev);
+        return encode_wide_lane_maps(buf, nzp, ny, nx, lanes, ty, tz, phi, prev);
     else
         return encode_lane_maps(buf, nzp, ny, nx, lanes, tz, phi, prev);
 }
@@ -1426,23 +1508,54 @@ int pack_lanes(const cdftb_operator* op, const void* block, int in_dtype, int64_
         return pack_block<L>(op, block, in_dtype, batch, nx, ny, nz, nzp, lanes, dst, stream);
 }
 
+// The tilings (rows TY x columns TZ) each lane layout has: the 8-byte-lane kernel 8 x 32 and 8 x 36;
+// the wide kernel also 13 x 24 (65 rows in five tiles, 66 columns in three: He at h = 0.25).
+struct Tile {
+    int ty, tz;
+};
+constexpr Tile kNarrowTiles[] = {{8, 32}, {8, 36}};
+constexpr Tile kWideTiles[] = {{8, 32}, {8, 36}, {13, 24}};
+
 template <typename L>
-int launch_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
-    if constexpr (L::WIDE)
-        return tz == 36 ? launch_wide<L, 36>(m, a, lanes, stream, xchunk) : launch_wide<L, 32>(m, a, lanes, stream, xchunk);
-    else
+int launch_tz(int ty, int tz, const FilterMaps& m, const FilterArgs& a, int64_t lanes, cudaStream_t stream,
+              int xchunk = 0) {
+    if constexpr (L::WIDE) {
+        if (ty == 13) return launch_wide<L, 13, 24>(m, a, lanes, stream, xchunk);
+        return tz == 36 ? launch_wide<L, 8, 36>(m, a, lanes, stream, xchunk)
+                        : launch_wide<L, 8, 32>(m, a, lanes, stream, xchunk);
+    } else {
         return launch_any_tz<L>(tz, m, a, lanes, stream, xchunk);
+    }
+}
+
+// The tiling that wastes the fewest padded points (ties: the earlier entry).
+template <typename L>
+Tile choose_tile(int ny, int nzp) {
+    Tile best = L::WIDE ? kWideTiles[0] : kNarrowTiles[0];
+    int64_t best_pts = -1;
+    const Tile* list = L::WIDE ? kWideTiles : kNarrowTiles;
+    const int count = L::WIDE ? 3 : 2;
+    for (int i = 0; i < count; ++i) {
+        const int64_t pts = ceil_div(ny, list[i].ty) * list[i].ty * ceil_div(nzp, list[i].tz) * list[i].tz;
+        if (best_pts < 0 || pts < best_pts) {
+            best_pts = pts;
+            best = list[i];
+        }
+    }
+    return best;
 }
 
 // ---- the tile autotuner
-// The z tile (32 or 36 columns) and the x chunk of a slab launch decide the CTA count, the waves
-// and the halo work; which wins depends on the grid, the lane count and the GPU. With the autotuner
+// The tile (8 x 32, 8 x 36, and for the wide kernel 13 x 24 rows x columns) and the x chunk of a slab
+// launch decide the CTA count, the waves, the padding and the halo work; which wins depends on the
+// grid, the lane count and the GPU. With the autotuner
 // on, the first filter call for a (device, grid, precision, lanes) key times every candidate on the
 // call's own buffers (the first Chebyshev step, which the real run then recomputes), keeps the
 // fastest in a host table, and every later filter or apply launch for that key uses it. Every
 // candidate gives bit-identical results: each output is formed by the same arithmetic in the same
-// order whatever the tiling. Off, the heuristics choose_tz / choose_chunk decide.
+// order whatever the tiling. Off, the heuristics choose_tile / choose_chunk decide.
 struct TileChoice {
+    int ty;
     int tz;
     int xchunk;  // 0: choose_chunk
 };
@@ -1484,12 +1597,16 @@ int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf
         return st;
     }
     float best_ms = -1.0f;
-    *best = TileChoice{choose_tz(nzp), 0};
-    for (int tz : {32, 36}) {
+    const Tile t0 = choose_tile<Lane>(ny, nzp);
+    *best = TileChoice{t0.ty, t0.tz, 0};
+    const Tile* list = Lane::WIDE ? kWideTiles : kNarrowTiles;
+    const int count = Lane::WIDE ? 3 : 2;
+    for (int ti = 0; ti < count; ++ti) {
+        const int ty = list[ti].ty, tz = list[ti].tz;
         FilterMaps m{};
         const bool kinetic = apply != nullptr && apply->kinetic_only;
-        if ((st = prepare_geometry<Lane>(op, batch, geo_base, tz, kinetic, &m, stream)) != CDFTB_OK) break;
-        if ((st = encode_lanes<Lane>(buf[2], nzp, ny, nx, lanes, tz, &m.phi, &m.prev)) != CDFTB_OK) break;
+        if ((st = prepare_geometry<Lane>(op, batch, geo_base, ty, tz, kinetic, &m, stream)) != CDFTB_OK) break;
+        if ((st = encode_lanes<Lane>(buf[2], nzp, ny, nx, lanes, ty, tz, &m.phi, &m.prev)) != CDFTB_OK) break;
         FilterArgs a = base_args(op, batch);
         if (apply) {
             a = *apply;
@@ -1502,7 +1619,7 @@ int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf
             a.out = buf[0];
             a.out_dtype = 0;
         }
-        const int64_t tiles = int64_t(ceil_div(ny, TY)) * ceil_div(nzp, tz);
+        const int64_t tiles = int64_t(ceil_div(ny, ty)) * ceil_div(nzp, tz);
         int chunks_list[5] = {1, 2, 3, 4, 0};
         chunks_list[4] = static_cast<int>(ceil_div(nx, choose_chunk(nx, tiles * lanes, sm_count())));
         for (int c = 0; c < 5 && st == CDFTB_OK; ++c) {
@@ -1510,9 +1627,9 @@ int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf
             if (chunks < 1 || (c == 4 && chunks <= 4)) continue;  // the heuristic's chunk, when not already tried
             const int xchunk = static_cast<int>(ceil_div(nx, chunks));
             if (chunks > 1 && (xchunk < 8 || ceil_div(nx, xchunk) != chunks)) continue;
-            if ((st = launch_tz<Lane>(tz, m, a, lanes, stream, xchunk)) != CDFTB_OK) break;
+            if ((st = launch_tz<Lane>(ty, tz, m, a, lanes, stream, xchunk)) != CDFTB_OK) break;
             if ((st = check(cudaEventRecord(e0, stream))) != CDFTB_OK) break;
-            for (int r = 0; r < 3 && st == CDFTB_OK; ++r) st = launch_tz<Lane>(tz, m, a, lanes, stream, xchunk);
+            for (int r = 0; r < 3 && st == CDFTB_OK; ++r) st = launch_tz<Lane>(ty, tz, m, a, lanes, stream, xchunk);
             if (st != CDFTB_OK) break;
             if ((st = check(cudaEventRecord(e1, stream))) != CDFTB_OK) break;
             if ((st = check(cudaEventSynchronize(e1))) != CDFTB_OK) break;
@@ -1520,7 +1637,7 @@ int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf
             if ((st = check(cudaEventElapsedTime(&ms, e0, e1))) != CDFTB_OK) break;
             if (best_ms < 0.0f || ms < best_ms) {
                 best_ms = ms;
-                *best = TileChoice{tz, xchunk};
+                *best = TileChoice{ty, tz, xchunk};
             }
         }
         if (st != CDFTB_OK) break;
@@ -1541,7 +1658,8 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
     void* buf[3] = {w, w + lanes * lane_bytes, w + 2 * lanes * lane_bytes};
     int st = pack_lanes<Lane>(op, block, in_dtype, batch, nx, ny, nz, nzp, lanes, buf[2], stream);
     if (st != CDFTB_OK) return st;
-    TileChoice choice{choose_tz(nzp), 0};
+    const Tile t0 = choose_tile<Lane>(ny, nzp);
+    TileChoice choice{t0.ty, t0.tz, 0};
     const TuneKey key = tune_key(op, lanes, Lane::WIDE);
     bool autotune;
     {
@@ -1555,13 +1673,14 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         g_tuned[key] = choice;
     }
-    const int tz = choice.tz;
+    const int ty = choice.ty, tz = choice.tz;
     FilterMaps geo_maps{};
-    if ((st = prepare_geometry<Lane>(op, batch, w + 3 * lanes * lane_bytes, tz, false, &geo_maps, stream)) != CDFTB_OK)
+    if ((st = prepare_geometry<Lane>(op, batch, w + 3 * lanes * lane_bytes, ty, tz, false, &geo_maps, stream)) !=
+        CDFTB_OK)
         return st;
     FilterMaps maps[3];
     for (int b = 0; b < 3; ++b)
-        if ((st = encode_lanes<Lane>(buf[b], nzp, ny, nx, lanes, tz, &maps[b].phi, &maps[b].prev)) != CDFTB_OK)
+        if ((st = encode_lanes<Lane>(buf[b], nzp, ny, nx, lanes, ty, tz, &maps[b].phi, &maps[b].prev)) != CDFTB_OK)
             return st;
     FilterArgs a = base_args(op, batch);
     a.coef = coefficients;
@@ -1579,7 +1698,7 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
         FilterMaps m = geo_maps;
         m.phi = maps[y].phi;
         m.prev = maps[prev >= 0 ? prev : y].prev;
-        if ((st = launch_tz<Lane>(tz, m, a, lanes, stream, choice.xchunk)) != CDFTB_OK) return st;
+        if ((st = launch_tz<Lane>(ty, tz, m, a, lanes, stream, choice.xchunk)) != CDFTB_OK) return st;
         prev = y;
         y = dst;
     }
@@ -1594,7 +1713,8 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
     const int64_t lanes = lane_count<Lane>(op, batch);
     const int64_t lane_bytes = int64_t(nx) * ny * nzp * lane_point_bytes<Lane>();
     char* w = static_cast<char*>(work);
-    TileChoice choice{choose_tz(nzp), 0};
+    const Tile t0 = choose_tile<Lane>(ny, nzp);
+    TileChoice choice{t0.ty, t0.tz, 0};
     const TuneKey key = tune_key(op, lanes, Lane::WIDE);
     const bool known = tuned_choice(key, &choice);
     int st = pack_lanes<Lane>(op, phi, in_dtype, batch, nx, ny, nz, nzp, lanes, w, stream);
@@ -1619,12 +1739,12 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         g_tuned[key] = choice;
     }
-    const int tz = choice.tz;
+    const int ty = choice.ty, tz = choice.tz;
     FilterMaps m{};
-    if ((st = prepare_geometry<Lane>(op, batch, w + lanes * lane_bytes, tz, kinetic_only != 0, &m, stream)) !=
+    if ((st = prepare_geometry<Lane>(op, batch, w + lanes * lane_bytes, ty, tz, kinetic_only != 0, &m, stream)) !=
         CDFTB_OK)
         return st;
-    if ((st = encode_lanes<Lane>(w, nzp, ny, nx, lanes, tz, &m.phi, &m.prev)) != CDFTB_OK) return st;
+    if ((st = encode_lanes<Lane>(w, nzp, ny, nx, lanes, ty, tz, &m.phi, &m.prev)) != CDFTB_OK) return st;
     FilterArgs a = base_args(op, batch);
     a.apply_only = 1;
     a.kinetic_only = kinetic_only != 0;
@@ -1632,7 +1752,7 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
     a.final_out = 1;
     a.out = out;
     a.out_dtype = out_dtype;
-    return launch_tz<Lane>(tz, m, a, lanes, stream, choice.xchunk);
+    return launch_tz<Lane>(ty, tz, m, a, lanes, stream, choice.xchunk);
 }
 
 // Wide lanes serve every filter and apply with one shared geometry (lanes need not follow orbital
@@ -1714,6 +1834,16 @@ extern "C" int cdftb_filter_tuned_tile(int nx, int ny, int nz, int dtype, int64_
     }
     *tile_z = c.tz;
     *x_chunk = c.xchunk;
+    return CDFTB_OK;
+}
+
+extern "C" int cdftb_filter_tuned_tile_rows(int nx, int ny, int nz, int dtype, int64_t lanes, int* tile_y) {
+    if (!tile_y || nx <= 0 || ny <= 0 || nz <= 0 || lanes <= 0) return CDFTB_ERR_ARGUMENT;
+    int dev = 0;
+    int st = cdftb::check(cudaGetDevice(&dev));
+    if (st != CDFTB_OK) return st;
+    cdftb::TileChoice c{};
+    *tile_y = cdftb::tuned_choice(cdftb::TuneKey(dev, nx, ny, nz, dtype, lanes), &c) ? c.ty : 0;
     return CDFTB_OK;
 }
 

@@ -111,13 +111,16 @@ int cdftb_chebyshev_filter(const cdftb_operator* op, const void* block, int in_d
  * fastest, and every later filter or apply launch for the key uses it. That first call synchronises
  * its stream (make it before any stream capture); results are bit-identical whatever the tiling. Disabled (the
  * default in the C library), heuristics choose the tiling. cdftb_filter_tuned_tile reports the
- * table's entry for a key (tile_z 32 or 36, x_chunk in planes; both 0 when the key is not tuned);
+ * table's entry for a key (tile_z 32, 36 or 24, x_chunk in planes; both 0 when the key is not tuned)
+ * and cdftb_filter_tuned_tile_rows its tile rows (8, or 13 for the wide kernel's 13 x 24 tile; 0 when
+ * not tuned);
  * dtype is CDFTB_F32 or CDFTB_F64 and lanes is the launch's lane count (cdftb_operator orbitals in
  * pairs for float32, one each for float64); for the wide-lane kernels (cdftb_filter_wide) dtype is
  * CDFTB_F32 + CDFTB_WIDE_LANES or CDFTB_F64 + CDFTB_WIDE_LANES and lanes counts four float32 or two
  * float64 orbitals each. */
 int cdftb_filter_autotune(int enable);
 int cdftb_filter_tuned_tile(int nx, int ny, int nz, int dtype, int64_t lanes, int* tile_z, int* x_chunk);
+int cdftb_filter_tuned_tile_rows(int nx, int ny, int nz, int dtype, int64_t lanes, int* tile_y);
 
 /* No reference counterpart: wide lanes for cdftb_chebyshev_filter and cdftb_cusp_apply. Enabled
  * (the default), every order-8 call with one shared geometry (no per-system geometry) runs a

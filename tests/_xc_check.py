@@ -12,11 +12,11 @@ the other's 1) the derivative terms of (1 -/+ zeta)^(1/3) are four orders larger
 they cancel to, so the host-to-device difference reaches a few 1e-12 of the n^(1/3) scale there.
 """
 
-DEVICE_STOL = 1e-11
-
 from __future__ import annotations
 
 import numpy as np
+
+DEVICE_STOL = 1e-11
 
 THRESHOLD = 1.0e-14
 SCALE_POWER = {"e": 4.0 / 3.0, "v": 1.0 / 3.0, "vs": -4.0 / 3.0}

@@ -214,7 +214,9 @@ def _scan_system(bond, spacing=0.4):
 def test_variational_nuclear_gradient_bare_h2plus(pkg, cuda):
     """dE/dR_a of H2+ (R = 2.6, h = 0.4) from the stationarity of the Lagrangian at the converged
     orbital (no re-solve) against central differences of converged energies (step 1e-4), to 1e-6
-    relative; the transverse components vanish by symmetry."""
+    relative on the bond axis and to 1e-6 of it on every other component. The grid is not symmetric
+    about the bond axis (26 points per transverse edge with the nuclei on a lattice line: 12 on one
+    side, 13 on the other), so the transverse components are small but not zero."""
     system = _scan_system(2.6)
     eigen = pkg.EigenConfig(residual_tol=1e-12)
     geo = _geometry(pkg, system, cuda)
@@ -235,8 +237,8 @@ def test_variational_nuclear_gradient_bare_h2plus(pkg, cuda):
     fd = pkg.adjoint.nuclear_gradient(energy_at, system.positions, delta=1e-4)
     assert abs(grad[1, 2]) > 1e-3
     np.testing.assert_allclose(grad[:, 2], fd[:, 2], rtol=1e-6, atol=0)
-    assert np.abs(grad[:, :2]).max() < 1e-9 and np.abs(fd[:, :2]).max() < 1e-7
-    assert abs(grad[0, 2] + grad[1, 2]) < 1e-8  # equal and opposite on the symmetric molecule
+    np.testing.assert_allclose(grad, fd, rtol=0, atol=1e-6 * abs(grad[1, 2]))
+    assert np.abs(grad[:, :2]).max() < 1e-2 * abs(grad[1, 2])  # small off the axis
 
 
 def test_variational_nuclear_gradient_interacting(pkg, cuda):

@@ -163,7 +163,7 @@ def test_autotuned_tiling_is_bit_identical(pkg, cuda, dtype):
         lib.cdftb_filter_autotune(1)
         tuned = pkg.chebyshev_filter(ham, block, 6, 0.5, 3.0, -1.0)
         assert lib.cdftb_filter_tuned_tile(*shape, code, lanes, ctypes.byref(tz), ctypes.byref(xc)) == 0
-        assert tz.value in (32, 36) and 1 <= xc.value <= shape[0]
+        assert tz.value in (24, 32, 36) and 1 <= xc.value <= shape[0]
         again = pkg.chebyshev_filter(ham, block, 6, 0.5, 3.0, -1.0)
     finally:
         lib.cdftb_filter_autotune(1)
@@ -186,7 +186,7 @@ def test_autotuned_apply_is_bit_identical(pkg, cuda):
         lib.cdftb_filter_autotune(1)
         tuned = ham.apply(block)
         assert lib.cdftb_filter_tuned_tile(*shape, 0 + 16, 2, ctypes.byref(tz), ctypes.byref(xc)) == 0
-        assert tz.value in (32, 36) and 1 <= xc.value <= shape[0]
+        assert tz.value in (24, 32, 36) and 1 <= xc.value <= shape[0]
     finally:
         lib.cdftb_filter_autotune(1)
     assert torch.equal(tuned, heuristic)
@@ -233,6 +233,39 @@ def test_wide_lanes_many_systems(pkg, cuda, shape, dtype):
         np.testing.assert_allclose(wide[s], want, rtol=0, atol=tol * np.abs(want).max())
     np.testing.assert_allclose(wide, narrow, rtol=0, atol=tol * np.abs(narrow).max())
     assert not np.array_equal(wide, narrow)  # the wide kernel ran (its sums run in another order)
+    assert _device_status(pkg) == (0, 0)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("shape", [(14, 13, 23), (11, 26, 47)])
+def test_wide_tile_of_13_rows(pkg, cuda, shape, dtype):
+    """The 13 x 24 tile of the wide kernel: 13 and 26 rows, nzp 24 and 48. With the autotuner off the
+    heuristic takes the tile with the fewest padded points, 13 x 24 here (8 x 32 and 8 x 36 pad the
+    rows to 16 or 32 and z to 32, 36, 64 or 72); against the oracle, and the autotuner's choice (8 or
+    13 rows) bit for bit the same."""
+    n = int(np.prod(shape))
+    faces, inv, q = _random_operator(shape, seed=51)
+    pot = np.random.default_rng(52).standard_normal(n)
+    ham_o, ham = _pair(pkg, cuda, shape, 0.3, faces, inv, q, pot, dtype=dtype)
+    block = np.random.default_rng(53).standard_normal((6, n))
+    lib = pkg._lib.library()
+    code = (1 if dtype == torch.float32 else 0) + 16
+    lanes = 2 if dtype == torch.float32 else 3
+    rows = ctypes.c_int(-1)
+    tol = 2e-5 if dtype == torch.float32 else 1e-12
+    try:
+        lib.cdftb_filter_autotune(0)
+        heuristic = pkg.chebyshev_filter(ham, _t(block, cuda), 5, 0.5, 3.0, -1.0)
+        lib.cdftb_filter_autotune(1)
+        tuned = pkg.chebyshev_filter(ham, _t(block, cuda), 5, 0.5, 3.0, -1.0)
+        assert lib.cdftb_filter_tuned_tile_rows(*shape, code, lanes, ctypes.byref(rows)) == 0
+        assert rows.value in (8, 13)
+    finally:
+        lib.cdftb_filter_autotune(1)
+    want = np.stack([oeigen.chebyshev_filter(ham_o, b, 5, 0.5, 3.0, -1.0) for b in block[:2]])
+    got = heuristic.cpu().numpy()
+    np.testing.assert_allclose(got[:2], want, rtol=0, atol=tol * np.abs(want).max())
+    assert torch.equal(tuned, heuristic)
     assert _device_status(pkg) == (0, 0)
 
 

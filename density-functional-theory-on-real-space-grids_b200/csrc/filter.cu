@@ -58,7 +58,6 @@ static_assert((RY & (RY - 1)) == 0, "result slots are a power of 2");
 constexpr int NG = 2;     // pass warp groups; planes alternate between them
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
 static_assert(R % NG == 0 && RY % NG == 0, "a slot is always served by the same pass group");
-constexpr unsigned kSuspendNs = 20000;  // try_wait suspend hint: a waiting warp sleeps instead of spinning
 constexpr unsigned kNapNs = 256;        // longest sleep between tries of the wide kernel's producer and pass groups
 
 constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
@@ -189,10 +188,10 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(bar), "r"(parity), "r"(kSuspendNs)
+        : "r"(bar), "r"(parity)
         : "memory");
     return done != 0;
 }
@@ -238,6 +237,15 @@ __device__ __forceinline__ bool wait_full(unsigned bar, unsigned parity, unsigne
 // makes the warp leave together, so no lane waits in __syncwarp for an exited one).
 __device__ __forceinline__ bool warp_wait(unsigned bar, unsigned parity, unsigned token, unsigned nap_ns = 0) {
     return __all_sync(0xffffffffu, wait_full(bar, parity, token, nap_ns)) != 0;
+}
+
+// warp_wait with a warp-uniform fast path: one try and one vote when the phase is complete for
+// every lane; otherwise the whole warp takes the bounded wait together. No branch around the wait
+// depends on a lane's own value, so the caller's code needs no divergence handling for it.
+__device__ __forceinline__ bool warp_wait_uniform(unsigned bar, unsigned parity, unsigned token,
+                                                  unsigned nap_ns = 0) {
+    if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+    return __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity, kWaitLimitNs, token, nap_ns)) != 0;
 }
 
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
@@ -664,8 +672,11 @@ struct WideD2 {  // two float64 orbitals
     }
 };
 
-constexpr int RW = 4;  // plane slots of the wide kernel (16-byte elements: a slot is 34-40 KB)
-static_assert(RW % NG == 0, "a slot is always served by the same pass group");
+// Plane slots of the wide kernel (16-byte elements: a slot is 31-41 KB): as many as shared memory
+// holds beside a result ring of at least 4, up to kWideMaxSlots. A deeper ring keeps more copies in
+// flight per SM, which is what hides the copies' latency behind the march.
+constexpr int kWideMaxSlots = 6;
+constexpr size_t kWideSmem = 232448;  // the opt-in shared memory of one CTA
 
 template <int TYW, int TZ, int SB, int ORB>  // TYW: tile rows; SB: bytes of a geometry element; ORB: potentials per lane
 struct WideShape {
@@ -702,16 +713,27 @@ struct WideShape {
     static constexpr size_t O_POT = O_INV + align128(TX_INV);  // ORB potentials, POT_STEP apart
     static constexpr size_t POT_STEP = align128(TX_POT);
     static constexpr size_t SLOT = O_POT + ORB * POT_STEP;
-    static constexpr size_t O_YZ = RW * SLOT;
     static constexpr size_t YZ_Z = size_t(TYW) * TZ * EB;
     static constexpr size_t YZ_SLOT = align128(YZ_Z + size_t(TYW) * ZROW * EB);
+    static constexpr size_t need(int rw, int ry) { return rw * SLOT + ry * YZ_SLOT + (2 * rw + 2 * ry) * 8; }
+    static constexpr int slots() {
+        int rw = kWideMaxSlots;
+        while (rw > 2 && need(rw, 4) > kWideSmem) --rw;
+        return rw;
+    }
+    static constexpr int RWS = slots();
     // y+z result slots: the march adds a plane's y+z part when that output completes, 7 planes after
-    // the pass formed it, so the ring is as deep as shared memory allows (8, else 6, else 4)
-    static constexpr size_t fits(int ry) { return O_YZ + ry * YZ_SLOT + (2 * RW + 2 * ry) * 8 <= 232448; }
-    static constexpr int RYW = fits(8) ? 8 : fits(6) ? 6 : 4;
+    // the pass formed it, so the result ring takes what is left, up to 8 (at least 4)
+    static constexpr int result_slots() {
+        int ry = 8;
+        while (ry > 4 && need(RWS, ry) > kWideSmem) --ry;
+        return ry;
+    }
+    static constexpr int RYW = result_slots();
+    static constexpr size_t O_YZ = RWS * SLOT;
     static constexpr size_t O_BAR = O_YZ + RYW * YZ_SLOT;
-    static constexpr size_t BYTES = O_BAR + (2 * RW + 2 * RYW) * 8;
-    static_assert(RYW % NG == 0, "a result slot is always served by the same pass group");
+    static constexpr size_t BYTES = O_BAR + (2 * RWS + 2 * RYW) * 8;
+    static_assert(RWS >= NG && need(RWS, RYW) <= kWideSmem, "the rings fit one CTA's shared memory");
     static_assert(TZ >= TYW && TZ % 4 == 0, "z segments of TYW inside the tile; 16-byte float32 geometry rows");
     static_assert(BW % 2 == 1 && ZROW % 2 == 1, "odd row pitches");
     static_assert((TZ - TYW) + NROWW <= BW - 1, "the last z segment's nodes lie inside the phi box");
@@ -741,6 +763,7 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
     constexpr int BW = SH::BW;
     extern __shared__ __align__(1024) unsigned char smem[];
     const unsigned bar_full = smem_u32(smem + SH::O_BAR);
+    constexpr int RW = SH::RWS;  // plane slots (planes n and n + RW share a slot)
     const unsigned bar_empty = bar_full + 8 * RW;
     const unsigned bar_yfull = bar_empty + 8 * RW;
     const unsigned bar_yempty = bar_yfull + 8 * SH::RYW;
@@ -861,7 +884,7 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
         }
         int s = pg, ph = 0;
         for (int n = pg; n < npl; n += NG) {
-            if (!warp_wait(bar_full + 8 * s, ph, a.token, kNapNs)) return;
+            if (!warp_wait_uniform(bar_full + 8 * s, ph, a.token, kNapNs)) return;
             const int q = q0 + n;
             if (q >= xa && q <= xe) {
                 E acc[TY];
@@ -898,7 +921,7 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
                 const int m = q - xa;
                 const int ys = m % SH::RYW;
                 const unsigned uy = m / SH::RYW;
-                if (uy >= 1 && !warp_wait(bar_yempty + 8 * ys, (uy - 1) & 1, a.token, kNapNs)) return;
+                if (uy >= 1 && !warp_wait_uniform(bar_yempty + 8 * ys, (uy - 1) & 1, a.token, kNapNs)) return;
                 if (active) {
                     E* out = reinterpret_cast<E*>(smem + SH::O_YZ + ys * SH::YZ_SLOT) + ob;
 #pragma unroll
@@ -955,13 +978,15 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
         acc[j] = W::zero();
     }
 
-    int s = 0, sph = 0;
+    const int own_off = y * nzp + z;  // this thread's point within a plane of the lane buffer
+    int s = 0, sph = 0;   // plane slot and its phase parity
+    int ys = 0, yph = 0;  // result slot of the next output completed, and its phase parity
     for (int n0 = 0; n0 < npl; n0 += 8) {
 #pragma unroll
         for (int g = 0; g < 8; ++g) {
             const int n = n0 + g;
             if (n >= npl) break;
-            if (!warp_wait(bar_full + 8 * s, sph, a.token)) return;
+            if (!warp_wait_uniform(bar_full + 8 * s, sph, a.token)) return;
             const unsigned char* slot = smem + s * SH::SLOT;
             const int q = q0 + n;
             phq[g] = reinterpret_cast<const E*>(slot + SH::O_PHI)[(ty + HALO) * BW + tz + 8];
@@ -972,53 +997,51 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
 #pragma unroll
                 for (int j = 1; j < 4; ++j)
                     sum = W::fmat(tap(j), W::sub(phq[(g + 1 + j) & 7], phq[(g + 8 - j) & 7]), sum);
-                const S wx = own_in ? reinterpret_cast<const S*>(slot + SH::O_W0)[own] : S(0);
+                // outside the grid the weight is the copy's zero fill (an idle thread's face is
+                // never stored)
+                const S wx = reinterpret_cast<const S*>(slot + SH::O_W0)[own];
                 face = W::mult(W::splat(wx), sum);  // x face q - 4
             }
             // the face reaches the open outputs q - 7 .. q (slot (g - d) & 7 holds output q - d, tap 7 - d)
 #pragma unroll
             for (int d = 1; d < 8; ++d) acc[(g - d) & 7] = W::fmat_k(tap4, 7 - d, face, acc[(g - d) & 7]);
             const int i = q - HALO;  // output complete at this plane (slot (g + 1) & 7)
-            E yz = W::zero();
             if (i >= xa) {
                 // the y+z part of output i, formed by a pass group 7 planes ago
-                const int m = i - xa;
-                const int ys = m % SH::RYW;
-                if (!warp_wait(bar_yfull + 8 * ys, (m / SH::RYW) & 1, a.token)) return;
+                if (!warp_wait_uniform(bar_yfull + 8 * ys, yph, a.token)) return;
                 const unsigned char* yzs = smem + SH::O_YZ + ys * SH::YZ_SLOT;
-                yz = W::add(reinterpret_cast<const E*>(yzs)[own],
-                            reinterpret_cast<const E*>(yzs + SH::YZ_Z)[ty * SH::ZROW + tz]);
+                const E yz = W::add(reinterpret_cast<const E*>(yzs)[own],
+                                    reinterpret_cast<const E*>(yzs + SH::YZ_Z)[ty * SH::ZROW + tz]);
                 __syncwarp();
                 if ((t & 31) == 0) mbar_arrive(bar_yempty + 8 * ys);
-            }
-            if (i >= xa && own_pad) {
+                if (++ys == SH::RYW) {
+                    ys = 0;
+                    yph ^= 1;
+                }
+                // every thread forms a result (the idle ones from their tile's first point); only
+                // the stores depend on the thread, so no branch here does
                 const E div = W::add(acc[(g + 1) & 7], yz);
-                const int64_t pt = int64_t(i) * plane_n + (own_in ? int64_t(y) * nz + z : 0);
-                E res = W::zero();
-                if (own_in) {
-                    const E phi = phq[(g + 1) & 7];
-                    const S inv = reinterpret_cast<const S*>(slot + SH::O_INV)[own];
-                    const E kin = W::mult(W::splat(S(0.5) * inv), div);
-                    if (a.kinetic_only) {
-                        res = kin;
-                    } else {
-                        S pv[ORB];
+                const E phi = phq[(g + 1) & 7];
+                const S inv = reinterpret_cast<const S*>(slot + SH::O_INV)[own];
+                E res = W::mult(W::splat(S(0.5) * inv), div);
+                if (!a.kinetic_only) {
+                    S pv[ORB];
 #pragma unroll
-                        for (int h = 0; h < ORB; ++h)
-                            pv[h] = reinterpret_cast<const S*>(slot + SH::O_POT + h * SH::POT_STEP)[own];
-                        const E potv = W::make(pv);
-                        const E applied = W::fma(phi, potv, kin);
-                        if (a.apply_only) {
-                            res = applied;
-                        } else {
-                            res = W::mul(W::fma(W::neg(cc), phi, applied), ca);
-                            if (has_prev)
-                                res = W::fma(W::neg(cb), reinterpret_cast<const E*>(slot + SH::O_PREV)[own], res);
-                        }
+                    for (int h = 0; h < ORB; ++h)
+                        pv[h] = reinterpret_cast<const S*>(slot + SH::O_POT + h * SH::POT_STEP)[own];
+                    const E applied = W::fma(phi, W::make(pv), res);
+                    if (a.apply_only) {
+                        res = applied;
+                    } else {
+                        res = W::mul(W::fma(W::neg(cc), phi, applied), ca);
+                        if (has_prev)
+                            res = W::fma(W::neg(cb), reinterpret_cast<const E*>(slot + SH::O_PREV)[own], res);
                     }
                 }
+                res = own_in ? res : W::zero();  // the padding column stays zero
                 if (a.final_out) {
                     if (own_in) {
+                        const int64_t pt = int64_t(i) * plane_n + int64_t(y) * nz + z;
                         S rv[ORB];
                         W::parts(res, rv);
 #pragma unroll
@@ -1026,9 +1049,9 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
                             if (orb0 + h < a.batch)
                                 store_as<S>(a.out, a.out_dtype, (orb0 + h) * (plane_n * nx) + pt, rv[h]);
                     }
-                } else {
-                    E* out = static_cast<E*>(a.out);
-                    out[(int64_t(lane) * nx + i) * (int64_t(ny) * nzp) + int64_t(y) * nzp + z] = res;
+                } else if (own_pad) {
+                    // the plane's offset is the same for the whole CTA (uniform arithmetic)
+                    static_cast<E*>(a.out)[(int64_t(lane) * nx + i) * (int64_t(ny) * nzp) + own_off] = res;
                 }
             }
             // the newest output, q, opens with its first face (its slot held output q - 8, completed

@@ -30,7 +30,7 @@ class Operator(ctypes.Structure):
         ("nx", c_int), ("ny", c_int), ("nz", c_int), ("accuracy", c_int), ("spacing", c_double),
         ("dtype", c_int), ("face_weights", c_void_p * 3), ("inverse_weight", c_void_p),
         ("potential", c_void_p), ("potential_stride", c_int64), ("orbitals_per_group", c_int),
-        ("quadrature", c_void_p), ("per_system_geometry", c_int),
+        ("quadrature", c_void_p), ("per_system_geometry", c_int), ("system_shapes", c_void_p),
     ]
 
 
@@ -109,6 +109,9 @@ SIGNATURES: dict[str, tuple] = {
     "cdftb_quadrature_many_scratch_bytes": (c_int64, [c_int64, c_int64]),
     "cdftb_quadrature_interpolate_many_f64": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p, c_int,
                                                       c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p]),
+    "cdftb_quadrature_interpolate_grouped_f64": (c_int, [c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p,
+                                                         c_void_p, c_int64, c_void_p, c_int, c_int64, c_void_p,
+                                                         c_int64, c_void_p, c_int64, c_void_p]),
     "cdftb_lift_segments_capacity": (c_int64, [c_int64, c_int64]),
     "cdftb_lift_segments_scratch_bytes": (c_int64, [c_int64]),
     "cdftb_lift_plan_segments": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int64, c_void_p, c_int64,

@@ -1102,6 +1102,8 @@ class MultiGeometryHamiltonian:
                 self.embed_into(self._inv64[s], s, inv)
                 self.embed_into(self.potentials[s], s, pot)
                 self.embed_into(self.q[s], s, measure.quadrature)
+            # each system's own grid: the kernel's tiles wholly beyond it store zeros without work
+            self._shapes = torch.tensor(self.shapes, dtype=torch.int32, device=first.device).contiguous()
         else:
             raise ValueError("use subset() to select systems")
         self.dtype = dtype
@@ -1162,6 +1164,7 @@ class MultiGeometryHamiltonian:
         op.orbitals_per_group = int(k)
         op.quadrature = self.q.data_ptr()
         op.per_system_geometry = 1
+        op.system_shapes = self._shapes.data_ptr()
         return op
 
     apply = BatchedHamiltonian.apply
@@ -1176,6 +1179,7 @@ class MultiGeometryHamiltonian:
         sub.potentials = self.potentials.index_select(0, idx).contiguous()
         sub.q = self.q.index_select(0, idx).contiguous()
         sub.shapes = [self.shapes[i] for i in index]
+        sub._shapes = self._shapes.index_select(0, idx).contiguous()
         sub.geometries = [self.geometries[i] for i in index]
         sub._cast()
         sub.applications = 0

@@ -148,6 +148,7 @@ struct FilterArgs {
     unsigned token;        // this launch's abort token (never 0)
     int apply_only;        // out = A phi (no recurrence; coef unused)
     int per_system_geometry;  // face weights and h^3/omega per orbital group (systems on their own grids)
+    const int* system_shapes;  // with per_system_geometry: each group's own grid (nx, ny, nz), or null
     int lanes_per_group;      // > 0: lanes aligned to orbital groups (lane l holds group l / lanes_per_group)
     int kinetic_only;      // with apply_only: out = 0.5 (h^3/omega) div phi (no potential)
     int stop_after_planes;  // > 0 only in the timeout test: the producer issues this many planes' copies
@@ -312,6 +313,36 @@ __global__ void __launch_bounds__(Shape<TZ, sizeof(typename Lane::S)>::T, 1)
     const int g0 = a.shared_potential ? 0 : static_cast<int>(o0 / a.orb_per_group);
     const int g1 = a.shared_potential ? 0 : static_cast<int>(o1 / a.orb_per_group);
     const int gg = a.per_system_geometry ? static_cast<int>(o0 / a.orb_per_group) : 0;
+
+    // Systems on their own grids: a tile wholly beyond its lane's system (every point zero in every
+    // iterate: zero face weights, h^3/omega and potential there) stores its zeros and computes
+    // nothing; an empty lane stores zeros too. The whole CTA leaves before any barrier is used.
+    if (a.system_shapes != nullptr) {
+        const int* shape = a.system_shapes + 3 * (o0 >= 0 ? gg : 0);
+        if (o0 < 0 || xa >= shape[0] || y0 >= shape[1] || z0 >= shape[2]) {
+            const int64_t plane_n = int64_t(ny) * nz;
+            for (int k = t; k < (xe - xa + 1) * TY * TZ; k += blockDim.x) {
+                const int i = xa + k / (TY * TZ);
+                const int r = k % (TY * TZ);
+                const int y = y0 + r / TZ, z = z0 + r % TZ;
+                if (y >= ny || z >= nzp) continue;
+                if (a.final_out) {
+                    if (z >= nz) continue;
+                    const int64_t pt = int64_t(i) * plane_n + int64_t(y) * nz + z;
+                    if constexpr (Lane::ORBITALS == 2) {
+                        if (o0 >= 0) store_as<float>(a.out, a.out_dtype, o0 * (plane_n * nx) + pt, 0.0f);
+                        if (o1s >= 0) store_as<float>(a.out, a.out_dtype, o1s * (plane_n * nx) + pt, 0.0f);
+                    } else {
+                        if (o0 >= 0) store_as<double>(a.out, a.out_dtype, o0 * (plane_n * nx) + pt, 0.0);
+                    }
+                } else {
+                    static_cast<E*>(a.out)[(int64_t(lane) * nx + i) * (int64_t(ny) * nzp) + int64_t(y) * nzp + z] =
+                        Lane::zero();
+                }
+            }
+            return;
+        }
+    }
 
     if (t == 0) {
         for (int s = 0; s < R; ++s) {
@@ -1423,6 +1454,7 @@ FilterArgs base_args(const cdftb_operator* op, int64_t batch) {
     a.orb_per_group = op->orbitals_per_group;
     a.shared_potential = op->potential_stride == 0;
     a.per_system_geometry = op->per_system_geometry != 0;
+    a.system_shapes = op->per_system_geometry ? op->system_shapes : nullptr;
     a.lanes_per_group = aligned_lanes_per_group(op);
     const StaggeredTaps taps = staggered_taps(8);
     const double scale = 1.0 / op->spacing;  // taps c_k * (1/h), divergence.py:112, 121

@@ -335,6 +335,68 @@ __global__ void __launch_bounds__(256) interpolate_many_kernel(const int* __rest
     store_tile(tile, j0, m, nf, out, out_stride);
 }
 
+// The interpolant for nodes grouped by their base cell: the nodes of a group read the same 8 x 8 x 8
+// box, so one warp reads each box row once for up to GROUP_BATCH nodes (a cell near a nucleus holds
+// ~6 nodes at He 65^3) instead of once per node. Each node's sums run in the same order as in
+// interpolate_many_kernel (z, then y, then x, each a chain of fmas from zero), so the results are the
+// same bit for bit. One warp per group, lanes over the fields of the row layout.
+constexpr int GROUP_BATCH = 4;
+
+__global__ void __launch_bounds__(256, 2) interpolate_grouped_kernel(const int* __restrict__ base,
+                                                                  const double* __restrict__ w1d,
+                                                                  const int* __restrict__ group_nodes,
+                                                                  const int* __restrict__ group_ptr, int64_t groups,
+                                                                  int ny, int nz, const double* __restrict__ rows,
+                                                                  int nf, double* __restrict__ out,
+                                                                  int64_t out_stride) {
+    const int lane = threadIdx.x & 31;
+    const int64_t g = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (g >= groups) return;
+    const int first = group_ptr[g], last = group_ptr[g + 1];
+    const int lead = group_nodes[first];
+    const int bx = base[lead * 3 + 0] - HALFD, by = base[lead * 3 + 1] - HALFD, bz = base[lead * 3 + 2] - HALFD;
+    for (int b0 = first; b0 < last; b0 += GROUP_BATCH) {
+        const int count = last - b0 < GROUP_BATCH ? last - b0 : GROUP_BATCH;
+        int node[GROUP_BATCH];
+        double wz[GROUP_BATCH][KTAP], acc[GROUP_BATCH];
+#pragma unroll
+        for (int j = 0; j < GROUP_BATCH; ++j) {
+            node[j] = group_nodes[b0 + (j < count ? j : 0)];  // a short batch repeats its first node
+            const double* w = w1d + int64_t(node[j]) * 24;
+#pragma unroll
+            for (int c = 0; c < KTAP; ++c) wz[j][c] = __ldg(w + 16 + c);
+            acc[j] = 0.0;
+        }
+        for (int a = 0; a < KTAP; ++a) {
+            const double* plane = rows + (int64_t(bx + a) * ny + by) * int64_t(nz) * MANY + int64_t(bz) * MANY + lane;
+            double sa[GROUP_BATCH];
+#pragma unroll
+            for (int j = 0; j < GROUP_BATCH; ++j) sa[j] = 0.0;
+#pragma unroll 1
+            for (int b = 0; b < KTAP; ++b) {
+                const double* row = plane + int64_t(b) * nz * MANY;
+                double v[KTAP];
+#pragma unroll
+                for (int c = 0; c < KTAP; ++c) v[c] = row[c * MANY];
+#pragma unroll
+                for (int j = 0; j < GROUP_BATCH; ++j) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int c = 0; c < KTAP; ++c) t = fma(wz[j][c], v[c], t);
+                    sa[j] = fma(__ldg(w1d + int64_t(node[j]) * 24 + 8 + b), t, sa[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < GROUP_BATCH; ++j) acc[j] = fma(__ldg(w1d + int64_t(node[j]) * 24 + a), sa[j], acc[j]);
+        }
+        if (lane < nf) {
+#pragma unroll
+            for (int j = 0; j < GROUP_BATCH; ++j)
+                if (j < count) out[lane * out_stride + node[j]] = acc[j];
+        }
+    }
+}
+
 int fields_to_rows(const double* src, int nf, int64_t stride, int64_t n, double* dst, cudaStream_t s) {
     fields_to_rows_kernel<<<static_cast<unsigned>(ceil_div(n, MANY)), dim3(MANY, 8), 0, s>>>(src, nf, stride, n, dst);
     return check_launch();
@@ -371,6 +433,31 @@ extern "C" int cdftb_quadrature_interpolate_many_f64(const int* base, const doub
         if (st != CDFTB_OK) return st;
         cdftb::interpolate_many_kernel<<<static_cast<unsigned>(ceil_div(m, cdftb::MANY)), 256, 0, s>>>(
             base, w1d, m, ny, nz, rows, count, out + f0 * out_stride, out_stride);
+        st = check_launch();
+        if (st != CDFTB_OK) return st;
+    }
+    return CDFTB_OK;
+}
+
+extern "C" int cdftb_quadrature_interpolate_grouped_f64(const int* base, const double* w1d, int64_t m, int nx,
+                                                        int ny, int nz, const int* group_nodes, const int* group_ptr,
+                                                        int64_t groups, const double* fields, int nf,
+                                                        int64_t field_stride, double* out, int64_t out_stride,
+                                                        void* scratch, int64_t scratch_bytes, cdftb_stream_t stream) {
+    const int64_t n_points = int64_t(nx) * ny * nz;
+    if (m < 0 || nf < 1 || n_points <= 0 || groups < 0 || groups > m ||
+        (m > 0 && (!base || !w1d || !group_nodes || !group_ptr || !fields || !out || !scratch)))
+        return CDFTB_ERR_ARGUMENT;
+    if (scratch_bytes < n_points * cdftb::MANY * 8) return CDFTB_ERR_ARGUMENT;
+    if (m == 0 || groups == 0) return CDFTB_OK;
+    cudaStream_t s = as_stream(stream);
+    double* rows = static_cast<double*>(scratch);
+    for (int f0 = 0; f0 < nf; f0 += cdftb::MANY) {
+        const int count = nf - f0 < cdftb::MANY ? nf - f0 : cdftb::MANY;
+        int st = cdftb::fields_to_rows(fields + f0 * field_stride, count, field_stride, n_points, rows, s);
+        if (st != CDFTB_OK) return st;
+        cdftb::interpolate_grouped_kernel<<<static_cast<unsigned>(ceil_div(groups, 8)), 256, 0, s>>>(
+            base, w1d, group_nodes, group_ptr, groups, ny, nz, rows, count, out + f0 * out_stride, out_stride);
         st = check_launch();
         if (st != CDFTB_OK) return st;
     }

@@ -65,6 +65,11 @@ typedef struct cdftb_operator {
     int orbitals_per_group;
     const double* quadrature;
     int per_system_geometry;
+    /* With per_system_geometry: each orbital group's own grid (nx, ny, nz), 3 ints per group in
+     * device memory, or NULL. A system sits at the low corner of the operator's box and is zero
+     * beyond its own grid; the slab kernel's CTAs whose tile lies wholly beyond it store zeros and
+     * compute nothing. No reference counterpart: the reference solves one grid at a time. */
+    const int* system_shapes;
 } cdftb_operator;
 
 /* (a1) out = sum_d D_d^T [w_d D_d box], f64, batched.
@@ -343,6 +348,16 @@ int cdftb_quadrature_interpolate_many_f64(const int* base, const double* w1d, in
                                           const double* fields, int nf, int64_t field_stride, double* out,
                                           int64_t out_stride, void* scratch, int64_t scratch_bytes,
                                           cdftb_stream_t stream);
+/* The many-field interpolant with the nodes grouped by base cell: group_nodes (m node indices,
+ * grouped) and group_ptr (groups + 1 offsets) list the nodes of each cell; the nodes of a group
+ * read the same 8 x 8 x 8 box, which one warp reads once per four of them. Results equal
+ * cdftb_quadrature_interpolate_many_f64's bit for bit; the same scratch. No reference counterpart
+ * (the reference multiplies by its CSR matrix L, quadrature.py:613-620). */
+int cdftb_quadrature_interpolate_grouped_f64(const int* base, const double* w1d, int64_t m, int nx, int ny, int nz,
+                                             const int* group_nodes, const int* group_ptr, int64_t groups,
+                                             const double* fields, int nf, int64_t field_stride, double* out,
+                                             int64_t out_stride, void* scratch, int64_t scratch_bytes,
+                                             cdftb_stream_t stream);
 int cdftb_quadrature_lift_many_f64(const long long* row_ptr, const int* col, const double* values, const int* seg_ptr,
                                    const int* seg_row, int64_t seg_capacity, int nx, int ny, int nz, int64_t m,
                                    const double* node_values, int nf, int64_t x_stride, double* out,

@@ -99,6 +99,46 @@ def test_filter_vjp_is_the_transpose(pkg, he25, cuda, dtype):
     assert abs(lhs - rhs) <= tol * abs(lhs)
 
 
+def test_composed_gradient_central_differences(pkg, he25, cuda):
+    """The VJPs composed into one end-to-end gradient: a scalar through the filter, the apply, the
+    Poisson solve and the XC energy, E(phi, alpha) = <Y, A(V0 + alpha g) Y> + (1/2) <rho, G rho> h^3
+    + E_xc[rho + 0.01] with Y = p(A) phi and rho = sum of Y^2, differentiated by autograd through
+    the hand-written backward passes, against central differences along a random direction in
+    (phi, alpha), to 1e-7 relative."""
+    _, geo = he25
+    ham = pkg.CuspFactoredHamiltonian(geo.grid, geo.factor, quadrature=geo.quadrature)
+    solver = pkg.CoulombCutoffPoisson(geo.grid, pad_factor=2.5)
+    n = geo.grid.n_points
+    h3 = geo.grid.spacing ** 3
+    v0 = ham.graph_potential()
+    g = torch.exp(-(geo.grid.points() ** 2).sum(dim=1) / 4.0)  # a smooth external perturbation
+    w = torch.full((n,), h3, dtype=torch.float64, device=cuda)
+    phi0 = _rand((2, n), 21, cuda)
+    phi0 = phi0 / phi0.norm(dim=1, keepdim=True)
+
+    def energy(phi, alpha):
+        y = pkg.adjoint.ChebyshevFilter.apply(phi, ham, 4, 2.0, 60.0, -3.0)
+        ay = pkg.adjoint.CuspApply.apply(y, v0 + alpha * g, ham)
+        rho = (y * y).sum(dim=0)
+        e_band = (y * ay).sum()
+        e_h = 0.5 * (rho * pkg.adjoint.PoissonSolve.apply(rho, solver)).sum() * h3
+        e_xc = pkg.adjoint.XCEnergy.apply(rho + 0.01, w, "lda_vwn")
+        return e_band + e_h + e_xc
+
+    phi = phi0.clone().requires_grad_(True)
+    alpha = torch.tensor(0.05, dtype=torch.float64, device=cuda, requires_grad=True)
+    energy(phi, alpha).backward()
+    d_phi, d_alpha = _rand((2, n), 22, cuda) * 1e-2, 0.3
+    eps = 1e-4
+    with torch.no_grad():
+        plus = energy(phi0 + eps * d_phi, alpha.detach() + eps * d_alpha)
+        minus = energy(phi0 - eps * d_phi, alpha.detach() - eps * d_alpha)
+    fd = float((plus - minus) / (2 * eps))
+    ad = float((phi.grad * d_phi).sum() + alpha.grad * d_alpha)
+    assert abs(ad) > 1e-6
+    assert abs(fd - ad) <= 1e-7 * abs(ad), (fd, ad)
+
+
 def _solve(pkg, step, tight=True):
     scf = pkg.SCFConfig(energy_tol=1e-11, density_tol=1e-8, max_iterations=400) if tight else None
     out = pkg.solve_self_consistent(step, pkg.MixingConfig(scheme="linear", alpha=0.3), scf)

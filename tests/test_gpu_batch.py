@@ -62,8 +62,12 @@ def _scan_geometry(pkg, cuda, bond, spacing=0.25, transverse=12.0):
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
 def test_multi_grid_filter_matches_single_grids(pkg, cuda, dtype):
-    """One launch over systems of different nz equals the per-system filters."""
-    geos = [_scan_geometry(pkg, cuda, bond, spacing=0.4, transverse=10.0) for bond in (0.8, 2.6, 4.1)]
+    """One launch over systems of different grids (26 x 26 x 33, 26 x 26 x 37, 33 x 33 x 41) equals the
+    per-system filters; the tiles wholly beyond a system's own grid (rows from 32 on for the 26-row
+    systems) store zeros without computing, and the result equals the launch that computes them (no
+    system shapes given)."""
+    geos = [_scan_geometry(pkg, cuda, bond, spacing=0.4, transverse=t)
+            for bond, t in ((0.8, 10.0), (2.6, 10.0), (4.1, 12.8))]
     assert len({g.grid.shape for g in geos}) == 3
     h = pkg.batch.MultiGeometryHamiltonian(geos)
     if dtype == torch.float32:
@@ -86,7 +90,19 @@ def test_multi_grid_filter_matches_single_grids(pkg, cuda, dtype):
         outside = got[s].reshape(-1, *h.grid.shape)
         sx, sy, sz = g.grid.shape
         assert float(outside[:, sx:].abs().max() if sx < h.grid.shape[0] else 0.0) == 0.0
+        assert float(outside[:, :, sy:].abs().max() if sy < h.grid.shape[1] else 0.0) == 0.0
         assert float(outside[:, :, :, sz:].abs().max() if sz < h.grid.shape[2] else 0.0) == 0.0
+    assert min(s[1] for s in h.shapes) <= 32 < h.grid.shape[1]
+
+    class Unshaped(type(h)):
+        def _op(self, k):
+            op = super()._op(k)
+            op.system_shapes = None
+            return op
+
+    full = Unshaped.__new__(Unshaped)
+    full.__dict__.update(h.__dict__)
+    assert torch.equal(full.filter(big, table, degree), got)
 
 
 SCAN = tuple(0.8 + k * 5.2 / 47 for k in (0, 11, 23, 35, 47))

@@ -216,6 +216,15 @@ def test_interpolate_and_lift_many_fields(pkg, he25, cuda, nf):
         one_l = quad._lift_raw(nodes[f:f + 1].contiguous(), 1)[0]
         torch.testing.assert_close(many_i[f], one_i, rtol=0, atol=1e-13 * float(one_i.abs().max()))
         torch.testing.assert_close(many_l[f], one_l, rtol=0, atol=1e-13 * float(one_l.abs().max()))
+    # the many-field interpolant runs grouped by base cell: bit for bit the ungrouped kernel
+    assert quad.n_groups < quad.n_nodes
+    scratch = quad._many_scratch(fields.device)
+    plain = torch.empty_like(many_i)
+    pkg._lib.call("cdftb_quadrature_interpolate_many_f64", quad.base.data_ptr(), quad.w1d.data_ptr(), quad.n_nodes,
+                  *geo.grid.shape, fields.data_ptr(), nf, geo.grid.n_points, plain.data_ptr(), quad.n_nodes,
+                  scratch.data_ptr(), scratch.numel(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert torch.equal(many_i, plain)
     # and the oracle, for one field
     want = quad_o.interpolate(_np(fields[0]))
     np.testing.assert_allclose(_np(many_i[0]), want, rtol=0, atol=1e-12 * np.abs(want).max())

@@ -305,8 +305,15 @@ class CuspQuadrature:
         key, order = torch.sort(key, stable=True)
         _, counts = torch.unique_consecutive(key, return_counts=True)
         self.group_nodes = order.to(torch.int32).contiguous()
-        self.group_ptr = torch.cat([counts.new_zeros(1), torch.cumsum(counts, 0)]).to(torch.int32).contiguous()
-        self.n_groups = int(counts.numel())
+        # work items of at most GROUP_BATCH nodes of one cell (a cell near a nucleus holds up to ~80
+        # nodes): one warp each, so that a crowded cell does not hold up the launch
+        starts = torch.cumsum(counts, 0) - counts
+        items = (counts + self.GROUP_BATCH - 1) // self.GROUP_BATCH
+        first = torch.repeat_interleave(starts, items)
+        k = torch.arange(int(items.sum()), device=dev) - torch.repeat_interleave(torch.cumsum(items, 0) - items, items)
+        item_start = first + k * self.GROUP_BATCH
+        self.group_ptr = torch.cat([item_start, counts.sum().reshape(1)]).to(torch.int32).contiguous()
+        self.n_groups = int(item_start.numel())
         # far factor, plain and lumped far mass weights
         self.far = torch.empty(n, **f)
         self.far_weights = torch.empty(n, **f)
@@ -355,6 +362,8 @@ class CuspQuadrature:
     # --- interpolation and its transpose (quadrature.py:613-650) ---
     #: From this many fields on, L and L^T run one pass per 32 fields (the batched systems).
     MANY_FIELDS = 8
+    #: Nodes of one cell per warp of the grouped interpolant (GROUP_BATCH in csrc/quadrature.cu).
+    GROUP_BATCH = 4
 
     def _many_scratch(self, device) -> torch.Tensor:
         nbytes = _lib.library().cdftb_quadrature_many_scratch_bytes(self.n_nodes, self.grid.n_points)

@@ -348,9 +348,10 @@ int cdftb_quadrature_interpolate_many_f64(const int* base, const double* w1d, in
                                           const double* fields, int nf, int64_t field_stride, double* out,
                                           int64_t out_stride, void* scratch, int64_t scratch_bytes,
                                           cdftb_stream_t stream);
-/* The many-field interpolant with the nodes grouped by base cell: group_nodes (m node indices,
- * grouped) and group_ptr (groups + 1 offsets) list the nodes of each cell; the nodes of a group
- * read the same 8 x 8 x 8 box, which one warp reads once per four of them. Results equal
+/* The many-field interpolant with the nodes grouped by base cell: group_nodes (m node indices) and
+ * group_ptr (groups + 1 offsets) cut the nodes into groups whose members share a base cell (the
+ * host keeps groups to four nodes, so that a crowded cell does not hold up the launch). The nodes of
+ * a group read the same 8 x 8 x 8 box, which one warp reads once for four of them. Results equal
  * cdftb_quadrature_interpolate_many_f64's bit for bit; the same scratch. No reference counterpart
  * (the reference multiplies by its CSR matrix L, quadrature.py:613-620). */
 int cdftb_quadrature_interpolate_grouped_f64(const int* base, const double* w1d, int64_t m, int nx, int ny, int nz,

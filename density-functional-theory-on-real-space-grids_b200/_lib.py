@@ -129,6 +129,8 @@ SIGNATURES: dict[str, tuple] = {
                                               c_void_p, c_void_p]),
     "cdftb_row_sums_scratch_bytes": (c_int64, [c_int, c_int64]),
     "cdftb_row_sums_f64": (c_int, [c_void_p, c_int, c_int64, c_void_p, c_void_p, c_int64, c_void_p]),
+    "cdftb_gradient_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_double, c_int64,
+                                   c_void_p]),
     "cdftb_fd_derivative_f64": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_double,
                                         c_int64, c_int, c_double, c_void_p]),
     "cdftb_geometry_cusp_fields": (c_int, [c_int, c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_double, c_double,

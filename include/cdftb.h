@@ -407,6 +407,11 @@ int cdftb_row_sums_f64(const double* a, int rows, int64_t len, double* out, void
 int cdftb_fd_derivative_f64(const double* in, double* out, int nx, int ny, int nz, int axis, int accuracy,
                             const double* coefficients, double spacing, int64_t batch, int accumulate, double sign,
                             cdftb_stream_t stream);
+/* The three partial derivatives of a batch of fields (src/cdft/grid.py:740-743 gradient): in is
+ * (batch, N), out (batch, 3, N); each component is bit for bit cdftb_fd_derivative_f64's for its
+ * axis (accumulate 0, sign 1), from one pass over the field. */
+int cdftb_gradient_f64(const double* in, double* out, int nx, int ny, int nz, int accuracy, const double* coefficients,
+                       double spacing, int64_t batch, cdftb_stream_t stream);
 
 /* ---- geometry on the device (src/cdft/operators/cusp.py, quadrature.py, scf/step.py:129-165) ----
  * In these entry points `charges`, `positions` and `spheres` are HOST arrays (a few numbers per

@@ -201,6 +201,21 @@ def test_config2_he65_lda_scf(pkg, cuda, golden_values):
     assert out.scf_iterations == ref["iterations"]
 
 
+def test_gradient_is_three_partial_derivatives(pkg, he25, cuda):
+    """The one-pass gradient (cdftb_gradient_f64) equals the three partial derivatives bit for bit,
+    for a batch of fields and for one."""
+    from importlib import import_module
+
+    geometry = import_module(pkg.__name__ + ".geometry")
+    _, geo, _ = he25
+    g = torch.Generator().manual_seed(17)
+    fields = torch.randn((3, geo.grid.n_points), dtype=torch.float64, generator=g).to(cuda)
+    for f in (fields, fields[1]):
+        got = geometry.gradient(geo.grid, f)
+        want = torch.stack([geometry.partial_derivative(geo.grid, f, d) for d in range(3)], dim=-2)
+        assert got.shape == want.shape and torch.equal(got, want)
+
+
 @pytest.mark.parametrize("nf", [8, 13, 40])
 def test_interpolate_and_lift_many_fields(pkg, he25, cuda, nf):
     """The 32-fields-per-pass L and L^T (batched systems) against the one-field path."""

@@ -811,12 +811,48 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
     const int npl = xe + HALO + 1 - q0;
     const bool has_prev = a.has_prev != 0;
 
-    // the lane's orbitals (an empty slot borrows the first orbital's group for its lookups)
-    // the lane's orbitals: ORB lane + h, present when below the batch (an empty slot borrows the
-    // first orbital's group for its lookups); formed where they are used, so that no role keeps them
-    // in registers through its loop
-    const int64_t orb0 = int64_t(ORB) * lane;
-    auto orbital_of = [&](int h) -> int64_t { return orb0 + h < a.batch ? orb0 + h : orb0; };
+    // The lane's orbitals: ORB lane + h in order, or, with lanes aligned to orbital groups (systems
+    // on their own grids), orbitals ORB (l mod lpg) + h of group l / lpg; -1 for an empty slot, which
+    // borrows the lane's first orbital for its lookups. Formed where they are used, so that no role
+    // keeps them in registers through its loop.
+    auto orbital_at = [&](int h) -> int64_t {
+        return lane_orbital<ORB>(lane, h, a.batch, a.orb_per_group, a.lanes_per_group);
+    };
+    auto orbital_of = [&](int h) -> int64_t {
+        const int64_t o = orbital_at(h), o0 = orbital_at(0);
+        return o >= 0 ? o : (o0 >= 0 ? o0 : 0);
+    };
+    // the lane's geometry: its system's with per-system geometry, else the one shared copy
+    const int geo = a.per_system_geometry ? static_cast<int>(orbital_of(0) / a.orb_per_group) : 0;
+
+    // Systems on their own grids: a tile wholly beyond its lane's system (zero there in every
+    // iterate) stores its zeros and computes nothing; so does an empty lane. The whole CTA leaves
+    // before any barrier is used.
+    if (a.system_shapes != nullptr) {
+        const int* shape = a.system_shapes + 3 * geo;
+        if (orbital_at(0) < 0 || xa >= shape[0] || y0 >= shape[1] || z0 >= shape[2]) {
+            const int64_t plane_n = int64_t(ny) * nz;
+            for (int k = t; k < (xe - xa + 1) * TY * TZ; k += blockDim.x) {
+                const int i = xa + k / (TY * TZ);
+                const int r = k % (TY * TZ);
+                const int y = y0 + r / TZ, z = z0 + r % TZ;
+                if (y >= ny || z >= nzp) continue;
+                if (a.final_out) {
+                    if (z >= nz) continue;
+                    const int64_t pt = int64_t(i) * plane_n + int64_t(y) * nz + z;
+#pragma unroll
+                    for (int h = 0; h < ORB; ++h) {
+                        const int64_t o = orbital_at(h);
+                        if (o >= 0) store_as<S>(a.out, a.out_dtype, o * (plane_n * nx) + pt, S(0));
+                    }
+                } else {
+                    static_cast<E*>(a.out)[(int64_t(lane) * nx + i) * (int64_t(ny) * nzp) + int64_t(y) * nzp + z] =
+                        W::zero();
+                }
+            }
+            return;
+        }
+    }
 
     if (t == 0) {
         for (int s = 0; s < RW; ++s) {
@@ -860,10 +896,10 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
             // lane buffers as 8-byte elements, two per point: x = 2 z
             tma_load_4d(slot + SH::O_PHI, &maps.phi, 2 * (z0 - 8), y0 - HALO, q, lane, full);
             if (has_prev) tma_load_4d(slot + SH::O_PREV, &maps.prev, 2 * z0, y0, q - HALO, lane, full);
-            tma_load_4d(slot + SH::O_W0, &maps.w0, z0, y0, q, 0, full);
-            tma_load_4d(slot + SH::O_W1, &maps.w1, z0, y0, q, 0, full);
-            tma_load_4d(slot + SH::O_W2, &maps.w2, z0, y0, q, 0, full);
-            tma_load_4d(slot + SH::O_INV, &maps.inv, z0, y0, q - HALO, 0, full);
+            tma_load_4d(slot + SH::O_W0, &maps.w0, z0, y0, q, geo, full);
+            tma_load_4d(slot + SH::O_W1, &maps.w1, z0, y0, q, geo, full);
+            tma_load_4d(slot + SH::O_W2, &maps.w2, z0, y0, q, geo, full);
+            tma_load_4d(slot + SH::O_INV, &maps.inv, z0, y0, q - HALO, geo, full);
 #pragma unroll
             for (int h = 0; h < ORB; ++h)
                 tma_load_4d(slot + SH::O_POT + h * SH::POT_STEP, &maps.pot, z0, y0, q - HALO, grp[h], full);
@@ -1077,8 +1113,8 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
                         W::parts(res, rv);
 #pragma unroll
                         for (int h = 0; h < ORB; ++h)
-                            if (orb0 + h < a.batch)
-                                store_as<S>(a.out, a.out_dtype, (orb0 + h) * (plane_n * nx) + pt, rv[h]);
+                            if (const int64_t o = orbital_at(h); o >= 0)
+                                store_as<S>(a.out, a.out_dtype, o * (plane_n * nx) + pt, rv[h]);
                     }
                 } else if (own_pad) {
                     // the plane's offset is the same for the whole CTA (uniform arithmetic)
@@ -1156,7 +1192,7 @@ __global__ void pack_lanes_kernel(const void* __restrict__ in, int in_dtype, int
 // thread.
 template <typename W>
 __global__ void pack_wide_kernel(const void* __restrict__ in, int in_dtype, int64_t batch, int nx, int ny, int nz,
-                                 int nzp, int64_t lanes, typename W::E* __restrict__ out) {
+                                 int nzp, int64_t lanes, int opg, int lpg, typename W::E* __restrict__ out) {
     using S = typename W::S;
     constexpr int ORB = W::ORB;
     const int64_t per_lane = int64_t(nx) * ny * nzp;
@@ -1166,7 +1202,7 @@ __global__ void pack_wide_kernel(const void* __restrict__ in, int in_dtype, int6
         typename W::E* dst = out + l * per_lane;
         int64_t orb[ORB];
 #pragma unroll
-        for (int h = 0; h < ORB; ++h) orb[h] = (ORB * l + h < batch) ? ORB * l + h : -1;
+        for (int h = 0; h < ORB; ++h) orb[h] = lane_orbital<ORB>(l, h, batch, opg, lpg);
         for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < per_lane;
              k += int64_t(gridDim.x) * blockDim.x) {
             int64_t xy;
@@ -1491,7 +1527,6 @@ int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_
     a.tiles_z = static_cast<int>(ceil_div(a.nzp, TZ));
     const int64_t tiles = int64_t(tiles_y) * a.tiles_z;
     a.xchunk = xchunk > 0 ? (xchunk < a.nx ? xchunk : a.nx) : choose_chunk(a.nx, tiles * lanes, sm_count());
-    a.lanes_per_group = 0;
     const int chunks = static_cast<int>(ceil_div(a.nx, a.xchunk));
     for (int64_t first = 0; first < lanes; first += 65535) {
         const int64_t count = (lanes - first) < 65535 ? (lanes - first) : 65535;
@@ -1519,25 +1554,40 @@ int encode_wide_lane_maps(void* buf, int nzp, int ny, int nx, int64_t lanes, int
 
 template <typename W>
 int pack_wide(const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz, int nzp, int64_t lanes,
-              void* dst, cudaStream_t stream) {
+              int opg, int lpg, void* dst, cudaStream_t stream) {
     if ((reinterpret_cast<uintptr_t>(dst) & 15) != 0) return CDFTB_ERR_ARGUMENT;
     const int64_t per_lane = int64_t(nx) * ny * nzp;
     const unsigned ly = static_cast<unsigned>(std::min<int64_t>(lanes, 65535));
     const unsigned bx = static_cast<unsigned>(
         std::max<int64_t>(1, std::min<int64_t>(ceil_div(per_lane, 256), ceil_div(int64_t(148) * 16, ly))));
-    pack_wide_kernel<W><<<dim3(bx, ly), 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes,
+    pack_wide_kernel<W><<<dim3(bx, ly), 256, 0, stream>>>(block, in_dtype, batch, nx, ny, nz, nzp, lanes, opg, lpg,
                                                           static_cast<typename W::E*>(dst));
     return check_launch();
 }
 
 // The same steps for both lane layouts: two-orbital (LaneF2) or one-orbital (LaneD) lane points of
 // 8 bytes, or wide ones of 16 bytes (WideF4, WideD2).
+// Wide lanes per orbital group when lanes are aligned to groups (per-system geometry), else 0.
+int wide_lanes_per_group(const cdftb_operator* op, int orbitals) {
+    return op->per_system_geometry ? static_cast<int>(ceil_div(op->orbitals_per_group, orbitals)) : 0;
+}
+
 template <typename L>
 int64_t lane_count(const cdftb_operator* op, int64_t batch) {
-    if constexpr (L::WIDE)
-        return ceil_div(batch, L::ORB);
-    else
+    if constexpr (L::WIDE) {
+        const int lpg = wide_lanes_per_group(op, L::ORB);
+        return lpg > 0 ? ceil_div(batch, op->orbitals_per_group) * lpg : ceil_div(batch, L::ORB);
+    } else {
         return lanes_of(op, batch);
+    }
+}
+
+// The call's arguments for lane layout L (the wide layouts align their own lanes to groups).
+template <typename L>
+FilterArgs lane_args(const cdftb_operator* op, int64_t batch) {
+    FilterArgs a = base_args(op, batch);
+    if constexpr (L::WIDE) a.lanes_per_group = wide_lanes_per_group(op, L::ORB);
+    return a;
 }
 
 template <typename L>
@@ -1558,7 +1608,8 @@ template <typename L>
 int pack_lanes(const cdftb_operator* op, const void* block, int in_dtype, int64_t batch, int nx, int ny, int nz,
                int nzp, int64_t lanes, void* dst, cudaStream_t stream) {
     if constexpr (L::WIDE)
-        return pack_wide<L>(block, in_dtype, batch, nx, ny, nz, nzp, lanes, dst, stream);
+        return pack_wide<L>(block, in_dtype, batch, nx, ny, nz, nzp, lanes, op->orbitals_per_group,
+                            wide_lanes_per_group(op, L::ORB), dst, stream);
     else
         return pack_block<L>(op, block, in_dtype, batch, nx, ny, nz, nzp, lanes, dst, stream);
 }
@@ -1662,7 +1713,7 @@ int tune_slab(const cdftb_operator* op, int64_t batch, void* geo_base, void* buf
         const bool kinetic = apply != nullptr && apply->kinetic_only;
         if ((st = prepare_geometry<Lane>(op, batch, geo_base, ty, tz, kinetic, &m, stream)) != CDFTB_OK) break;
         if ((st = encode_lanes<Lane>(buf[2], nzp, ny, nx, lanes, ty, tz, &m.phi, &m.prev)) != CDFTB_OK) break;
-        FilterArgs a = base_args(op, batch);
+        FilterArgs a = lane_args<Lane>(op, batch);
         if (apply) {
             a = *apply;
         } else {
@@ -1737,7 +1788,7 @@ int slab_filter(const cdftb_operator* op, const void* block, int in_dtype, void*
     for (int b = 0; b < 3; ++b)
         if ((st = encode_lanes<Lane>(buf[b], nzp, ny, nx, lanes, ty, tz, &maps[b].phi, &maps[b].prev)) != CDFTB_OK)
             return st;
-    FilterArgs a = base_args(op, batch);
+    FilterArgs a = lane_args<Lane>(op, batch);
     a.coef = coefficients;
     a.degree = degree;
     // Y_1 -> buf0, Y_2 -> buf1, then Y_{k+1} overwrites Y_{k-1} in place (a point's previous value
@@ -1780,7 +1831,7 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
         autotune = g_autotune;
     }
     if (!known && autotune) {
-        FilterArgs t = base_args(op, batch);
+        FilterArgs t = lane_args<Lane>(op, batch);
         t.apply_only = 1;
         t.kinetic_only = kinetic_only != 0;
         t.degree = 1;
@@ -1800,7 +1851,7 @@ int slab_apply(const cdftb_operator* op, const void* phi, int in_dtype, void* ou
         CDFTB_OK)
         return st;
     if ((st = encode_lanes<Lane>(w, nzp, ny, nx, lanes, ty, tz, &m.phi, &m.prev)) != CDFTB_OK) return st;
-    FilterArgs a = base_args(op, batch);
+    FilterArgs a = lane_args<Lane>(op, batch);
     a.apply_only = 1;
     a.kinetic_only = kinetic_only != 0;
     a.degree = 1;
@@ -1819,18 +1870,15 @@ bool wide_applies(const cdftb_operator* op, int64_t batch) {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         on = g_wide;
     }
-    return on && !op->per_system_geometry && batch > 0;
+    return on && batch > 0;
 }
 
 // Lane bytes of the larger layout a call may use (the wide one when it can apply).
 int64_t lane_bytes_total(const cdftb_operator* op, int64_t batch) {
     const int64_t points = int64_t(op->nx) * op->ny * padded_z(op->nz);
     int64_t total = lanes_of(op, batch) * points * 8;
-    if (!op->per_system_geometry) {
-        const int per = op->dtype == CDFTB_F32 ? WideF4::ORB : WideD2::ORB;
-        total = std::max<int64_t>(total, ceil_div(batch, per) * points * 16);
-    }
-    return total;
+    const int64_t wide = op->dtype == CDFTB_F32 ? lane_count<WideF4>(op, batch) : lane_count<WideD2>(op, batch);
+    return std::max<int64_t>(total, wide * points * 16);
 }
 
 }  // namespace

@@ -56,27 +56,31 @@ def test_argument_errors_need_no_gpu(pkg):
 
 @pytest.mark.parametrize("dtype", [0, 1])  # CDFTB_F64, CDFTB_F32
 def test_work_sizes_cover_the_wide_lanes(pkg, dtype):
-    """Host-side size queries: with one shared geometry the work buffers hold the 16-byte wide lanes
-    (four float32 or two float64 orbitals per point) as well as the 8-byte ones; with per-system
-    geometry only the 8-byte lanes, which follow the orbital groups."""
+    """Host-side size queries: the work buffers hold the 16-byte wide lanes (four float32 or two
+    float64 orbitals per point) as well as the 8-byte ones. With one shared geometry the lanes run
+    over the whole batch; with per-system geometry both layouts start each orbital group on a
+    fresh lane. The filter holds three lane copies and the apply one, beside the same geometry
+    copies, so the two sizes differ by two lane copies."""
     lib = pkg._lib.library()
     op = pkg._lib.Operator()
     op.nx, op.ny, op.nz = 9, 9, 13
     op.accuracy, op.spacing, op.dtype, op.orbitals_per_group = 8, 0.3, dtype, 5
     points = 9 * 9 * 14  # nz padded to even
-    batch = 5
-    narrow_shared = (batch + 1) // 2 if dtype == 1 else batch  # float2 pairs / one orbital per lane
-    narrow_grouped = 3 if dtype == 1 else batch                # lanes of one 5-orbital group: 3 pairs / 5
-    wide = -(-batch // (4 if dtype == 1 else 2))
-    lane_shared = max(narrow_shared * 8, wide * 16) * points
-    lane_grouped = narrow_grouped * 8 * points
+    batch, groups = 10, 2
+    per_wide = 4 if dtype == 1 else 2
+    narrow_shared = (batch + 1) // 2 if dtype == 1 else batch   # float2 pairs / one orbital per lane
+    narrow_grouped = groups * 3 if dtype == 1 else batch        # 3 pairs per 5-orbital group / 10
+    wide_shared = -(-batch // per_wide)                         # 3 / 5
+    wide_grouped = groups * -(-5 // per_wide)                   # 2 x 2 / 2 x 3
+    lane_shared = max(narrow_shared * 8, wide_shared * 16) * points
+    lane_grouped = max(narrow_grouped * 8, wide_grouped * 16) * points
+    assert lane_grouped > lane_shared
     op.per_system_geometry = 0
     filt_shared = lib.cdftb_chebyshev_filter_work_bytes(ctypes.byref(op), batch)
     apply_shared = lib.cdftb_cusp_apply_work_bytes(ctypes.byref(op), batch)
     op.per_system_geometry = 1
     filt_grouped = lib.cdftb_chebyshev_filter_work_bytes(ctypes.byref(op), batch)
     apply_grouped = lib.cdftb_cusp_apply_work_bytes(ctypes.byref(op), batch)
-    # the geometry copies are the same for one system either way, so the differences are the lanes'
-    assert filt_shared - filt_grouped == 3 * (lane_shared - lane_grouped)
-    assert apply_shared - apply_grouped == lane_shared - lane_grouped
-    assert filt_shared >= 3 * wide * 16 * points and apply_shared >= wide * 16 * points
+    assert filt_shared - apply_shared == 2 * lane_shared
+    assert filt_grouped - apply_grouped == 2 * lane_grouped
+    assert filt_grouped > filt_shared and apply_grouped > apply_shared  # two geometry copies, wider lanes

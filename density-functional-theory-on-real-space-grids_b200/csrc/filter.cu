@@ -261,14 +261,17 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
 // The orbital held by half h of lane l, or -1 for an empty half. Lanes run over the orbitals in order
 // (lane l: orbitals ORBITALS l + h) or, aligned to orbital groups, over each group separately, so that
 // no lane mixes two groups (lane l: group l / lpg, orbitals ORBITALS (l mod lpg) + h of that group).
+// Lane indices fit 32 bits (a lane is a whole grid of points), so the division is a 32-bit one, which
+// the compiler inlines: no call interrupts the loops that form orbitals on the fly.
 template <int ORBITALS>
 __host__ __device__ __forceinline__ int64_t lane_orbital(int64_t l, int h, int64_t batch, int opg, int lpg) {
     int64_t o;
     if (lpg > 0) {
-        const int64_t g = l / lpg;
-        const int64_t j = ORBITALS * (l - g * lpg) + h;
+        const int li = static_cast<int>(l);
+        const int g = li / lpg;
+        const int j = ORBITALS * (li - g * lpg) + h;
         if (j >= opg) return -1;
-        o = g * opg + j;
+        o = int64_t(g) * opg + j;
     } else {
         o = ORBITALS * l + h;
     }
@@ -782,7 +785,11 @@ constexpr int wide_max_registers() {
     return (16384 / (((T / 32) + 3) / 4 * 32)) / 8 * 8 < 255 ? (16384 / (((T / 32) + 3) / 4 * 32)) / 8 * 8 : 255;
 }
 
-template <typename W, int TYW, int TZ>
+// GENERAL: the lane's orbitals, its geometry and the skip of tiles beyond its system's grid are
+// looked up at run time, for lanes in orbital order or aligned to orbital groups (per-system
+// geometry, a.lanes_per_group > 0). Otherwise the kernel takes lanes in orbital order over one
+// shared geometry only, and carries none of those lookups.
+template <typename W, int TYW, int TZ, bool GENERAL>
 __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typename W::S), W::ORB>::T>()))
     slab_filter_wide_kernel(const __grid_constant__ FilterMaps maps, const FilterArgs a) {
     using E = typename W::E;
@@ -815,20 +822,25 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
     // on their own grids), orbitals ORB (l mod lpg) + h of group l / lpg; -1 for an empty slot, which
     // borrows the lane's first orbital for its lookups. Formed where they are used, so that no role
     // keeps them in registers through its loop.
+    const int64_t orb0 = int64_t(ORB) * lane;
     auto orbital_at = [&](int h) -> int64_t {
-        return lane_orbital<ORB>(lane, h, a.batch, a.orb_per_group, a.lanes_per_group);
+        if constexpr (GENERAL) return lane_orbital<ORB>(lane, h, a.batch, a.orb_per_group, a.lanes_per_group);
+        return orb0 + h < a.batch ? orb0 + h : -1;
     };
     auto orbital_of = [&](int h) -> int64_t {
-        const int64_t o = orbital_at(h), o0 = orbital_at(0);
-        return o >= 0 ? o : (o0 >= 0 ? o0 : 0);
+        if constexpr (GENERAL) {
+            const int64_t o = orbital_at(h), o0 = orbital_at(0);
+            return o >= 0 ? o : (o0 >= 0 ? o0 : 0);
+        }
+        return orb0 + h < a.batch ? orb0 + h : orb0;
     };
     // the lane's geometry: its system's with per-system geometry, else the one shared copy
-    const int geo = a.per_system_geometry ? static_cast<int>(orbital_of(0) / a.orb_per_group) : 0;
+    const int geo = (GENERAL && a.per_system_geometry) ? static_cast<int>(orbital_of(0) / a.orb_per_group) : 0;
 
     // Systems on their own grids: a tile wholly beyond its lane's system (zero there in every
     // iterate) stores its zeros and computes nothing; so does an empty lane. The whole CTA leaves
     // before any barrier is used.
-    if (a.system_shapes != nullptr) {
+    if (GENERAL && a.system_shapes != nullptr) {
         const int* shape = a.system_shapes + 3 * geo;
         if (orbital_at(0) < 0 || xa >= shape[0] || y0 >= shape[1] || z0 >= shape[2]) {
             const int64_t plane_n = int64_t(ny) * nz;
@@ -1112,9 +1124,14 @@ __global__ void __maxnreg__((wide_max_registers<WideShape<TYW, TZ, sizeof(typena
                         S rv[ORB];
                         W::parts(res, rv);
 #pragma unroll
-                        for (int h = 0; h < ORB; ++h)
-                            if (const int64_t o = orbital_at(h); o >= 0)
-                                store_as<S>(a.out, a.out_dtype, o * (plane_n * nx) + pt, rv[h]);
+                        for (int h = 0; h < ORB; ++h) {
+                            if constexpr (GENERAL) {
+                                if (const int64_t o = orbital_at(h); o >= 0)
+                                    store_as<S>(a.out, a.out_dtype, o * (plane_n * nx) + pt, rv[h]);
+                            } else if (orb0 + h < a.batch) {
+                                store_as<S>(a.out, a.out_dtype, (orb0 + h) * (plane_n * nx) + pt, rv[h]);
+                            }
+                        }
                     }
                 } else if (own_pad) {
                     // the plane's offset is the same for the whole CTA (uniform arithmetic)
@@ -1508,17 +1525,17 @@ int launch_any_tz(int tz, const FilterMaps& m, const FilterArgs& a, int64_t lane
 // ---- wide lanes (slab_filter_wide_kernel): launch, lane maps, packing
 bool g_wide = true;  // guarded by g_tune_mutex (declared below with the tuner)
 
-template <typename W, int TYW, int TZ>
-int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
+template <typename W, int TYW, int TZ, bool GENERAL>
+int launch_wide_as(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_t stream, int xchunk) {
     using SH = WideShape<TYW, TZ, sizeof(typename W::S), W::ORB>;
     static bool configured = false;
     if (!configured) {
-        int st = check(cudaFuncSetAttribute(slab_filter_wide_kernel<W, TYW, TZ>,
+        int st = check(cudaFuncSetAttribute(slab_filter_wide_kernel<W, TYW, TZ, GENERAL>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(SH::BYTES)));
         if (st != CDFTB_OK) return st;
         // a CTA this kernel's registers cannot hold is refused here, before any launch
         cudaFuncAttributes attr{};
-        st = check(cudaFuncGetAttributes(&attr, slab_filter_wide_kernel<W, TYW, TZ>));
+        st = check(cudaFuncGetAttributes(&attr, slab_filter_wide_kernel<W, TYW, TZ, GENERAL>));
         if (st != CDFTB_OK) return st;
         if (attr.maxThreadsPerBlock < SH::T) return CDFTB_ERR_CAPACITY;
         configured = true;
@@ -1534,11 +1551,25 @@ int launch_wide(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStream_
         a.token = next_launch_token(true);
         a.stop_after_planes = take_test_stop();
         dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(chunks), static_cast<unsigned>(count));
-        slab_filter_wide_kernel<W, TYW, TZ><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
+        slab_filter_wide_kernel<W, TYW, TZ, GENERAL><<<grid, SH::T, SH::BYTES, stream>>>(maps, a);
         int st = check_launch();
         if (st != CDFTB_OK) return st;
     }
     return CDFTB_OK;
+}
+
+// Lanes aligned to orbital groups (per-system geometry) take the general instantiation, and so do
+// all float64 lanes: the general float64 kernels keep every value in registers, where the in-order
+// ones spill 4 bytes (at 16 He 65^3 systems, 8 x 36 tiles: 257.7 against 262.1 us per step). The
+// float32 in-order kernels are the faster ones (128 systems, 13 x 24: 1102 against 1124 us).
+template <typename W, int TYW, int TZ>
+int launch_wide(const FilterMaps& maps, const FilterArgs& a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
+    if constexpr (W::ORB == 2) {
+        return launch_wide_as<W, TYW, TZ, true>(maps, a, lanes, stream, xchunk);
+    } else {
+        return a.lanes_per_group > 0 ? launch_wide_as<W, TYW, TZ, true>(maps, a, lanes, stream, xchunk)
+                                     : launch_wide_as<W, TYW, TZ, false>(maps, a, lanes, stream, xchunk);
+    }
 }
 
 // Lane buffers of 16-byte points described as 8-byte elements, two per point.

@@ -1559,12 +1559,13 @@ int launch_wide_as(const FilterMaps& maps, FilterArgs a, int64_t lanes, cudaStre
 }
 
 // Lanes aligned to orbital groups (per-system geometry) take the general instantiation, and so do
-// all float64 lanes: the general float64 kernels keep every value in registers, where the in-order
-// ones spill 4 bytes (at 16 He 65^3 systems, 8 x 36 tiles: 257.7 against 262.1 us per step). The
-// float32 in-order kernels are the faster ones (128 systems, 13 x 24: 1102 against 1124 us).
+// the float64 lanes in 8-row tiles: there the general kernels keep every value in registers, where
+// the in-order ones spill 4 bytes (16 He 65^3 systems, 8 x 36: 257.7 against 262.1 us per step).
+// Elsewhere the in-order kernels are the faster ones (float32, 128 systems, 13 x 24: 1102 against
+// 1124 us; float64, one system, 13 x 24: 33.3 against 34.1 us).
 template <typename W, int TYW, int TZ>
 int launch_wide(const FilterMaps& maps, const FilterArgs& a, int64_t lanes, cudaStream_t stream, int xchunk = 0) {
-    if constexpr (W::ORB == 2) {
+    if constexpr (W::ORB == 2 && TYW == 8) {
         return launch_wide_as<W, TYW, TZ, true>(maps, a, lanes, stream, xchunk);
     } else {
         return a.lanes_per_group > 0 ? launch_wide_as<W, TYW, TZ, true>(maps, a, lanes, stream, xchunk)

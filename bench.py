@@ -50,7 +50,8 @@ def _args():
     p.add_argument("--kernel-only", action="store_true",
                    help="time only the fused Chebyshev step on a He grid of --edge points (for profiling)")
     p.add_argument("--breakdown", action="store_true",
-                   help="device time per kernel of one solve (torch.profiler, no replay) instead of the bench line")
+                   help="device time per kernel of one solve (torch.profiler, no replay) instead of the bench line; "
+                        "with --workload h2plus-scan, of one batched scan solve (one GPU)")
     p.add_argument("--workload", choices=("he-lda", "h2plus-scan", "adjoint"), default="he-lda",
                    help="he-lda: the headline He-LDA 65^3 solve; h2plus-scan: the 48-system bond scan; "
                         "adjoint: energy gradients of He-LDA at h 0.16 (101^3) against central differences")
@@ -408,6 +409,21 @@ def run_scan(args) -> None:
     for bond in SCAN_BONDS:
         system = scan_system(bond)
         shapes.append(pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev).shape)
+    if args.breakdown and world == 1:
+        geos = []
+        for bond in SCAN_BONDS:
+            system = scan_system(bond)
+            grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev)
+            geos.append(pkg.build_cusp_geometry(grid, system.charges, system.positions))
+
+        def solve(_):
+            solve.last = None
+            return pkg.batch.solve_noninteracting_batch(geos, 1.0, filter_precision=precision)
+
+        for _ in range(args.warmup):  # the first solve also runs the tile autotuner's timings
+            solve(None)
+        _breakdown(solve, None)
+        return
     costs = [pkg.replicas.system_cost(s) for s in shapes]
     shares = pkg.replicas.partition_by_cost(costs, world)
     figures = scan_figures(pkg, dev, precision, args.warmup, one_by_one=world == 1, indices=shares[rank])

@@ -258,11 +258,9 @@ def run_adjoint(args) -> None:
     import torch
 
     import __graft_entry__
-    from oracle import scf as oscf  # the system definition only
-
     pkg = __graft_entry__.package()
     dev = torch.device("cuda:0")
-    system = oscf.he_lda(spacing=0.16, edge=16.0)
+    system = pkg.systems.he_lda(spacing=0.16, edge=16.0)
     grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev)
     geo = pkg.build_cusp_geometry(grid, system.charges, system.positions)
     scf = pkg.SCFConfig(energy_tol=1e-11, density_tol=1e-8, max_iterations=400)
@@ -323,9 +321,9 @@ SCAN_BONDS = [0.8 + k * 5.2 / 47 for k in range(48)]
 
 
 def scan_system(bond: float):
-    from oracle import scf as oscf  # the system definitions only
+    import __graft_entry__
 
-    return oscf.h2_plus(bond, spacing=0.25, transverse=12.0)
+    return __graft_entry__.package().systems.h2_plus(bond, spacing=0.25, transverse=12.0)
 
 
 def scan_figures(pkg, dev, precision, warmup: int, one_by_one: bool = True, indices=None) -> dict:
@@ -831,9 +829,7 @@ def main() -> None:
 
     pkg = __graft_entry__.package()
     lib = pkg._lib.library()
-    from oracle import scf as oscf  # the system definition only (charges, box, spacing)
-
-    system = oscf.he_lda()
+    system = pkg.systems.he_lda()
     grid = pkg.UniformGrid.box(system.box_lengths, system.spacing, system.anchor, device=dev)
     geometry = pkg.build_cusp_geometry(grid, system.charges, system.positions)
     precision = torch.float32 if args.form == "mixed" else torch.float64
@@ -985,10 +981,13 @@ def main() -> None:
         result["plain_fp64"] = plain
         result["batched_mixed_over_plain_fp64"] = value / (world * plain["value"])
     if rank == 0 and not args.no_cpu_baseline and world == 1:
+        from oracle import scf as oscf  # the CPU baseline leg: the oracle's own system and solve
+
         cores = os.cpu_count() or 1
-        cpu_geometry = oscf.build_geometry(system)
-        oracle_warmup(system, cpu_geometry, cores)
-        cpu_result, cpu_s, breakdown = oracle_solve(system, cpu_geometry, cores)
+        cpu_system = oscf.he_lda()
+        cpu_geometry = oscf.build_geometry(cpu_system)
+        oracle_warmup(cpu_system, cpu_geometry, cores)
+        cpu_result, cpu_s, breakdown = oracle_solve(cpu_system, cpu_geometry, cores)
         result["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": UNIT, "cores": cores, "kind": "port",
                                   "sample": _solve_text(cpu_result, cpu_s, cores, breakdown, "one whole SCF solve"),
                                   "energy_error_vs_reference_cpu_fp64_ha":

@@ -88,3 +88,20 @@ def test_threaded_whole_solve_is_the_oracle_solve():
     # the operator applications plus one kinetic application per energy evaluation
     assert breakdown["block_applications"] == want["applications"] + want["scf_iterations"] + 1
     assert seconds > 0.0
+
+
+@pytest.mark.parametrize("which", ["he65", "he101", "h2plus_short", "h2plus_long"])
+def test_workload_systems_are_the_oracle_systems(pkg, which):
+    """The measured workloads build their grids from the package's own system definitions; the CPU
+    baseline and the parity tests from the oracle's. Both describe the same nuclei, electrons, box,
+    spacing and anchoring."""
+    from oracle import scf as oscf
+
+    ours, theirs = {
+        "he65": (pkg.systems.he_lda(), oscf.he_lda()),
+        "he101": (pkg.systems.he_lda(spacing=0.16, edge=16.0), oscf.he_lda(spacing=0.16, edge=16.0)),
+        "h2plus_short": (pkg.systems.h2_plus(0.8), oscf.h2_plus(0.8, spacing=0.25, transverse=12.0)),
+        "h2plus_long": (pkg.systems.h2_plus(6.0, spacing=0.4, transverse=10.0), oscf.h2_plus(6.0, 0.4, 10.0)),
+    }[which]
+    for field in ("charges", "positions", "n_electrons", "box_lengths", "spacing", "anchor"):
+        assert getattr(ours, field) == getattr(theirs, field), field

@@ -9,7 +9,7 @@ and registers it as ``cdft_b200``.
 
 from __future__ import annotations
 
-from . import _lib, adjoint, batch, eigen, geometry, operators, poisson, replicas, rng, scf, systems, xc
+from . import _lib, adjoint, batch, carriers, eigen, geometry, operators, poisson, replicas, rng, scf, systems, xc
 from .eigen import (
     ChebyshevFilteredSubspace,
     EigenConfig,

@@ -535,7 +535,8 @@ class BatchedKohnShamStep:
         self.batch = int(batch)
         self.n_electrons = float(n_electrons)
         self.n_states = max(1, int(-(-self.n_electrons // 2.0)))
-        self.eigen = eigen or EigenConfig()
+        from .carriers import eigen_config
+        self.eigen = eigen_config(eigen)
         self.seeds = list(seeds) if seeds is not None else list(range(self.batch))
         if len(self.seeds) != self.batch:
             raise ValueError("one seed per system")
@@ -823,8 +824,9 @@ def solve_self_consistent_batch(step: BatchedKohnShamStep, mixing: MixingConfig 
     sweep); the final full diagonalisation filters in float64.
     """
     started = time.perf_counter()
-    mixing = mixing or MixingConfig()
-    scf = scf or SCFConfig()
+    from .carriers import mixing_config, scf_config
+    mixing = mixing_config(mixing)
+    scf = scf_config(scf)
     b = step.batch
     dev = step.grid.device
     q = step.quadrature
@@ -1197,7 +1199,8 @@ def solve_noninteracting_batch(geometries, n_electrons: float, *, seeds=None, ei
     """
     from .scf import aufbau_occupations, nuclear_repulsion
 
-    config = eigen or EigenConfig()
+    from .carriers import eigen_config
+    config = eigen_config(eigen)
     b = len(geometries)
     seeds = list(seeds) if seeds is not None else [0] * b
     h = MultiGeometryHamiltonian(geometries)

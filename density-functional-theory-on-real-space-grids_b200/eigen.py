@@ -241,6 +241,7 @@ class EigenConfig:
     bound_safety: float = 1.02
     max_iterations: int = 300
     residual_tol: float = 1.0e-8
+    cross_check: bool = False
     cross_check_tol: float = 1.0e-8
 
 

@@ -91,7 +91,8 @@ class KohnShamStep:
         needed = max(1, int(-(-self.n_electrons // 2.0)))
         self.n_states = max(needed, n_states or needed)
         self.n_spin = 1
-        self.eigen = eigen or EigenConfig()
+        from .carriers import eigen_config
+        self.eigen = eigen_config(eigen)
         self.seed = seed
         self.ion_ion = nuclear_repulsion(geometry.charges, geometry.positions)
         self.poisson = CoulombCutoffPoisson(self.grid, pad_factor=pad_factor)
@@ -551,9 +552,10 @@ def solve_self_consistent(step: KohnShamStep, mixing: MixingConfig | None = None
     loop continues with the float64 filter until the same test passes again, and the final full
     diagonalisation filters in float64, so the converged density carries no float32 noise.
     """
+    from .carriers import mixing_config, scf_config
     started = time.perf_counter()
-    mixing = mixing or MixingConfig()
-    scf = scf or SCFConfig()
+    mixing = mixing_config(mixing)
+    scf = scf_config(scf)
     q = step.quadrature
     mass = q.mass_weights
     f2 = step._f2_grid
@@ -698,19 +700,22 @@ def lobpcg_cross_check(hamiltonian, eigenvalues: torch.Tensor, n_states: int, ei
 
 def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: int = 0,
                          eigen: EigenConfig | None = None, external_potential: torch.Tensor | None = None,
-                         cross_check: bool = False) -> dict:
+                         cross_check: bool | None = None) -> dict:
     """(``src/cdft/scf/noninteracting.py:118-330``) for the cusp-factorised path, ``ritz_stop=True``.
 
     ``external_potential`` adds a diagonal term to the operator (an external perturbation in the
     form quadrature.effective_potential gives it). The result also holds the occupied orbitals and
     their occupations (``"orbitals"``, ``"occupations"``), normalised in the measure.
     """
+    from .carriers import eigen_config
+    eigen = eigen_config(eigen)
+    cross_check = eigen.cross_check if cross_check is None else cross_check
     grid = geometry.grid
     ham = CuspFactoredHamiltonian(grid, geometry.factor, extra_potential=external_potential,
                                   quadrature=geometry.quadrature)
     n_states = max(1, int(-(-float(n_electrons) // 2.0)))
     generator = SeededStream(seed, grid.device)
-    solver = ChebyshevFilteredSubspace(grid, eigen or EigenConfig(), ritz_stop=True)
+    solver = ChebyshevFilteredSubspace(grid, eigen, ritz_stop=True)
     result = solver.solve(ham, n_states, generator=generator)
     occ = torch.from_numpy(aufbau_occupations(n_states, float(n_electrons))).to(grid.device)
     kinetic = ham.kinetic_energy_tensor(result.eigenvectors, occ[0])
@@ -723,5 +728,5 @@ def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: in
            "iterations": result.n_iterations, "converged": result.converged, "applications": float(ham.apply_count),
            "stop_reason": solver.stop_reason, "orbitals": result.eigenvectors, "occupations": occ[0]}
     if cross_check:
-        out.update(lobpcg_cross_check(ham, result.eigenvalues, n_states, eigen or EigenConfig(), seed))
+        out.update(lobpcg_cross_check(ham, result.eigenvalues, n_states, eigen, seed))
     return out

@@ -208,6 +208,12 @@ class DeviceTimeout(CdftbError):
     """A kernel's bounded wait gave up (``CDFTB_ERR_TIMEOUT``): its outputs are not valid."""
 
 
+#: How many timed-out launches :func:`check_device_status` has reported in this process. A captured
+#: graph replays its launches with the abort token they had at capture, so a graph captured before a
+#: timeout is not replayed after one (``eigen.GraphedChebyshevFilter`` captures again).
+timeouts_reported = 0
+
+
 def check_device_status(where: str = "") -> None:
     """Read and clear the library's device error flags; raise :class:`DeviceTimeout` if any was set.
 
@@ -222,6 +228,8 @@ def check_device_status(where: str = "") -> None:
         return
     text = lib.cdftb_status_string(status).decode()
     if flags.value:
+        global timeouts_reported
+        timeouts_reported += 1
         raise DeviceTimeout(f"{where or 'cdftb'}: a kernel gave up waiting ({text}, flags {flags.value}); "
                             "its results were discarded")
     raise CdftbError(f"cdftb_device_status: {text} (status {status})")

@@ -103,6 +103,163 @@ def filter_with_table(hamiltonian, block: torch.Tensor, table: torch.Tensor, deg
     return out
 
 
+GRAPH_MAX_CAPTURES = 8
+
+
+class GraphedChebyshevFilter:
+    """``GraphedChebyshevFilter`` (``src/cdft/eigen/chefsi.py:185-392``): the fused filter replayed
+    from a ``torch.cuda.CUDAGraph``.
+
+    One capture per key (operator geometry and dtype, block shape, potential shape, degree) holds
+    the ``degree`` launches of one ``cdftb_chebyshev_filter`` call over static buffers: the block,
+    the potential (so a new SCF Hamiltonian on the same geometry replays the same graph), the
+    coefficient table, the output and the filter's scratch. Before each replay the block and the
+    potential are copied in on the device and the table comes from pinned memory by a non-blocking
+    copy, so a call reads nothing back to the host. The library call itself neither allocates nor
+    synchronises once the tile autotuner has seen the shape, and a direct call before each capture
+    makes sure it has.
+
+    As in the reference, nothing falls back silently: an operator without the graph seam (the
+    level-shifted rung), a capture or replay error, a first replay that differs from the direct call
+    by even one bit, or more than ``GRAPH_MAX_CAPTURES`` captures make the engine call the filter
+    directly, each counted by reason in :meth:`record`. A capture's first replay is checked against
+    the direct call, whose result that call returns. A capture made before a timed-out launch was
+    reported (``_lib.timeouts_reported``) is captured again, since a graph replays its launches with
+    their abort token of the capture.
+    """
+
+    def __init__(self, device, reason_disabled: str | None = None) -> None:
+        self.device = torch.device(device)
+        self.disabled_reason = reason_disabled
+        self.captures = 0
+        self.replays = 0
+        self.eager_calls: dict[str, int] = {}
+        self.warmup_applications = 0
+        self.validation_max_rel_diff: float | None = None
+        self._release()
+
+    def record(self) -> dict:
+        used = self.disabled_reason is None and self.replays > 0
+        out = {"used": used, "captures": self.captures, "replays": self.replays,
+               "eager_calls": dict(self.eager_calls), "warmup_applications": self.warmup_applications,
+               "validation_max_rel_diff": self.validation_max_rel_diff}
+        if not used:
+            out["reason"] = self.disabled_reason or (
+                "no filter call was graph-capable" if self.eager_calls else "the filter was never called")
+        return out
+
+    def _release(self) -> None:
+        self._graph = None
+        self._key = None
+        self._static = None
+        self._template = None
+        self._validated = False
+        self._generation = _lib.timeouts_reported
+
+    def _disable(self, reason: str) -> None:
+        self.disabled_reason = reason
+        self._release()
+
+    def _filter_directly(self, hamiltonian, block, degree, lower, upper, spectrum_min) -> torch.Tensor:
+        """The filter without a graph (the library call, or the recurrence over ``apply``)."""
+        return chebyshev_filter(hamiltonian, block, degree, lower, upper, spectrum_min)
+
+    def _direct(self, reason: str, hamiltonian, block, degree, lower, upper, spectrum_min) -> torch.Tensor:
+        self.eager_calls[reason] = self.eager_calls.get(reason, 0) + 1
+        return self._filter_directly(hamiltonian, block, degree, lower, upper, spectrum_min)
+
+    def _seam(self, hamiltonian, block: torch.Tensor):
+        """``(seam, None)``, where the seam builds the capture's operator (``operator``,
+        ``filter_potential``, ``graph_geometry_key``, ``note_applications``, ``dtype``), or
+        ``(None, why)`` when this call cannot replay."""
+        for name in ("operator", "filter_potential", "graph_geometry_key", "note_applications", "dtype"):
+            if not hasattr(hamiltonian, name):
+                return None, f"operator {type(hamiltonian).__name__} has no graph seam"
+        return hamiltonian, None
+
+    def __call__(self, hamiltonian, block: torch.Tensor, degree: int, lower: float, upper: float,
+                 spectrum_min: float) -> torch.Tensor:
+        if upper <= lower:
+            raise ValueError(f"filter interval is empty: lower={lower}, upper={upper}")
+        if self.disabled_reason is not None:
+            return self._direct("disabled", hamiltonian, block, degree, lower, upper, spectrum_min)
+        if block.device.type != "cuda":
+            return self._direct(f"block on {block.device.type}; graphs are CUDA-only", hamiltonian, block, degree,
+                                lower, upper, spectrum_min)
+        seam, why = self._seam(hamiltonian, block)
+        if seam is None:
+            return self._direct(why, hamiltonian, block, degree, lower, upper, spectrum_min)
+        rows = chebyshev_coefficients(degree, lower, upper, spectrum_min)
+        potential = seam.filter_potential()
+        key = (seam.graph_geometry_key(), seam.dtype, tuple(block.shape), block.dtype, tuple(potential.shape),
+               potential.dtype, int(degree))
+        if key != self._key or self._generation != _lib.timeouts_reported:
+            if self.captures >= GRAPH_MAX_CAPTURES:
+                self._disable(f"more than {GRAPH_MAX_CAPTURES} captures (block shape or geometry keeps changing)")
+                return self._direct("disabled", hamiltonian, block, degree, lower, upper, spectrum_min)
+            try:
+                self._capture(seam, block, potential, rows, key)
+            except Exception as exc:  # noqa: BLE001 - any capture failure is recorded, then direct calls
+                self._disable(f"capture failed: {type(exc).__name__}: {exc}")
+                return self._direct("disabled", hamiltonian, block, degree, lower, upper, spectrum_min)
+        s = self._static
+        try:
+            table = torch.tensor(rows, dtype=torch.float64).pin_memory()
+            s["table"].copy_(table, non_blocking=True)
+            if potential.data_ptr() != s["potential"].data_ptr():
+                s["potential"].copy_(potential)
+            s["input"].copy_(block)
+            self._graph.replay()
+        except Exception as exc:  # noqa: BLE001 - a replay failure is recorded, then direct calls
+            self._disable(f"replay failed: {type(exc).__name__}: {exc}")
+            return self._direct("disabled", hamiltonian, block, degree, lower, upper, spectrum_min)
+        if not self._validated:
+            direct = self._filter_directly(hamiltonian, block, degree, lower, upper, spectrum_min)
+            diff, scale = torch.stack([(direct - s["output"]).abs().max(), direct.abs().max()]).tolist()
+            relative = diff / scale if scale > 0.0 else diff
+            self.validation_max_rel_diff = max(relative, self.validation_max_rel_diff or 0.0)
+            self.eager_calls["validation of a new capture"] = self.eager_calls.get("validation of a new capture", 0) + 1
+            if diff != 0.0:
+                self._disable(f"replay differs from the direct call by {relative:.3e} (relative)")
+            else:
+                self._validated = True
+            return direct
+        self.replays += 1
+        seam.note_applications(degree)
+        return s["output"].clone()
+
+    def _capture(self, hamiltonian, block: torch.Tensor, potential: torch.Tensor, rows, key) -> None:
+        self._release()
+        device = block.device
+        x = block.contiguous()
+        batch = x.numel() // x.shape[-1]
+        static = {"input": x.clone(), "potential": potential.detach().clone(),
+                  "table": torch.tensor(rows, dtype=torch.float64, device=device), "output": torch.empty_like(x)}
+        op = hamiltonian.operator(static["potential"], orbitals_per_group=batch)
+        static["work"] = filter_workspace(op, batch, device)
+        static["op"] = op
+        degree = len(rows)
+
+        def launch():
+            call("cdftb_chebyshev_filter", ctypes.byref(op), ptr(static["input"]), _lib.dtype_code(static["input"]),
+                 ptr(static["output"]), _lib.dtype_code(static["output"]), ptr(static["work"]),
+                 static["work"].numel(), batch, ptr(static["table"]), degree, stream_handle(device))
+
+        # a direct call first: the tile autotuner (which synchronises) sees the shape outside the capture
+        launch()
+        self.warmup_applications += degree
+        torch.cuda.current_stream(device).synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            launch()
+        self._graph = graph
+        self._template = hamiltonian  # keeps every geometry tensor the graph reads alive
+        self._static = static
+        self._key = key
+        self._validated = False
+        self.captures += 1
+
+
 class RitzWorkspace:
     """Device buffers of one Rayleigh--Ritz step, reused across calls of the same shape."""
 
@@ -268,9 +425,11 @@ class ChebyshevFilteredSubspace:
     """
 
     def __init__(self, grid, config: EigenConfig, ritz_stop: bool = True, filter_hamiltonian=None,
-                 switch_residual: float | None = None) -> None:
+                 switch_residual: float | None = None, filter_engine=None) -> None:
         self.grid = grid
         self.config = config
+        #: A ``GraphedChebyshevFilter`` to run the filter through (None: direct library calls).
+        self.filter_engine = filter_engine
         self.ritz_stop = ritz_stop
         self.filter_hamiltonian = filter_hamiltonian
         #: With a float filter: once the worst wanted residual falls below this, filter in float64
@@ -337,7 +496,8 @@ class ChebyshevFilteredSubspace:
                 fraction = _interval_fraction(lower, spectrum_min, spectrum_max)
             top_fraction = max(top_fraction, fraction)
             lower = min(max(lower, spectrum_min + 1e-8), spectrum_max - 1e-8)
-            filtered = chebyshev_filter(filt, vectors, cfg.chebyshev_degree, lower, spectrum_max, spectrum_min)
+            filtered = (self.filter_engine or chebyshev_filter)(filt, vectors, cfg.chebyshev_degree, lower,
+                                                                 spectrum_max, spectrum_min)
             if filt is not hamiltonian:
                 hamiltonian.note_applications(cfg.chebyshev_degree)
                 self.float_filter_iterations += 1

@@ -171,7 +171,12 @@ class CuspFactoredHamiltonian:
         return self._potential
 
     def graph_geometry_key(self) -> tuple:
-        return ("cusp-native", id(self.grid), tuple(f.data_ptr() for f in self._faces), self._inv.data_ptr())
+        return ("cusp-native", id(self.grid), tuple(f.data_ptr() for f in self._faces), self._inv.data_ptr(),
+                self.measure.quadrature.data_ptr())
+
+    def filter_potential(self) -> torch.Tensor:
+        """The potential as the filter reads it (in the operator's dtype)."""
+        return self._pot_cast
 
     def local_potential(self) -> torch.Tensor:
         return self._potential

@@ -16,8 +16,7 @@ CUDA path dispatches through, and nothing else:
   ``ChebyshevFilteredSubspace.solve`` and the graph engine): the fused filter, one launch per step;
 - ``graphed_filter_for`` in ``cdft.eigen.chefsi`` and, imported there by name, in ``cdft.scf.loop``
   (``loop.py:34``) and ``cdft.scf.noninteracting`` (``noninteracting.py:30``): an engine with the
-  graph engine's call and ``record()`` keys whose calls are the fused filter (no graph is needed:
-  one launch per step, no host synchronisation);
+  graph engine's call and ``record()`` keys that replays the fused filter from a CUDA graph;
 - ``CoulombCutoffPoisson.solve`` (``src/cdft/operators/poisson.py:66``, a class method because the
   class is imported by name in ``step.py:53`` and ``loop.py:43``): the native pruned-FFT plan;
 - ``SemiLocalFunctional.evaluate`` (``src/cdft/xc/base.py:115``, the base of every functional the
@@ -45,6 +44,7 @@ import torch
 
 from . import _lib
 from ._lib import call, ptr, stream_handle
+from .eigen import GraphedChebyshevFilter
 
 ENV_NATIVE = "CDFT_NATIVE"
 MODES = ("auto", "on", "off")
@@ -258,41 +258,76 @@ def chebyshev_filter(hamiltonian, block, degree, lower, upper, spectrum_min):
     return out
 
 
-class NativeFilterEngine:
-    """In place of ``GraphedChebyshevFilter`` (``chefsi.py:185-392``): the same call and the same
-    ``record()`` keys. Its calls are the fused filter -- one launch per step, no host read -- so
-    there is nothing to capture; an operator the fused filter does not cover runs the reference's
-    eager recurrence, counted by reason as the graph engine counts its eager calls."""
+class _ReferenceSeam:
+    """The graph seam of the native filter over the reference's ``CuspFactoredHamiltonian``: its
+    geometry and potential as a ``cdftb_operator`` (``_operator_of``), keyed by the pointers the
+    operator carries."""
 
-    def __init__(self, device) -> None:
-        self.device = torch.device(device)
-        self.captures = 0
-        self.replays = 0
-        self.eager_calls: collections.Counter = collections.Counter()
-        self.warmup_applications = 0
-        self.validation_max_rel_diff = None
-        self.disabled_reason = None
+    dtype = torch.float64
 
-    def __call__(self, hamiltonian, block, degree, lower, upper, spectrum_min):
-        if upper <= lower:
-            raise ValueError(f"filter interval is empty: lower={lower}, upper={upper}")
-        out, why = native_filter(hamiltonian, block, degree, lower, upper, spectrum_min)
+    def __init__(self, ham, potential: torch.Tensor, op) -> None:
+        self.ham = ham
+        self._potential = potential
+        faces, inv, _ = op._keep
+        self._key = ("cusp-reference", tuple(int(n) for n in ham.grid.shape), float(ham.grid.spacing),
+                     tuple(f.data_ptr() for f in faces), inv.data_ptr())
+
+    def operator(self, potential: torch.Tensor, orbitals_per_group: int = 1):
+        op, why = _operator_of(self.ham, potential)
+        if op is None:
+            raise RuntimeError(why)
+        op.orbitals_per_group = int(orbitals_per_group)
+        return op
+
+    def filter_potential(self) -> torch.Tensor:
+        return self._potential
+
+    def graph_geometry_key(self) -> tuple:
+        return self._key
+
+    def note_applications(self, count: int) -> None:
+        self.ham.note_applications(int(count))
+
+
+class NativeFilterEngine(GraphedChebyshevFilter):
+    """In place of ``GraphedChebyshevFilter`` (``chefsi.py:185-392``), with its call and its
+    ``record()`` keys: the fused filter on the reference's operator, replayed from a CUDA graph
+    per block shape and geometry (this package's engine). An operator the fused filter does not
+    cover (the level-shifted rung) runs the reference's eager recurrence, counted by reason as
+    the reference's engine counts its eager calls."""
+
+    def _seam(self, ham, block):
+        if block.dtype != torch.float64:
+            return None, "not float64"
+        if not all(hasattr(ham, a) for a in ("grid", "factor", "_inverse_weight", "graph_potential",
+                                             "note_applications")):
+            return None, f"operator {type(ham).__name__} is not a cusp-factorised Hamiltonian"
+        potential = ham.graph_potential()
+        if potential.dim() != 1:
+            return None, "potential is not one (n_points,) field"
+        potential = potential.to(torch.float64).contiguous()
+        op, why = _operator_of(ham, potential)
+        if op is None:
+            return None, why
+        return _ReferenceSeam(ham, potential, op), None
+
+    def _filter_directly(self, ham, block, degree, lower, upper, spectrum_min):
+        out = None
+        if block.device.type == "cuda":
+            out, _ = native_filter(ham, block, degree, lower, upper, spectrum_min)
         if out is None:
-            self.eager_calls[why] += 1
             original = _original("cdft.eigen.chefsi", "chebyshev_filter")
-            return original(hamiltonian, block, degree, lower=lower, upper=upper, spectrum_min=spectrum_min)
-        self.replays += 1
+            return original(ham, block, degree, lower=lower, upper=upper, spectrum_min=spectrum_min)
+        return out
+
+    def __call__(self, ham, block, degree, lower, upper, spectrum_min):
+        out = super().__call__(ham, block, degree, lower, upper, spectrum_min)
         _STATE.native_calls["filter_engine"] += 1
         return out
 
     def record(self) -> dict:
-        used = self.replays > 0
-        out = {"used": used, "captures": self.captures, "replays": self.replays,
-               "eager_calls": dict(self.eager_calls), "warmup_applications": self.warmup_applications,
-               "validation_max_rel_diff": self.validation_max_rel_diff,
-               "engine": f"{TIER} fused filter (one launch per Chebyshev step; no graph)"}
-        if not used:
-            out["reason"] = "no filter call was native" if self.eager_calls else "the filter was never called"
+        out = super().record()
+        out["engine"] = f"{TIER} fused filter (one launch per Chebyshev step) replayed from a CUDA graph"
         return out
 
 

@@ -22,7 +22,7 @@ import torch
 from . import _lib
 from ._lib import call, ptr, stream_handle
 from .eigen import (BOUND_REUSE_RITZ_FRACTION, ChebyshevFilteredSubspace, EigenConfig, EigenResult,
-                    SpectralBoundsHint)
+                    GraphedChebyshevFilter, SpectralBoundsHint)
 from .geometry import CuspGeometry, _hptr, _host, gradient, partial_derivative, row_sums
 from .operators import CuspFactoredHamiltonian, measure_cross
 from .poisson import CoulombCutoffPoisson
@@ -77,7 +77,10 @@ class KohnShamStep:
 
     def __init__(self, geometry: CuspGeometry, functional: str, n_electrons: float, eigen: EigenConfig | None = None,
                  *, seed: int = 0, pad_factor: float = 2.5, filter_precision: torch.dtype = torch.float64,
-                 n_states: int | None = None, external_potential: torch.Tensor | None = None) -> None:
+                 n_states: int | None = None, external_potential: torch.Tensor | None = None,
+                 graphs: bool = False) -> None:
+        # graphs: run every Chebyshev filter of the solve through one GraphedChebyshevFilter (its
+        # record lands in the outcome's measurements["cuda_graphs"])
         # external_potential: an extra diagonal term of the operator (an external perturbation in the
         # form quadrature.effective_potential gives it). It enters the Hamiltonian and so the band
         # energy, but not the Hartree/XC double counting, so the total energy gains Q[n dv].
@@ -99,6 +102,7 @@ class KohnShamStep:
         self._bare = CuspFactoredHamiltonian(self.grid, self.factor, quadrature=self.quadrature)
         self.filter_precision = filter_precision
         self._f2_grid = self.factor.weight
+        self.filter_engine = GraphedChebyshevFilter(self.grid.device) if graphs else None
         n = self.grid.n_points
         dev = self.grid.device
         self._fields = torch.empty((2, n), dtype=torch.float64, device=dev)
@@ -260,7 +264,7 @@ class KohnShamStep:
             cfg = EigenConfig(**{**cfg.__dict__, "max_iterations": max_iterations})
         switch = self.FLOAT_FILTER_SWITCH_RESIDUAL if max_iterations is None else None
         solver = ChebyshevFilteredSubspace(self.grid, cfg, ritz_stop=False, filter_hamiltonian=filter_hamiltonian,
-                                           switch_residual=switch)
+                                           switch_residual=switch, filter_engine=self.filter_engine)
         result = solver.solve(hamiltonian, self.n_states, initial=initial, generator=generator, bounds=bounds)
         info = {"eigen_stop_reason": solver.stop_reason, "eigen_eigenvalue_drift": solver.eigenvalue_drift,
                 "eigen_spectral_bounds": list(solver.spectral_bounds or ()), "eigen_bounds_source": solver.bounds_source,
@@ -680,6 +684,8 @@ def solve_self_consistent(step: KohnShamStep, mixing: MixingConfig | None = None
         "fused_kernels": {"tier": "native-sm100a", "library": _lib.LIBRARY_PATH.name},
         "wall_s": time.perf_counter() - started,
     }
+    if step.filter_engine is not None:
+        measurements["cuda_graphs"] = step.filter_engine.record()
     return SCFOutcome(energies=final, eigenvalues=host[nt + 1:], scf_iterations=iteration,
                       converged=converged and eigen.converged, applications=measurements["hamiltonian_applications"],
                       energy_history=energies, residual_history=residuals, density=n_out, measurements=measurements)
@@ -700,7 +706,7 @@ def lobpcg_cross_check(hamiltonian, eigenvalues: torch.Tensor, n_states: int, ei
 
 def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: int = 0,
                          eigen: EigenConfig | None = None, external_potential: torch.Tensor | None = None,
-                         cross_check: bool | None = None) -> dict:
+                         cross_check: bool | None = None, graphs: bool = False) -> dict:
     """(``src/cdft/scf/noninteracting.py:118-330``) for the cusp-factorised path, ``ritz_stop=True``.
 
     ``external_potential`` adds a diagonal term to the operator (an external perturbation in the
@@ -715,7 +721,8 @@ def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: in
                                   quadrature=geometry.quadrature)
     n_states = max(1, int(-(-float(n_electrons) // 2.0)))
     generator = SeededStream(seed, grid.device)
-    solver = ChebyshevFilteredSubspace(grid, eigen, ritz_stop=True)
+    engine = GraphedChebyshevFilter(grid.device) if graphs else None
+    solver = ChebyshevFilteredSubspace(grid, eigen, ritz_stop=True, filter_engine=engine)
     result = solver.solve(ham, n_states, generator=generator)
     occ = torch.from_numpy(aufbau_occupations(n_states, float(n_electrons))).to(grid.device)
     kinetic = ham.kinetic_energy_tensor(result.eigenvectors, occ[0])
@@ -727,6 +734,8 @@ def solve_noninteracting(geometry: CuspGeometry, n_electrons: float, *, seed: in
     out = {"total": kinetic + external + ion_ion, "kinetic": kinetic, "eigenvalues": vals[2:],
            "iterations": result.n_iterations, "converged": result.converged, "applications": float(ham.apply_count),
            "stop_reason": solver.stop_reason, "orbitals": result.eigenvectors, "occupations": occ[0]}
+    if engine is not None:
+        out["cuda_graphs"] = engine.record()
     if cross_check:
         out.update(lobpcg_cross_check(ham, result.eigenvalues, n_states, eigen, seed))
     return out

@@ -86,10 +86,12 @@ def test_filter_and_engine(plugin, he17):
     assert why is None and ham._apply_count == 12
     assert np.abs(out.cpu().numpy() - want).max() < 1e-11 * np.abs(want).max()
     engine = plugin.graphed_filter_for(x.device)
-    again = engine(ham, x, *args)
-    assert torch.equal(again, out)
+    first = engine(ham, x, *args)  # captures, replays once and returns the direct call it checked against
+    again = engine(ham, x, *args)  # a replay
+    assert torch.equal(first, out) and torch.equal(again, out)
     rec = engine.record()
-    assert rec["used"] and rec["replays"] == 1
+    assert rec["used"] and rec["replays"] == 1 and rec["captures"] == 1
+    assert rec["validation_max_rel_diff"] == 0.0
     assert {"used", "captures", "replays", "eager_calls", "warmup_applications",
             "validation_max_rel_diff"} <= set(rec)
     assert plugin.graphed_filter_for(torch.device("cpu")) is None

@@ -356,16 +356,16 @@ def batched_chefsi(h: BatchedHamiltonian, h32: BatchedHamiltonian | None, n_stat
     extra = max(config.n_extra_states, int(config.extra_states_fraction * n_states))
     m = min(n_states + extra, n)
     # the start block, written once in place: the carried vectors, then each system's fresh draws
-    block = torch.empty((b, m, n), dtype=torch.float64, device=dev)
-    for s in range(b):
-        if initial is None:
-            block[s] = streams[s].randn((m, n))
-        else:
-            blk = initial[s].reshape(-1, n)
-            k = min(blk.shape[0], m)
-            block[s, :k] = blk[:k]
-            if k < m:
-                block[s, k:] = streams[s].randn((m - k, n))
+    # (one gather of the b draws and one copy of the carried rows, not a copy per system)
+    if initial is None:
+        block = torch.stack([streams[s].randn((m, n)) for s in range(b)])
+    else:
+        carried = initial.reshape(b, -1, n)
+        k = min(carried.shape[1], m)
+        block = torch.empty((b, m, n), dtype=torch.float64, device=dev)
+        block[:, :k] = carried[:, :k]
+        if k < m:
+            block[:, k:] = torch.stack([streams[s].randn((m - k, n)) for s in range(b)])
     states = [_EigenState(float_filter=h32 is not None and (float_mask is None or bool(float_mask[s])))
               for s in range(b)]
     need = [s for s in range(b) if bounds[s] is None]

@@ -322,3 +322,24 @@ def test_fused_density_residual_and_external_terms(pkg, cuda, k):
     dot = (grad[:, 0] * grad_u[0] + grad[:, 1] * grad_u[1]) + grad[:, 2] * grad_u[2]
     assert torch.equal(out[:, 0], far[None] * (weight[None] * dot))
     assert torch.equal(out[:, 1], far[None] * ((weight[None] * rho) * tpot[None]))
+
+
+def test_lift_plan_is_the_point_node_order(pkg, he25):
+    """The CSR of L^T (``cdftb_lift_plan_build``): every (node, tap) entry, ordered by grid point and,
+    within a point, by node -- the order of a sort on the full (point, node) keys."""
+    _, geo, _ = he25
+    q = geo.quadrature
+    nx, ny, nz = geo.grid.shape
+    base = q.base.cpu().numpy().astype(np.int64)
+    m = base.shape[0]
+    t = np.arange(512)
+    a, b, c = t >> 6, (t >> 3) & 7, t & 7
+    ix = base[:, 0:1] - 3 + a[None, :]
+    iy = base[:, 1:2] - 3 + b[None, :]
+    iz = base[:, 2:3] - 3 + c[None, :]
+    point = ((ix * ny + iy) * nz + iz).ravel()
+    node = np.repeat(np.arange(m), 512)
+    order = np.lexsort((node, point))
+    assert np.array_equal(q.col.cpu().numpy(), node[order].astype(np.int32))
+    counts = np.bincount(point, minlength=nx * ny * nz)
+    assert np.array_equal(q.row_ptr.cpu().numpy(), np.concatenate([[0], np.cumsum(counts)]))
